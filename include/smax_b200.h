@@ -1,0 +1,155 @@
+/*
+ * smax_b200.h -- C ABI of the SmaxKernels sm_100a (B200) CUDA platform.
+ *
+ * This is the boundary a SmaxKernels build binds to run its
+ * PlatformType::CUDA kernels on a B200.  It replaces, one for one, the
+ * reference's per-platform entry points
+ *
+ *   SPMV::initialize_cuda / apply_cuda / finalize_cuda
+ *       (src/kernels/spmv/spmv_cuda.hpp:137-184, bodies in
+ *        src/kernels/spmv/spmv_cuda/spmv_cuda_core.cuh:11-205)
+ *
+ * and adds the CUDA arms the reference lacks for SpMM, SpGEMM, SpTRSV and
+ * SpTRSM (src/kernels/spmm.hpp:68-100, spgemm.hpp:91-130, sptrsv.hpp:74-113,
+ * sptrsm.hpp:67-106 only dispatch to the CPU).  The objects mirror the
+ * reference's own:
+ *
+ *   smax_ctx     <-> SMAX::Interface's UtilitiesContainer (level pointers
+ *                    written by Utils::generate_perm, src/common.hpp:187-195)
+ *   smax_kernel  <-> one registered SMAX::Kernel: KernelContext + Args + Flags
+ *                    (src/kernel.hpp:7-127, src/kernels/<k>/<k>_common.hpp)
+ *
+ * Conventions
+ *   - Every function returns smax_status: 0 on success, a negative SMAX_ERR_*
+ *     code otherwise; smax_last_error() then holds a message for the calling
+ *     thread.  Nothing here exits, aborts or traps.
+ *   - Pointers given to register_* are HOST pointers owned by the caller, as in
+ *     the reference (src/kernels/spmv.hpp:89-91), unless the kernel has the
+ *     SMAX_FLAG_DEVICE_POINTERS flag, in which case B and C are device pointers.
+ *   - Index type int32 and value types float32/float64 are supported; other
+ *     combinations return SMAX_ERR_UNSUPPORTED_TYPE.
+ *   - Streams are passed as void* (a cudaStream_t).
+ */
+#ifndef SMAX_B200_H
+#define SMAX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SMAX_B200_ABI_VERSION 1
+
+typedef int smax_status;
+
+/* status codes */
+#define SMAX_OK 0
+#define SMAX_ERR_BAD_ARG (-1)
+#define SMAX_ERR_UNSUPPORTED_TYPE (-2)
+#define SMAX_ERR_OOM (-3)
+#define SMAX_ERR_ZERO_DIAG (-4)
+#define SMAX_ERR_NO_DIAG (-5)
+#define SMAX_ERR_TIMEOUT (-6)
+#define SMAX_ERR_CUDA (-7)
+#define SMAX_ERR_COL_OOB (-8)
+#define SMAX_ERR_STATE (-9)
+#define SMAX_ERR_UNSUPPORTED (-10)
+
+/* kernel types, in the order of SMAX::KernelType (src/common.hpp:12) */
+#define SMAX_KERNEL_SPMV 0
+#define SMAX_KERNEL_SPMM 1
+#define SMAX_KERNEL_SPGEMM 2
+#define SMAX_KERNEL_SPTRSV 3
+#define SMAX_KERNEL_SPTRSM 4
+
+/* index / value types, in the order of SMAX::IntType / SMAX::FloatType
+ * (src/common.hpp:25-28) */
+#define SMAX_INT16 0
+#define SMAX_INT32 1
+#define SMAX_INT64 2
+#define SMAX_UINT16 3
+#define SMAX_UINT32 4
+#define SMAX_UINT64 5
+#define SMAX_FLOAT32 0
+#define SMAX_FLOAT64 1
+
+/* kernel flags: the reference's Kernel::set_* setters (src/kernel.hpp:58-90)
+ * plus platform options */
+#define SMAX_FLAG_MAT_PERM 0           /* set_mat_perm: level-scheduled solve */
+#define SMAX_FLAG_MAT_UPPER_TRIANG 1   /* set_mat_upper_triang */
+#define SMAX_FLAG_MAT_LOWER_TRIANG 2   /* set_mat_lower_triang */
+#define SMAX_FLAG_VEC_ROW_MAJOR 3      /* set_vec_row_major */
+#define SMAX_FLAG_MAT_SCS 4            /* set_mat_scs */
+#define SMAX_FLAG_MAT_BCRS 5           /* set_mat_bcrs */
+#define SMAX_FLAG_BLOCK_COLUMN_MAJOR 6 /* set_block_column_major */
+#define SMAX_FLAG_KERNEL_IMPL 7        /* set_kernel_implementation(SpMVType) */
+#define SMAX_FLAG_DEVICE_POINTERS 8    /* B and C registered as device pointers */
+#define SMAX_FLAG_A_DIRTY 9            /* re-upload A at the next initialize */
+
+typedef struct smax_ctx_s *smax_ctx;
+typedef struct smax_kernel_s *smax_kernel;
+
+/* ---------------------------------------------------------------- library */
+int smax_abi_version(void);
+const char *smax_last_error(void);
+
+/* ---------------------------------------------------------------- context */
+/* Interface-level state; kernels created from one context share its level
+ * sets (src/interface.hpp:23-26, src/interface.cpp:53-57). */
+smax_status smax_ctx_create(smax_ctx *out);
+smax_status smax_ctx_destroy(smax_ctx ctx);
+int smax_ctx_get_n_levels(smax_ctx ctx);             /* Interface::get_n_levels */
+int smax_ctx_get_level_ptr_at(smax_ctx ctx, int idx); /* Interface::get_level_ptr_at */
+
+/* ---------------------------------------------------------------- kernels */
+/* Interface::register_kernel(name, KernelType, PlatformType::CUDA, IntType,
+ * FloatType) (src/interface.cpp:59-123). */
+smax_status smax_kernel_create(smax_kernel *out, smax_ctx ctx, int kernel_type, int int_type,
+                               int float_type);
+smax_status smax_kernel_destroy(smax_kernel k);
+smax_status smax_kernel_set_flag(smax_kernel k, int flag, int value);
+
+/* register_A for a CRS matrix, argument order of src/kernels/spmv.hpp:77-91
+ * (also SpMM, SpGEMM A, SpTRSV and SpTRSM: spmm.hpp:24-38, spgemm.hpp:34-48,
+ * sptrsv.hpp:23-37, sptrsm.hpp:23-37). */
+smax_status smax_kernel_register_A_crs(smax_kernel k, uint64_t n_rows, uint64_t n_cols, uint64_t nnz,
+                                       void *col, void *row_ptr, void *val);
+
+/* register_B / register_C of a dense operand: (n_rows, val) for vectors
+ * (spmv.hpp:97-115, sptrsv.hpp:40-58) or (n_rows, n_cols, val) for blocks of
+ * vectors (spmm.hpp:40-61, sptrsm.hpp:40-60).  slot 1 = B, slot 2 = C. */
+smax_status smax_kernel_register_dense(smax_kernel k, int slot, uint64_t n_rows, uint64_t n_cols, void *val);
+
+/* Kernel::initialize / apply / finalize / run with the reference's offset
+ * arguments (src/kernel.hpp:48-52,99-111).  On this platform initialize
+ * uploads A (only when registered anew or marked dirty) and B, apply launches
+ * the kernel asynchronously on the kernel's stream, finalize downloads C and
+ * synchronises. */
+smax_status smax_kernel_initialize(smax_kernel k, uint64_t A_offset, uint64_t B_offset, uint64_t C_offset);
+smax_status smax_kernel_apply(smax_kernel k, uint64_t A_offset, uint64_t B_offset, uint64_t C_offset);
+smax_status smax_kernel_finalize(smax_kernel k, uint64_t A_offset, uint64_t B_offset, uint64_t C_offset);
+smax_status smax_kernel_run(smax_kernel k, uint64_t A_offset, uint64_t B_offset, uint64_t C_offset);
+
+/* Waits for the kernel's stream and reports any device-side error. */
+smax_status smax_kernel_sync(smax_kernel k);
+
+/* Accumulated seconds of a stopwatch ("initialize", "apply", "finalize", ...;
+ * src/kernel.hpp:36-43).  "apply" is measured with CUDA events on the
+ * kernel's stream. */
+smax_status smax_kernel_get_timer(smax_kernel k, const char *name, double *seconds);
+
+/* The kernel's CUDA stream (a cudaStream_t). */
+void *smax_kernel_stream(smax_kernel k);
+
+/* Runs the kernel's work on the caller's stream (a cudaStream_t, e.g. the
+ * current stream of a framework) instead of its own; NULL restores its own.
+ * The caller keeps ownership of the stream. */
+smax_status smax_kernel_set_stream(smax_kernel k, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SMAX_B200_H */

@@ -1,0 +1,81 @@
+"""ctypes binding of libsmax_b200.so (the C ABI declared in include/smax_b200.h).
+
+The library is built in-tree by ``python smaxkernels_b200/build.py`` (or
+``__graft_entry__.build()``).  There is no fallback: if the library is missing
+or cannot be loaded, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsmax_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is not built; run `python smaxkernels_b200/build.py`")
+
+lib = C.CDLL(LIB_PATH)
+
+P = C.c_void_p
+U64 = C.c_uint64
+I32 = C.c_int
+PP = C.POINTER(C.c_void_p)
+PU64 = C.POINTER(C.c_uint64)
+
+# name -> (restype, argtypes); kept in the order of include/smax_b200.h
+SIGNATURES = {
+    "smax_abi_version": (I32, []),
+    "smax_last_error": (C.c_char_p, []),
+    "smax_ctx_create": (I32, [PP]),
+    "smax_ctx_destroy": (I32, [P]),
+    "smax_ctx_get_n_levels": (I32, [P]),
+    "smax_ctx_get_level_ptr_at": (I32, [P, I32]),
+    "smax_kernel_create": (I32, [PP, P, I32, I32, I32]),
+    "smax_kernel_destroy": (I32, [P]),
+    "smax_kernel_set_flag": (I32, [P, I32, I32]),
+    "smax_kernel_register_A_crs": (I32, [P, U64, U64, U64, P, P, P]),
+    "smax_kernel_register_dense": (I32, [P, I32, U64, U64, P]),
+    "smax_kernel_initialize": (I32, [P, U64, U64, U64]),
+    "smax_kernel_apply": (I32, [P, U64, U64, U64]),
+    "smax_kernel_finalize": (I32, [P, U64, U64, U64]),
+    "smax_kernel_run": (I32, [P, U64, U64, U64]),
+    "smax_kernel_sync": (I32, [P]),
+    "smax_kernel_get_timer": (I32, [P, C.c_char_p, C.POINTER(C.c_double)]),
+    "smax_kernel_stream": (P, [P]),
+    "smax_kernel_set_stream": (I32, [P, P]),
+}
+
+for _name, (_res, _args) in SIGNATURES.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+# status codes (include/smax_b200.h)
+OK = 0
+ERR_BAD_ARG = -1
+ERR_UNSUPPORTED_TYPE = -2
+ERR_OOM = -3
+ERR_ZERO_DIAG = -4
+ERR_NO_DIAG = -5
+ERR_TIMEOUT = -6
+ERR_CUDA = -7
+ERR_COL_OOB = -8
+ERR_STATE = -9
+ERR_UNSUPPORTED = -10
+
+STATUS_NAMES = {0: "OK", -1: "BAD_ARG", -2: "UNSUPPORTED_TYPE", -3: "OOM", -4: "ZERO_DIAG", -5: "NO_DIAG",
+                -6: "TIMEOUT", -7: "CUDA", -8: "COL_OOB", -9: "STATE", -10: "UNSUPPORTED"}
+
+
+class SmaxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{STATUS_NAMES.get(code, code)}] {msg}")
+        self.code = code
+
+
+def check(rc: int) -> int:
+    if rc != OK:
+        msg = lib.smax_last_error()
+        raise SmaxError(rc, msg.decode() if msg else "")
+    return rc

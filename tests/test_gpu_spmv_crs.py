@@ -1,0 +1,99 @@
+"""Parity of the CUDA CRS SpMV with the oracle (and the reference's golden
+vectors), through the C ABI via the Python mirror of SMAX::Interface."""
+import numpy as np
+import pytest
+
+import golden_cases as G
+from helpers import gpu_spmv, normwise, rand_crs, tol
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+O = Oracle()
+
+
+def test_golden_spmv_test():
+    c = G.spmv_case()
+    y = gpu_spmv(c["row_ptr"], c["col"], c["val"], c["x"])
+    assert G.almost_equal(y, c["y"], np.float64)
+
+
+@pytest.mark.parametrize("vt", [np.float64, np.float32])
+@pytest.mark.parametrize("case", ["small", "empty_rows", "long_rows", "single_row", "ragged"])
+def test_random_vs_oracle(vt, case):
+    kw = dict(small=dict(n=257, maxlen=9), empty_rows=dict(n=3001, maxlen=40, empty_frac=0.5),
+              long_rows=dict(n=5000, maxlen=20, long_rows=(1025, 2049, 4097, 4999)),
+              single_row=dict(n=1, maxlen=1, n_cols=7000, long_rows=(6000,)),
+              ragged=dict(n=20011, maxlen=300))[case]
+    n_cols = kw.pop("n_cols", None)
+    rp, col, val = rand_crs(seed=11, vt=vt, n_cols=n_cols, **kw)
+    x = np.random.default_rng(12).uniform(-1, 1, n_cols or len(rp) - 1).astype(vt)
+    y = gpu_spmv(rp, col, val, x)
+    y_ref = O.spmv_crs(rp, col, val, x)  # reference arithmetic in VT
+    assert normwise(y, y_ref) <= tol(vt)
+    y64 = O.spmv_crs(rp, col, val.astype(np.float64), x.astype(np.float64))
+    assert normwise(y, y64) <= tol(vt)
+
+
+def test_all_rows_empty():
+    n = 1000
+    rp = np.zeros(n + 1, np.int32)
+    y = gpu_spmv(rp, np.zeros(0, np.int32), np.zeros(0), np.ones(n))
+    assert np.all(y == 0)
+
+
+def test_config0_laplace64():
+    from smaxkernels_b200 import matrices as M
+    rp, col, val = M.laplace3d_7pt(64)
+    x = M.uniform_vector(len(rp) - 1, 0)
+    y = gpu_spmv(rp, col, val, x)
+    assert normwise(y, O.spmv_crs(rp, col, val, x)) <= 1e-12
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("vt", [np.float64, np.float32])
+def test_config1_lognormal_full_size(vt):
+    from smaxkernels_b200 import matrices as M
+    rp, col, val = M.lognormal_random(1 << 22, dtype=vt)
+    x = M.uniform_vector(len(rp) - 1, 1, dtype=vt)
+    y = gpu_spmv(rp, col, val, x)
+    assert normwise(y, O.spmv_crs(rp, col, val, x)) <= tol(vt)
+    y64 = O.spmv_crs(rp, col, val.astype(np.float64), x.astype(np.float64))
+    assert normwise(y, y64) <= tol(vt)
+
+
+def test_offsets_and_repeated_runs():
+    """x/y offsets (src/kernel.hpp:99-111) and reuse of the resident matrix."""
+    from smaxkernels_b200 import FloatType, Interface, KernelType, PlatformType, IntType
+    rp, col, val = rand_crs(2000, 30, 5)
+    n = 2000
+    X = np.random.default_rng(1).uniform(-1, 1, 2 * n)
+    Y = np.zeros(2 * n)
+    smax = Interface()
+    smax.register_kernel("k", KernelType.SPMV, PlatformType.CUDA, IntType.INT32, FloatType.FLOAT64)
+    k = smax.kernel("k")
+    k.register_A(n, n, len(col), col, rp, val)
+    k.register_B(2 * n, X)
+    k.register_C(2 * n, Y)
+    k.run(0, n, 0)
+    k.run(0, 0, n)
+    assert normwise(Y[:n], O.spmv_crs(rp, col, val, X[n:])) <= 1e-12
+    assert normwise(Y[n:], O.spmv_crs(rp, col, val, X[:n])) <= 1e-12
+    assert k.timer("apply") > 0
+    smax.close()
+
+
+def test_device_pointers_torch():
+    import torch
+    from smaxkernels_b200 import FloatType, Interface, KernelType, PlatformType, IntType
+    rp, col, val = rand_crs(4000, 50, 6)
+    x = torch.rand(4000, dtype=torch.float64, device="cuda")
+    y = torch.zeros(4000, dtype=torch.float64, device="cuda")
+    smax = Interface()
+    smax.register_kernel("k", KernelType.SPMV, PlatformType.CUDA, IntType.INT32, FloatType.FLOAT64)
+    k = smax.kernel("k")
+    k.register_A(4000, 4000, len(col), col, rp, val)
+    k.register_B(4000, x)
+    k.register_C(4000, y)
+    k.run()
+    assert normwise(y.cpu().numpy(), O.spmv_crs(rp, col, val, x.cpu().numpy())) <= 1e-12
+    smax.close()
