@@ -30,6 +30,31 @@ int sm_count() {
     return n;
 }
 
+namespace {
+// One pass over an uploaded CRS matrix: row_ptr[0] == 0, row_ptr[n] == nnz,
+// row_ptr non-decreasing, every column in [0, n_cols).  Hot kernels trust the
+// matrix afterwards, so malformed input becomes an error status here instead
+// of an out-of-bounds access later.
+__global__ void validate_crs_kernel(const int *__restrict__ row_ptr, const int *__restrict__ col, int64_t n,
+                                    int64_t nnz, int64_t n_cols, DevStatus *st) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0 && (row_ptr[0] != 0 || row_ptr[n] != nnz)) report(st, SMAX_ERR_BAD_ARG, 0);
+    for (int64_t r = t; r < n; r += stride)
+        if (row_ptr[r + 1] < row_ptr[r]) report(st, SMAX_ERR_BAD_ARG, r);
+    for (int64_t j = t; j < nnz; j += stride) {
+        int c = col[j];
+        if (c < 0 || c >= n_cols) report(st, SMAX_ERR_COL_OOB, j);
+    }
+}
+}  // namespace
+
+void validate_crs(const DevCRS &m, DevStatus *st, cudaStream_t s) {
+    int blocks = 4 * sm_count();
+    validate_crs_kernel<<<blocks, 256, 0, s>>>(m.rp(), m.ci(), m.n_rows, m.nnz, m.n_cols, st);
+    SMAX_CUDA(cudaGetLastError());
+}
+
 void DevCRS::upload(const RegCRS &r, int vbytes, cudaStream_t st) {
     n_rows = (int64_t)r.n_rows;
     n_cols = (int64_t)r.n_cols;
@@ -92,6 +117,8 @@ void require(bool c, int code, const char *msg) {
     if (!c) fail(code, msg);
 }
 
+void read_status(smax_kernel_s *k);
+
 smax_kernel_s *K(smax_kernel k) {
     require(k != nullptr, SMAX_ERR_BAD_ARG, "null kernel handle");
     return k;
@@ -115,6 +142,8 @@ void spmv_initialize(smax_kernel_s *k) {
     require(!k->f_scs && !k->f_bcrs, SMAX_ERR_UNSUPPORTED, "SCS/BCRS SpMV not available in this build");
     if (k->a_dirty) {
         k->dA.upload(k->A, k->vbytes, k->stream);
+        validate_crs(k->dA, k->status.as<DevStatus>(), k->stream);
+        read_status(k);
         k->crs_plan.build(k->dA.rp(), k->dA.n_rows, crs_default_cap(k->vbytes * 8), k->stream);
         k->a_dirty = false;
     }
@@ -156,8 +185,20 @@ void do_initialize(smax_kernel_s *k) {
     k->timers["initialize"] += wall_s() - t0;
 }
 
+// Operand extents the kernel reads (B) and writes (C), in elements.
+void check_extents(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
+    uint64_t need_b = 0, need_c = 0;
+    switch (k->ktype) {
+    case SMAX_KERNEL_SPMV: need_b = k->A.n_cols; need_c = k->A.n_rows; break;
+    default: break;
+    }
+    require(b_off + need_b <= k->B.elems(), SMAX_ERR_BAD_ARG, "B (with offset) is smaller than the operator needs");
+    require(c_off + need_c <= k->C.elems(), SMAX_ERR_BAD_ARG, "C (with offset) is smaller than the operator needs");
+}
+
 void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
     require(!k->a_dirty, SMAX_ERR_STATE, "initialize before apply");
+    check_extents(k, b_off, c_off);
     auto ev = k->apply_events.acquire();
     SMAX_CUDA(cudaEventRecord(ev.first, k->stream));
     switch (k->ktype) {

@@ -47,6 +47,8 @@ struct DevCRS {
     const int *ci() const { return col.as<int>(); }
 };
 
+void validate_crs(const DevCRS &m, DevStatus *st, cudaStream_t s);
+
 struct PendingEvents {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> live, spare;
     std::pair<cudaEvent_t, cudaEvent_t> acquire();

@@ -97,3 +97,52 @@ def test_device_pointers_torch():
     k.run()
     assert normwise(y.cpu().numpy(), O.spmv_crs(rp, col, val, x.cpu().numpy())) <= 1e-12
     smax.close()
+
+
+@pytest.mark.parametrize("poison", ["col_oob", "col_negative", "row_ptr_decreasing", "row_ptr_end"])
+def test_malformed_matrix_is_an_error_status(poison):
+    """Malformed CRS input is rejected by the upload-time validation pass with
+    an error status (the reference aborts in debug mode,
+    src/kernels/kernels_common.hpp:21-28); no kernel reads out of bounds."""
+    from smaxkernels_b200 import FloatType, Interface, IntType, KernelType, PlatformType, SmaxError
+    from smaxkernels_b200 import _lib
+    rp, col, val = rand_crs(300, 10, 3)
+    rp = rp.copy()
+    col = col.copy()
+    expect = _lib.ERR_COL_OOB
+    if poison == "col_oob":
+        col[len(col) // 2] = 300
+    elif poison == "col_negative":
+        col[0] = -1
+    elif poison == "row_ptr_decreasing":
+        rp[100], rp[101] = rp[101] + 1, rp[100]
+        expect = _lib.ERR_BAD_ARG
+    else:
+        rp[-1] = len(col) - 1
+        expect = _lib.ERR_BAD_ARG
+    smax = Interface()
+    smax.register_kernel("k", KernelType.SPMV, PlatformType.CUDA, IntType.INT32, FloatType.FLOAT64)
+    k = smax.kernel("k")
+    k.register_A(300, 300, len(col), col, rp, val)
+    k.register_B(300, np.ones(300))
+    k.register_C(300, np.zeros(300))
+    with pytest.raises(SmaxError) as e:
+        k.run()
+    assert e.value.code == expect
+    # the kernel object stays usable after the error
+    k.register_A(300, 300, len(col), *rand_crs(300, 10, 3)[1:2], rand_crs(300, 10, 3)[0], val)
+    smax.close()
+
+
+def test_operand_too_small_is_rejected():
+    from smaxkernels_b200 import FloatType, Interface, IntType, KernelType, PlatformType, SmaxError
+    rp, col, val = rand_crs(300, 10, 3)
+    smax = Interface()
+    smax.register_kernel("k", KernelType.SPMV, PlatformType.CUDA, IntType.INT32, FloatType.FLOAT64)
+    k = smax.kernel("k")
+    k.register_A(300, 300, len(col), col, rp, val)
+    k.register_B(300, np.ones(300))
+    k.register_C(299, np.zeros(299))
+    with pytest.raises(SmaxError):
+        k.run()
+    smax.close()
