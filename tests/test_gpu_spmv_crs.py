@@ -130,7 +130,14 @@ def test_malformed_matrix_is_an_error_status(poison):
         k.run()
     assert e.value.code == expect
     # the kernel object stays usable after the error
-    k.register_A(300, 300, len(col), *rand_crs(300, 10, 3)[1:2], rand_crs(300, 10, 3)[0], val)
+    rp2, col2, val2 = rand_crs(300, 10, 3)
+    x = np.ones(300)
+    y = np.zeros(300)
+    k.register_A(300, 300, len(col2), col2, rp2, val2)
+    k.register_B(300, x)
+    k.register_C(300, y)
+    k.run()
+    assert normwise(y, O.spmv_crs(rp2, col2, val2, x)) <= 1e-12
     smax.close()
 
 
