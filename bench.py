@@ -210,6 +210,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=N_ROWS, help="rows per rank (default 2^22)")
+    ap.add_argument("--variant", type=int, default=0, help="CRS kernel: 0 auto, 1 warp-stream, 2 row-tile")
     args = ap.parse_args()
     globals()["N_ROWS"] = args.rows
     if args.impl == "reference":
@@ -242,6 +243,8 @@ def main():
     smax = Interface()
     smax.register_kernel("spmv", KernelType.SPMV, PlatformType.CUDA, IntType.INT32, ft)
     k = smax.kernel("spmv")
+    if args.variant:
+        k.set_spmv_variant(args.variant)
     x_local = torch.from_numpy(np.random.default_rng(100 + rank).uniform(-1, 1, N_ROWS).astype(vt)).cuda()
     x_glob = torch.empty(n_cols, dtype=tdt, device="cuda")
     y = torch.empty(N_ROWS, dtype=tdt, device="cuda")
@@ -295,6 +298,8 @@ def main():
         if args.e2e_steps > 0:
             smax.register_kernel("spmv_host", KernelType.SPMV, PlatformType.CUDA, IntType.INT32, ft)
             ke = smax.kernel("spmv_host")
+            if args.variant:
+                ke.set_spmv_variant(args.variant)
             xh = torch.empty(n_cols, dtype=tdt).pin_memory()
             yh = torch.empty(N_ROWS, dtype=tdt).pin_memory()
             xh.copy_(x_glob.cpu())
@@ -349,13 +354,14 @@ def main():
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": f"{peak_kind} hbm_gbs",
                      "traffic": traffic, "algorithmic_bytes_per_launch": int(bytes_rank),
-                     "kernel": "crs_tile_kernel", "kernel_ms": round(t_kernel * 1e3, 5)},
+                     "kernel": "crs_tile_kernel" if args.variant == 2 else "crs_stream_kernel",
+                     "kernel_ms": round(t_kernel * 1e3, 5)},
         "cpu_baseline": cpu,
         "e2e": None if t_e2e is None else {
             "value": round(bytes_rank * world / t_e2e / 1e9, 3), "unit": UNIT,
             "h2d_bytes_per_step": int(n_cols * vbytes), "d2h_bytes_per_step": int(N_ROWS * vbytes),
             "ms_per_step": round(t_e2e * 1e3, 4)},
-        "gpu_launches": args.steps,  # one SpMV kernel per step (the all-gather is NCCL's)
+        "gpu_launches": args.steps * (1 if args.variant == 2 else 2),  # SpMV kernel (+ carry fix-up) per step
         "clocks": clocks,
     }
     if rank == 0:

@@ -87,6 +87,7 @@ typedef int smax_status;
 #define SMAX_FLAG_KERNEL_IMPL 7        /* set_kernel_implementation(SpMVType) */
 #define SMAX_FLAG_DEVICE_POINTERS 8    /* B and C registered as device pointers */
 #define SMAX_FLAG_A_DIRTY 9            /* re-upload A at the next initialize */
+#define SMAX_FLAG_SPMV_VARIANT 10      /* CRS SpMV kernel: 0 auto, 1 warp-stream, 2 row-tile */
 
 typedef struct smax_ctx_s *smax_ctx;
 typedef struct smax_kernel_s *smax_kernel;

@@ -55,15 +55,21 @@ void validate_crs(const DevCRS &m, DevStatus *st, cudaStream_t s) {
     SMAX_CUDA(cudaGetLastError());
 }
 
-void DevCRS::upload(const RegCRS &r, int vbytes, cudaStream_t st) {
+void DevCRS::upload(const RegCRS &r, int vbytes, cudaStream_t st, int64_t pad) {
     n_rows = (int64_t)r.n_rows;
     n_cols = (int64_t)r.n_cols;
     nnz = (int64_t)r.nnz;
-    if (r.n_rows >= (1ull << 31) || r.nnz >= (1ull << 31))
+    if (r.n_rows >= (1ull << 31) || r.nnz + (uint64_t)pad >= (1ull << 31))
         fail(SMAX_ERR_UNSUPPORTED, "int32 indices cannot address this matrix");
+    const int64_t cap = pad > 1 ? (nnz + pad - 1) / pad * pad : nnz;
     row_ptr.alloc(sizeof(int) * (r.n_rows + 1));
-    col.alloc(sizeof(int) * r.nnz);
-    val.alloc((size_t)vbytes * r.nnz);
+    col.alloc(sizeof(int) * cap);
+    val.alloc((size_t)vbytes * cap);
+    if (cap > nnz) {
+        SMAX_CUDA(cudaMemsetAsync(col.as<int>() + nnz, 0, sizeof(int) * (cap - nnz), st));
+        SMAX_CUDA(cudaMemsetAsync(static_cast<char *>(val.p) + (size_t)vbytes * nnz, 0,
+                                  (size_t)vbytes * (cap - nnz), st));
+    }
     SMAX_CUDA(cudaMemcpyAsync(row_ptr.p, r.row_ptr, sizeof(int) * (r.n_rows + 1), cudaMemcpyHostToDevice, st));
     if (r.nnz) {
         SMAX_CUDA(cudaMemcpyAsync(col.p, r.col, sizeof(int) * r.nnz, cudaMemcpyHostToDevice, st));
@@ -141,15 +147,29 @@ void spmv_initialize(smax_kernel_s *k) {
     require(k->A.set, SMAX_ERR_STATE, "register_A before initialize");
     require(!k->f_scs && !k->f_bcrs, SMAX_ERR_UNSUPPORTED, "SCS/BCRS SpMV not available in this build");
     if (k->a_dirty) {
-        k->dA.upload(k->A, k->vbytes, k->stream);
+        k->dA.upload(k->A, k->vbytes, k->stream, crs_stream_pad());
         validate_crs(k->dA, k->status.as<DevStatus>(), k->stream);
         read_status(k);
-        k->crs_plan.build(k->dA.rp(), k->dA.n_rows, crs_default_cap(k->vbytes * 8), k->stream);
+        k->crs_plan = CrsTilePlan();
+        k->crs_stream = CrsStreamPlan();
+        if (k->spmv_variant == 2)
+            k->crs_plan.build(k->dA.rp(), k->dA.n_rows, crs_default_cap(k->vbytes * 8), k->stream);
+        else
+            k->crs_stream.build(k->dA.rp(), k->dA.n_rows, k->dA.nnz, k->vbytes, k->stream);
         k->a_dirty = false;
     }
 }
 
 void spmv_apply(smax_kernel_s *k, const void *x, void *y) {
+    if (k->spmv_variant != 2) {
+        if (k->vbytes == 8)
+            crs_spmv_stream<double>(k->crs_stream, k->dA.ci(), k->dA.val.as<double>(),
+                                    static_cast<const double *>(x), static_cast<double *>(y), k->stream);
+        else
+            crs_spmv_stream<float>(k->crs_stream, k->dA.ci(), k->dA.val.as<float>(),
+                                   static_cast<const float *>(x), static_cast<float *>(y), k->stream);
+        return;
+    }
     if (k->vbytes == 8)
         crs_spmv<double>(k->crs_plan, k->dA.rp(), k->dA.ci(), k->dA.val.as<double>(),
                          static_cast<const double *>(x), static_cast<double *>(y), k->stream);
@@ -292,6 +312,11 @@ smax_status smax_kernel_set_flag(smax_kernel k, int flag, int value) {
         case SMAX_FLAG_KERNEL_IMPL: kk->impl = value; break;
         case SMAX_FLAG_DEVICE_POINTERS: kk->f_device = v; break;
         case SMAX_FLAG_A_DIRTY: kk->a_dirty = kk->a_dirty || v; break;
+        case SMAX_FLAG_SPMV_VARIANT:
+            require(value >= 0 && value <= 2, SMAX_ERR_BAD_ARG, "SpMV variant must be 0, 1 or 2");
+            if (value != kk->spmv_variant) kk->a_dirty = true;  // plans differ per variant
+            kk->spmv_variant = value;
+            break;
         default: fail(SMAX_ERR_BAD_ARG, "unknown flag");
         }
     });

@@ -42,7 +42,8 @@ struct RegDense {
 struct DevCRS {
     int64_t n_rows = 0, n_cols = 0, nnz = 0;
     DevBuf row_ptr, col, val;
-    void upload(const RegCRS &r, int vbytes, cudaStream_t st);
+    // pad: col/val are allocated and zero-filled up to a multiple of `pad` entries
+    void upload(const RegCRS &r, int vbytes, cudaStream_t st, int64_t pad = 1);
     const int *rp() const { return row_ptr.as<int>(); }
     const int *ci() const { return col.as<int>(); }
 };
@@ -79,6 +80,8 @@ struct smax_kernel_s {
     smax::DevCRS dA;
     smax::DevBuf dB, dC;
     smax::CrsTilePlan crs_plan;
+    smax::CrsStreamPlan crs_stream;
+    int spmv_variant = 0;  // 0 auto, 1 warp-stream, 2 row-tile
     smax::DevBuf status;  // smax::DevStatus
 
     // stopwatches

@@ -62,7 +62,8 @@ class SpMVType(enum.IntEnum):
 
 
 FLAG = dict(mat_perm=0, mat_upper_triang=1, mat_lower_triang=2, vec_row_major=3, mat_scs=4, mat_bcrs=5,
-            block_column_major=6, kernel_impl=7, device_pointers=8, a_dirty=9)
+            block_column_major=6, kernel_impl=7, device_pointers=8, a_dirty=9,
+            spmv_variant=10)
 
 
 def _is_torch_cuda(a) -> bool:
@@ -159,6 +160,10 @@ class Kernel:
 
     def set_kernel_implementation(self, impl):
         return self._flag("kernel_impl", int(impl))
+
+    def set_spmv_variant(self, v: int):
+        """CRS SpMV kernel: 0 auto, 1 warp-stream, 2 row-tile."""
+        return self._flag("spmv_variant", v)
 
     def mark_A_dirty(self):
         return self._flag("a_dirty", 1)

@@ -48,7 +48,7 @@ def rand_crs(n, maxlen, seed, vt=np.float64, n_cols=None, empty_frac=0.0, long_r
     return rp, col, val
 
 
-def gpu_spmv(row_ptr, col, val, x, n_cols=None):
+def gpu_spmv(row_ptr, col, val, x, n_cols=None, variant=0):
     from smaxkernels_b200 import FloatType, Interface, KernelType, PlatformType, IntType
     ft = FloatType.FLOAT32 if val.dtype == np.float32 else FloatType.FLOAT64
     n = len(row_ptr) - 1
@@ -56,6 +56,8 @@ def gpu_spmv(row_ptr, col, val, x, n_cols=None):
     smax = Interface()
     smax.register_kernel("k", KernelType.SPMV, PlatformType.CUDA, IntType.INT32, ft)
     k = smax.kernel("k")
+    if variant:
+        k.set_spmv_variant(variant)
     k.register_A(n, n_cols or len(x), len(col), col, row_ptr, val)
     k.register_B(len(x), np.ascontiguousarray(x, dtype=val.dtype))
     k.register_C(n, y)

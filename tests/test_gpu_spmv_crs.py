@@ -17,27 +17,29 @@ def test_golden_spmv_test():
     assert G.almost_equal(y, c["y"], np.float64)
 
 
+@pytest.mark.parametrize("variant", [1, 2])
 @pytest.mark.parametrize("vt", [np.float64, np.float32])
-@pytest.mark.parametrize("case", ["small", "empty_rows", "long_rows", "single_row", "ragged"])
-def test_random_vs_oracle(vt, case):
+@pytest.mark.parametrize("case", ["small", "empty_rows", "long_rows", "single_row", "ragged", "mostly_empty"])
+def test_random_vs_oracle(vt, case, variant):
     kw = dict(small=dict(n=257, maxlen=9), empty_rows=dict(n=3001, maxlen=40, empty_frac=0.5),
               long_rows=dict(n=5000, maxlen=20, long_rows=(1025, 2049, 4097, 4999)),
               single_row=dict(n=1, maxlen=1, n_cols=7000, long_rows=(6000,)),
-              ragged=dict(n=20011, maxlen=300))[case]
+              ragged=dict(n=20011, maxlen=300), mostly_empty=dict(n=4099, maxlen=3, empty_frac=0.95))[case]
     n_cols = kw.pop("n_cols", None)
     rp, col, val = rand_crs(seed=11, vt=vt, n_cols=n_cols, **kw)
     x = np.random.default_rng(12).uniform(-1, 1, n_cols or len(rp) - 1).astype(vt)
-    y = gpu_spmv(rp, col, val, x)
+    y = gpu_spmv(rp, col, val, x, variant=variant)
     y_ref = O.spmv_crs(rp, col, val, x)  # reference arithmetic in VT
     assert normwise(y, y_ref) <= tol(vt)
     y64 = O.spmv_crs(rp, col, val.astype(np.float64), x.astype(np.float64))
     assert normwise(y, y64) <= tol(vt)
 
 
-def test_all_rows_empty():
+@pytest.mark.parametrize("variant", [1, 2])
+def test_all_rows_empty(variant):
     n = 1000
     rp = np.zeros(n + 1, np.int32)
-    y = gpu_spmv(rp, np.zeros(0, np.int32), np.zeros(0), np.ones(n))
+    y = gpu_spmv(rp, np.zeros(0, np.int32), np.zeros(0), np.ones(n), variant=variant)
     assert np.all(y == 0)
 
 
@@ -50,12 +52,13 @@ def test_config0_laplace64():
 
 
 @pytest.mark.slow
+@pytest.mark.parametrize("variant", [1, 2])
 @pytest.mark.parametrize("vt", [np.float64, np.float32])
-def test_config1_lognormal_full_size(vt):
+def test_config1_lognormal_full_size(vt, variant):
     from smaxkernels_b200 import matrices as M
     rp, col, val = M.lognormal_random(1 << 22, dtype=vt)
     x = M.uniform_vector(len(rp) - 1, 1, dtype=vt)
-    y = gpu_spmv(rp, col, val, x)
+    y = gpu_spmv(rp, col, val, x, variant=variant)
     assert normwise(y, O.spmv_crs(rp, col, val, x)) <= tol(vt)
     y64 = O.spmv_crs(rp, col, val.astype(np.float64), x.astype(np.float64))
     assert normwise(y, y64) <= tol(vt)
