@@ -193,8 +193,7 @@ def run_reference(args):
 
 
 def config_dict(nnz, vbytes, world):
-    size = "2^22" if N_ROWS == 1 << 22 else str(N_ROWS)
-    return {"workload": f"crs_spmv_{'f64' if vbytes == 8 else 'f32'}_lognormal_{size}",
+    return {"workload": f"crs_spmv_{'f64' if vbytes == 8 else 'f32'}_lognormal_{N_ROWS}",
             "format": "CRS", "index": "int32", "n_rows_per_rank": N_ROWS, "n_cols": N_ROWS * world,
             "nnz_rank0": int(nnz), "row_length": "lognormal(mean 16, sigma 1.0), clip [1,4096]",
             "l2": "inputs larger than L2 (no flush)", "parallelism": f"row blocks x {world} ranks"}
