@@ -149,6 +149,27 @@ void *smax_kernel_stream(smax_kernel k);
  * The caller keeps ownership of the stream. */
 smax_status smax_kernel_set_stream(smax_kernel k, void *stream);
 
+/* ------------------------------------------------- allocation-free SpMV */
+/* CRS SpMV y = A*x for callers that cannot allocate device memory (an
+ * application whose pool already owns the GPU, a plugin whose host forbids
+ * device allocations, a loop that must not enter the allocator).  No
+ * counterpart exists in the reference.  All arrays are the caller's DEVICE
+ * arrays (int32 row_ptr/col, float32 or float64 val/x/y); the call allocates
+ * nothing and keeps its working data in one fixed scratch area of
+ * SMAX_NOALLOC_SCRATCH_BYTES per GPU, held from library load until exit.
+ * Limits: n_rows <= SMAX_NOALLOC_MAX_ROWS and nnz <= SMAX_NOALLOC_MAX_NNZ, else
+ * SMAX_ERR_BAD_ARG.  Calls share the scratch area: calls that overlap on the
+ * GPU race, so issue them on one stream or serialise them.  The first call on
+ * a device looks up the scratch address; make it before any stream capture.
+ * The call validates the matrix (SMAX_ERR_COL_OOB / SMAX_ERR_BAD_ARG) and
+ * synchronises `stream` (a cudaStream_t; NULL = legacy default stream). */
+#define SMAX_NOALLOC_MAX_ROWS (1 << 20)
+#define SMAX_NOALLOC_MAX_NNZ (1 << 24)
+#define SMAX_NOALLOC_SCRATCH_BYTES (7u << 20)
+smax_status smax_spmv_crs_noalloc(int float_type, uint64_t n_rows, uint64_t n_cols, uint64_t nnz,
+                                  const void *d_row_ptr, const void *d_col, const void *d_val, const void *d_x,
+                                  void *d_y, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

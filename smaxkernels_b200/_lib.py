@@ -44,6 +44,7 @@ SIGNATURES = {
     "smax_kernel_get_timer": (I32, [P, C.c_char_p, C.POINTER(C.c_double)]),
     "smax_kernel_stream": (P, [P]),
     "smax_kernel_set_stream": (I32, [P, P]),
+    "smax_spmv_crs_noalloc": (I32, [I32, U64, U64, U64, P, P, P, P, P, P]),
 }
 
 for _name, (_res, _args) in SIGNATURES.items():
