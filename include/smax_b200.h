@@ -118,6 +118,23 @@ smax_status smax_kernel_set_flag(smax_kernel k, int flag, int value);
 smax_status smax_kernel_register_A_crs(smax_kernel k, uint64_t n_rows, uint64_t n_cols, uint64_t nnz,
                                        void *col, void *row_ptr, void *val);
 
+/* register_A for a SELL-C-sigma matrix (with SMAX_FLAG_MAT_SCS), the 13
+ * arguments of src/kernels/spmv.hpp:25-53: C, sigma, n_rows, n_rows_padded,
+ * n_cols, n_chunks, n_elements, nnz, chunk_ptr, chunk_lengths, col, val, perm.
+ * y is produced in the permuted row order, of length n_rows_padded. */
+smax_status smax_kernel_register_A_scs(smax_kernel k, uint64_t C, uint64_t sigma, uint64_t n_rows,
+                                       uint64_t n_rows_padded, uint64_t n_cols, uint64_t n_chunks,
+                                       uint64_t n_elements, uint64_t nnz, void *chunk_ptr, void *chunk_lengths,
+                                       void *col, void *val, void *perm);
+
+/* register_A for a BCRS matrix (with SMAX_FLAG_MAT_BCRS), the 10 arguments of
+ * src/kernels/spmv.hpp:54-76: block rows, block columns, blocks, block height
+ * and width, height and width padding, col, row_ptr, val.  The in-block order
+ * follows SMAX_FLAG_BLOCK_COLUMN_MAJOR. */
+smax_status smax_kernel_register_A_bcrs(smax_kernel k, uint64_t n_rows, uint64_t n_cols, uint64_t n_blocks,
+                                        uint64_t b_height, uint64_t b_width, uint64_t height_pad,
+                                        uint64_t width_pad, void *col, void *row_ptr, void *val);
+
 /* register_B / register_C of a dense operand: (n_rows, val) for vectors
  * (spmv.hpp:97-115, sptrsv.hpp:40-58) or (n_rows, n_cols, val) for blocks of
  * vectors (spmm.hpp:40-61, sptrsm.hpp:40-60).  slot 1 = B, slot 2 = C. */
@@ -148,6 +165,29 @@ void *smax_kernel_stream(smax_kernel k);
  * current stream of a framework) instead of its own; NULL restores its own.
  * The caller keeps ownership of the stream. */
 smax_status smax_kernel_set_stream(smax_kernel k, void *stream);
+
+/* ------------------------------------------------------------------ utils */
+/* Utils::convert_crs_to_scs (src/utils/convert_formats.hpp:16-132), computed on
+ * the GPU.  meta[6] receives n_rows, n_rows_padded, n_cols, n_chunks,
+ * n_elements, nnz; the five arrays are allocated with new[] (release with
+ * delete[] or smax_free_host).  Rows of equal length inside a sigma window are
+ * ordered by ascending row index. */
+smax_status smax_utils_convert_crs_to_scs(int int_type, int float_type, uint64_t n_rows, uint64_t n_cols,
+                                          uint64_t nnz, const void *col, const void *row_ptr, const void *val,
+                                          uint64_t C, uint64_t sigma, uint64_t *meta, void **chunk_ptr,
+                                          void **chunk_lengths, void **col_out, void **val_out, void **perm);
+
+/* Utils::convert_crs_to_bcrs (src/utils/convert_formats.hpp:134-247), computed
+ * on the GPU.  meta[7] receives n_rows, n_cols, n_blocks, b_height, b_width,
+ * height_pad, width_pad (in blocks); arrays as above. */
+smax_status smax_utils_convert_crs_to_bcrs(int int_type, int float_type, uint64_t n_rows, uint64_t n_cols,
+                                           uint64_t nnz, const void *col, const void *row_ptr, const void *val,
+                                           uint64_t b_height, uint64_t b_width, uint64_t height_pad,
+                                           uint64_t width_pad, int block_column_major, uint64_t *meta,
+                                           void **col_out, void **row_ptr_out, void **val_out);
+
+/* Releases an array returned by an smax_utils_* function. */
+void smax_free_host(void *p);
 
 /* ------------------------------------------------- allocation-free SpMV */
 /* CRS SpMV y = A*x for callers that cannot allocate device memory (an

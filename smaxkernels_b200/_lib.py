@@ -35,6 +35,8 @@ SIGNATURES = {
     "smax_kernel_destroy": (I32, [P]),
     "smax_kernel_set_flag": (I32, [P, I32, I32]),
     "smax_kernel_register_A_crs": (I32, [P, U64, U64, U64, P, P, P]),
+    "smax_kernel_register_A_scs": (I32, [P] + [U64] * 8 + [P] * 5),
+    "smax_kernel_register_A_bcrs": (I32, [P] + [U64] * 7 + [P] * 3),
     "smax_kernel_register_dense": (I32, [P, I32, U64, U64, P]),
     "smax_kernel_initialize": (I32, [P, U64, U64, U64]),
     "smax_kernel_apply": (I32, [P, U64, U64, U64]),
@@ -44,6 +46,10 @@ SIGNATURES = {
     "smax_kernel_get_timer": (I32, [P, C.c_char_p, C.POINTER(C.c_double)]),
     "smax_kernel_stream": (P, [P]),
     "smax_kernel_set_stream": (I32, [P, P]),
+    "smax_utils_convert_crs_to_scs": (I32, [I32, I32, U64, U64, U64, P, P, P, U64, U64, PU64] + [PP] * 5),
+    "smax_utils_convert_crs_to_bcrs": (I32, [I32, I32, U64, U64, U64, P, P, P, U64, U64, U64, U64, I32, PU64]
+                                       + [PP] * 3),
+    "smax_free_host": (None, [P]),
     "smax_spmv_crs_noalloc": (I32, [I32, U64, U64, U64, P, P, P, P, P, P]),
 }
 

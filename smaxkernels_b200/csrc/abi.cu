@@ -1,114 +1,11 @@
-// abi.cu -- exported C functions of include/smax_b200.h: contexts, kernel
+// abi.cu -- exported C functions of include/smax_b200.h for contexts, kernel
 // objects, registration and the initialize / apply / finalize cycle.
-#include <chrono>
+//
+// Dispatch mirrors the reference's L2 kernel fronts (src/kernels/spmv.hpp:138-195,
+// spmm.hpp:68-100): the kernel type and the flags pick the format and kernel.
 #include <cstring>
 
 #include "kernel_obj.cuh"
-
-namespace smax {
-
-namespace {
-thread_local std::string g_last_error;
-
-double wall_s() {
-    using clk = std::chrono::steady_clock;
-    return std::chrono::duration<double>(clk::now().time_since_epoch()).count();
-}
-}  // namespace
-
-void set_last_error(const std::string &m) { g_last_error = m; }
-const char *last_error() { return g_last_error.c_str(); }
-
-int sm_count() {
-    static int cached[64] = {0};
-    int dev = 0;
-    SMAX_CUDA(cudaGetDevice(&dev));
-    if (dev < 64 && cached[dev]) return cached[dev];
-    int n = 0;
-    SMAX_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
-    if (dev < 64) cached[dev] = n;
-    return n;
-}
-
-namespace {
-// One pass over an uploaded CRS matrix: row_ptr[0] == 0, row_ptr[n] == nnz,
-// row_ptr non-decreasing, every column in [0, n_cols).  Hot kernels trust the
-// matrix afterwards, so malformed input becomes an error status here instead
-// of an out-of-bounds access later.
-__global__ void validate_crs_kernel(const int *__restrict__ row_ptr, const int *__restrict__ col, int64_t n,
-                                    int64_t nnz, int64_t n_cols, DevStatus *st) {
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t == 0 && (row_ptr[0] != 0 || row_ptr[n] != nnz)) report(st, SMAX_ERR_BAD_ARG, 0);
-    for (int64_t r = t; r < n; r += stride)
-        if (row_ptr[r + 1] < row_ptr[r]) report(st, SMAX_ERR_BAD_ARG, r);
-    for (int64_t j = t; j < nnz; j += stride) {
-        int c = col[j];
-        if (c < 0 || c >= n_cols) report(st, SMAX_ERR_COL_OOB, j);
-    }
-}
-}  // namespace
-
-void validate_crs(const DevCRS &m, DevStatus *st, cudaStream_t s) {
-    int blocks = 4 * sm_count();
-    validate_crs_kernel<<<blocks, 256, 0, s>>>(m.rp(), m.ci(), m.n_rows, m.nnz, m.n_cols, st);
-    SMAX_CUDA(cudaGetLastError());
-}
-
-void DevCRS::upload(const RegCRS &r, int vbytes, cudaStream_t st, int64_t pad) {
-    n_rows = (int64_t)r.n_rows;
-    n_cols = (int64_t)r.n_cols;
-    nnz = (int64_t)r.nnz;
-    if (r.n_rows >= (1ull << 31) || r.nnz + (uint64_t)pad >= (1ull << 31))
-        fail(SMAX_ERR_UNSUPPORTED, "int32 indices cannot address this matrix");
-    const int64_t cap = pad > 1 ? (nnz + pad - 1) / pad * pad : nnz;
-    row_ptr.alloc(sizeof(int) * (r.n_rows + 1));
-    col.alloc(sizeof(int) * cap);
-    val.alloc((size_t)vbytes * cap);
-    if (cap > nnz) {
-        SMAX_CUDA(cudaMemsetAsync(col.as<int>() + nnz, 0, sizeof(int) * (cap - nnz), st));
-        SMAX_CUDA(cudaMemsetAsync(static_cast<char *>(val.p) + (size_t)vbytes * nnz, 0,
-                                  (size_t)vbytes * (cap - nnz), st));
-    }
-    SMAX_CUDA(cudaMemcpyAsync(row_ptr.p, r.row_ptr, sizeof(int) * (r.n_rows + 1), cudaMemcpyHostToDevice, st));
-    if (r.nnz) {
-        SMAX_CUDA(cudaMemcpyAsync(col.p, r.col, sizeof(int) * r.nnz, cudaMemcpyHostToDevice, st));
-        SMAX_CUDA(cudaMemcpyAsync(val.p, r.val, (size_t)vbytes * r.nnz, cudaMemcpyHostToDevice, st));
-    }
-}
-
-std::pair<cudaEvent_t, cudaEvent_t> PendingEvents::acquire() {
-    std::pair<cudaEvent_t, cudaEvent_t> p;
-    if (!spare.empty()) {
-        p = spare.back();
-        spare.pop_back();
-    } else {
-        SMAX_CUDA(cudaEventCreate(&p.first));
-        SMAX_CUDA(cudaEventCreate(&p.second));
-    }
-    live.push_back(p);
-    return p;
-}
-
-double PendingEvents::drain() {
-    double s = 0.0;
-    for (auto &p : live) {
-        SMAX_CUDA(cudaEventSynchronize(p.second));
-        float ms = 0.f;
-        SMAX_CUDA(cudaEventElapsedTime(&ms, p.first, p.second));
-        s += ms * 1e-3;
-        spare.push_back(p);
-    }
-    live.clear();
-    return s;
-}
-
-PendingEvents::~PendingEvents() {
-    for (auto &p : live) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
-    for (auto &p : spare) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
-}
-
-}  // namespace smax
 
 smax_kernel_s::~smax_kernel_s() {
     if (stream) cudaStreamSynchronize(stream);
@@ -123,8 +20,6 @@ void require(bool c, int code, const char *msg) {
     if (!c) fail(code, msg);
 }
 
-void read_status(smax_kernel_s *k);
-
 smax_kernel_s *K(smax_kernel k) {
     require(k != nullptr, SMAX_ERR_BAD_ARG, "null kernel handle");
     return k;
@@ -137,45 +32,110 @@ void read_status(smax_kernel_s *k) {
     SMAX_CUDA(cudaStreamSynchronize(k->stream));
     if (st.code != 0) {
         SMAX_CUDA(cudaMemsetAsync(k->status.p, 0, sizeof(DevStatus), k->stream));
-        fail(st.code, "device reported error " + std::to_string(st.code) + " at index " +
-                          std::to_string(st.index));
+        SMAX_CUDA(cudaStreamSynchronize(k->stream));
+        fail(st.code, "device reported error " + std::to_string(st.code) + " at index " + std::to_string(st.index));
     }
 }
 
+DevStatus *dstatus(smax_kernel_s *k) { return k->status.as<DevStatus>(); }
+
+template <typename T> T *up(DevBuf &d, const void *h, uint64_t n, cudaStream_t st) {
+    d.alloc(sizeof(T) * (n ? n : 1));
+    if (n) SMAX_CUDA(cudaMemcpyAsync(d.p, h, sizeof(T) * n, cudaMemcpyHostToDevice, st));
+    return d.as<T>();
+}
+
 // ------------------------------------------------------------------ SpMV --
-void spmv_initialize(smax_kernel_s *k) {
-    require(k->A.set, SMAX_ERR_STATE, "register_A before initialize");
-    require(!k->f_scs && !k->f_bcrs, SMAX_ERR_UNSUPPORTED, "SCS/BCRS SpMV not available in this build");
-    if (k->a_dirty) {
-        k->dA.upload(k->A, k->vbytes, k->stream, crs_stream_pad());
-        validate_crs(k->dA, k->status.as<DevStatus>(), k->stream);
+void spmv_upload(smax_kernel_s *k) {
+    cudaStream_t st = k->stream;
+    if (k->f_scs) {
+        const RegSCS &r = k->A_scs;
+        require(r.set, SMAX_ERR_STATE, "register_A (SELL-C-sigma) before initialize");
+        require(r.C > 0 && r.n_chunks * r.C == r.n_rows_padded && r.n_rows <= r.n_rows_padded, SMAX_ERR_BAD_ARG,
+                "inconsistent SELL-C-sigma sizes");
+        require(r.n_elements < (1ull << 31) && r.n_cols < (1ull << 31), SMAX_ERR_UNSUPPORTED,
+                "int32 indices cannot address this matrix");
+        DevSCS &d = k->dS;
+        d.C = r.C; d.sigma = r.sigma; d.n_rows = r.n_rows; d.n_rows_padded = r.n_rows_padded;
+        d.n_cols = r.n_cols; d.n_chunks = r.n_chunks; d.n_elements = r.n_elements; d.nnz = r.nnz;
+        up<int>(d.chunk_ptr, r.chunk_ptr, r.n_chunks + 1, st);
+        up<int>(d.chunk_len, r.chunk_lengths, r.n_chunks, st);
+        up<int>(d.col, r.col, r.n_elements, st);
+        d.val.alloc((size_t)k->vbytes * (r.n_elements ? r.n_elements : 1));
+        if (r.n_elements)
+            SMAX_CUDA(cudaMemcpyAsync(d.val.p, r.val, (size_t)k->vbytes * r.n_elements, cudaMemcpyHostToDevice, st));
+        validate_scs(d, dstatus(k), st);
+        read_status(k);
+    } else if (k->f_bcrs) {
+        const RegBCRS &r = k->A_bcrs;
+        require(r.set, SMAX_ERR_STATE, "register_A (BCRS) before initialize");
+        require(r.hpad >= r.bh && r.wpad >= r.bw && r.hpad > 0 && r.wpad > 0, SMAX_ERR_BAD_ARG,
+                "block paddings must be at least the block sizes");
+        require(r.n_blocks < (1ull << 31) && r.n_rows < (1ull << 31), SMAX_ERR_UNSUPPORTED,
+                "int32 indices cannot address this matrix");
+        DevBCRS &d = k->dBc;
+        d.n_rows = r.n_rows; d.n_cols = r.n_cols; d.n_blocks = r.n_blocks; d.bh = r.bh; d.bw = r.bw;
+        d.hpad = r.hpad; d.wpad = r.wpad;
+        up<int>(d.row_ptr, r.row_ptr, r.n_rows + 1, st);
+        up<int>(d.col, r.col, r.n_blocks, st);
+        const uint64_t nv = r.n_blocks * r.hpad * r.wpad;
+        d.val.alloc((size_t)k->vbytes * (nv ? nv : 1));
+        if (nv) SMAX_CUDA(cudaMemcpyAsync(d.val.p, r.val, (size_t)k->vbytes * nv, cudaMemcpyHostToDevice, st));
+        validate_bcrs(d, dstatus(k), st);
+        read_status(k);
+    } else {
+        require(k->A.set, SMAX_ERR_STATE, "register_A before initialize");
+        upload_crs(k->dA, k->A, k->vbytes, st, crs_stream_pad());
+        validate_crs(k->dA, dstatus(k), st);
         read_status(k);
         k->crs_plan = CrsTilePlan();
         k->crs_stream = CrsStreamPlan();
         if (k->spmv_variant == 2)
-            k->crs_plan.build(k->dA.rp(), k->dA.n_rows, crs_default_cap(k->vbytes * 8), k->stream);
+            k->crs_plan.build(k->dA.rp(), k->dA.n_rows, crs_default_cap(k->vbytes * 8), st);
         else
-            k->crs_stream.build(k->dA.rp(), k->dA.n_rows, k->dA.nnz, k->vbytes, k->stream);
-        k->a_dirty = false;
+            k->crs_stream.build(k->dA.rp(), k->dA.n_rows, k->dA.nnz, k->vbytes, st);
     }
 }
 
-void spmv_apply(smax_kernel_s *k, const void *x, void *y) {
-    if (k->spmv_variant != 2) {
-        if (k->vbytes == 8)
-            crs_spmv_stream<double>(k->crs_stream, k->dA.ci(), k->dA.val.as<double>(),
-                                    static_cast<const double *>(x), static_cast<double *>(y), k->stream);
-        else
-            crs_spmv_stream<float>(k->crs_stream, k->dA.ci(), k->dA.val.as<float>(),
-                                   static_cast<const float *>(x), static_cast<float *>(y), k->stream);
-        return;
-    }
-    if (k->vbytes == 8)
-        crs_spmv<double>(k->crs_plan, k->dA.rp(), k->dA.ci(), k->dA.val.as<double>(),
-                         static_cast<const double *>(x), static_cast<double *>(y), k->stream);
+template <typename VT> void crs_spmv_any(smax_kernel_s *k, const VT *x, VT *y) {
+    if (k->spmv_variant == 2)
+        crs_spmv<VT>(k->crs_plan, k->dA.rp(), k->dA.ci(), k->dA.val.as<VT>(), x, y, k->stream);
     else
-        crs_spmv<float>(k->crs_plan, k->dA.rp(), k->dA.ci(), k->dA.val.as<float>(),
-                        static_cast<const float *>(x), static_cast<float *>(y), k->stream);
+        crs_spmv_stream<VT>(k->crs_stream, k->dA.ci(), k->dA.val.as<VT>(), x, y, k->stream);
+}
+
+template <typename VT> void spmv_apply_t(smax_kernel_s *k, const VT *x, VT *y) {
+    if (k->f_scs) {
+        scs_spmv<VT>(k->dS, x, y, k->stream);
+    } else if (k->f_bcrs) {
+        k->dBc.col_major = k->f_block_col_major;
+        bcrs_spmv<VT>(k->dBc, x, y, k->stream);
+    } else {
+        crs_spmv_any<VT>(k, x, y);
+    }
+}
+
+// ------------------------------------------------------------------ SpMM --
+void spmm_upload(smax_kernel_s *k) {
+    require(k->A.set, SMAX_ERR_STATE, "register_A before initialize");
+    upload_crs(k->dA, k->A, k->vbytes, k->stream, crs_stream_pad());
+    validate_crs(k->dA, dstatus(k), k->stream);
+    read_status(k);
+    k->crs_stream = CrsStreamPlan();
+    if (!k->f_row_major) k->crs_stream.build(k->dA.rp(), k->dA.n_rows, k->dA.nnz, k->vbytes, k->stream);
+}
+
+template <typename VT> void spmm_apply_t(smax_kernel_s *k, const VT *X, VT *Y) {
+    const int64_t kk = (int64_t)(k->B.n_cols ? k->B.n_cols : 1);
+    if (k->f_row_major) {
+        crs_spmm_row_major<VT>(k->dA, kk, X, Y, k->stream);
+    } else {
+        // column-major: the reference uses A's n_rows as the leading dimension
+        // of both X and Y (src/kernels/spmm/spmm_cpu/spmm_cpu_crs_impl.hpp:29,44)
+        const int64_t ld = k->dA.n_rows;
+        for (int64_t v = 0; v < kk; ++v)
+            crs_spmv_stream<VT>(k->crs_stream, k->dA.ci(), k->dA.val.as<VT>(), X + v * ld, Y + v * ld, k->stream);
+    }
 }
 
 // Device addresses of B and C (+ element offsets).
@@ -188,12 +148,38 @@ void *dev_c(smax_kernel_s *k, uint64_t off) {
     return base + off * k->vbytes;
 }
 
+// Operand extents the kernel reads (B) and writes (C), in elements.
+void check_extents(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
+    uint64_t need_b = 0, need_c = 0;
+    switch (k->ktype) {
+    case SMAX_KERNEL_SPMV:
+        if (k->f_scs) { need_b = k->A_scs.n_cols; need_c = k->A_scs.n_rows_padded; }
+        else if (k->f_bcrs) { need_b = k->A_bcrs.n_cols * k->A_bcrs.wpad; need_c = k->A_bcrs.n_rows * k->A_bcrs.hpad; }
+        else { need_b = k->A.n_cols; need_c = k->A.n_rows; }
+        break;
+    case SMAX_KERNEL_SPMM: {
+        const uint64_t kk = k->B.n_cols ? k->B.n_cols : 1;
+        require(k->C.n_cols == k->B.n_cols, SMAX_ERR_BAD_ARG, "X and Y must have the same number of vectors");
+        if (k->f_row_major) { need_b = k->A.n_cols * kk; need_c = k->A.n_rows * kk; }
+        else { need_b = (kk - 1) * k->A.n_rows + k->A.n_cols; need_c = k->A.n_rows * kk; }
+        break;
+    }
+    default: break;
+    }
+    require(b_off + need_b <= k->B.elems(), SMAX_ERR_BAD_ARG, "B (with offset) is smaller than the operator needs");
+    require(c_off + need_c <= k->C.elems(), SMAX_ERR_BAD_ARG, "C (with offset) is smaller than the operator needs");
+}
+
 void do_initialize(smax_kernel_s *k) {
     double t0 = wall_s();
     require(k->B.set && k->C.set, SMAX_ERR_STATE, "register_B and register_C before initialize");
-    switch (k->ktype) {
-    case SMAX_KERNEL_SPMV: spmv_initialize(k); break;
-    default: fail(SMAX_ERR_UNSUPPORTED, "kernel type not available in this build");
+    if (k->a_dirty) {
+        switch (k->ktype) {
+        case SMAX_KERNEL_SPMV: spmv_upload(k); break;
+        case SMAX_KERNEL_SPMM: spmm_upload(k); break;
+        default: fail(SMAX_ERR_UNSUPPORTED, "kernel type not available in this build");
+        }
+        k->a_dirty = false;
     }
     if (!k->f_device) {
         size_t bb = (size_t)k->B.elems() * k->vbytes, cb = (size_t)k->C.elems() * k->vbytes;
@@ -205,24 +191,23 @@ void do_initialize(smax_kernel_s *k) {
     k->timers["initialize"] += wall_s() - t0;
 }
 
-// Operand extents the kernel reads (B) and writes (C), in elements.
-void check_extents(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
-    uint64_t need_b = 0, need_c = 0;
-    switch (k->ktype) {
-    case SMAX_KERNEL_SPMV: need_b = k->A.n_cols; need_c = k->A.n_rows; break;
-    default: break;
-    }
-    require(b_off + need_b <= k->B.elems(), SMAX_ERR_BAD_ARG, "B (with offset) is smaller than the operator needs");
-    require(c_off + need_c <= k->C.elems(), SMAX_ERR_BAD_ARG, "C (with offset) is smaller than the operator needs");
-}
-
 void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
     require(!k->a_dirty, SMAX_ERR_STATE, "initialize before apply");
     check_extents(k, b_off, c_off);
     auto ev = k->apply_events.acquire();
     SMAX_CUDA(cudaEventRecord(ev.first, k->stream));
+    const void *b = dev_b(k, b_off);
+    void *c = dev_c(k, c_off);
+    const bool f64 = k->vbytes == 8;
     switch (k->ktype) {
-    case SMAX_KERNEL_SPMV: spmv_apply(k, dev_b(k, b_off), dev_c(k, c_off)); break;
+    case SMAX_KERNEL_SPMV:
+        if (f64) spmv_apply_t<double>(k, static_cast<const double *>(b), static_cast<double *>(c));
+        else spmv_apply_t<float>(k, static_cast<const float *>(b), static_cast<float *>(c));
+        break;
+    case SMAX_KERNEL_SPMM:
+        if (f64) spmm_apply_t<double>(k, static_cast<const double *>(b), static_cast<double *>(c));
+        else spmm_apply_t<float>(k, static_cast<const float *>(b), static_cast<float *>(c));
+        break;
     default: fail(SMAX_ERR_UNSUPPORTED, "kernel type not available in this build");
     }
     SMAX_CUDA(cudaEventRecord(ev.second, k->stream));
@@ -305,9 +290,18 @@ smax_status smax_kernel_set_flag(smax_kernel k, int flag, int value) {
         case SMAX_FLAG_MAT_PERM: kk->f_perm = v; break;
         case SMAX_FLAG_MAT_UPPER_TRIANG: kk->f_upper = v; break;
         case SMAX_FLAG_MAT_LOWER_TRIANG: kk->f_lower = v; break;
-        case SMAX_FLAG_VEC_ROW_MAJOR: kk->f_row_major = v; break;
-        case SMAX_FLAG_MAT_SCS: kk->f_scs = v; break;
-        case SMAX_FLAG_MAT_BCRS: kk->f_bcrs = v; break;
+        case SMAX_FLAG_VEC_ROW_MAJOR:
+            if (v != kk->f_row_major) kk->a_dirty = true;
+            kk->f_row_major = v;
+            break;
+        case SMAX_FLAG_MAT_SCS:
+            if (v != kk->f_scs) kk->a_dirty = true;
+            kk->f_scs = v;
+            break;
+        case SMAX_FLAG_MAT_BCRS:
+            if (v != kk->f_bcrs) kk->a_dirty = true;
+            kk->f_bcrs = v;
+            break;
         case SMAX_FLAG_BLOCK_COLUMN_MAJOR: kk->f_block_col_major = v; break;
         case SMAX_FLAG_KERNEL_IMPL: kk->impl = value; break;
         case SMAX_FLAG_DEVICE_POINTERS: kk->f_device = v; break;
@@ -329,6 +323,33 @@ smax_status smax_kernel_register_A_crs(smax_kernel k, uint64_t n_rows, uint64_t 
         require(row_ptr != nullptr, SMAX_ERR_BAD_ARG, "null row_ptr");
         require(nnz == 0 || (col && val), SMAX_ERR_BAD_ARG, "null col/val");
         kk->A = RegCRS{true, n_rows, n_cols, nnz, col, row_ptr, val};
+        kk->a_dirty = true;
+    });
+}
+
+smax_status smax_kernel_register_A_scs(smax_kernel k, uint64_t C, uint64_t sigma, uint64_t n_rows,
+                                       uint64_t n_rows_padded, uint64_t n_cols, uint64_t n_chunks,
+                                       uint64_t n_elements, uint64_t nnz, void *chunk_ptr, void *chunk_lengths,
+                                       void *col, void *val, void *perm) {
+    return guarded([&] {
+        smax_kernel_s *kk = K(k);
+        require(chunk_ptr && chunk_lengths, SMAX_ERR_BAD_ARG, "null chunk_ptr/chunk_lengths");
+        require(n_elements == 0 || (col && val), SMAX_ERR_BAD_ARG, "null col/val");
+        kk->A_scs = RegSCS{true, C, sigma, n_rows, n_rows_padded, n_cols, n_chunks, n_elements, nnz,
+                           chunk_ptr, chunk_lengths, col, val, perm};
+        kk->a_dirty = true;
+    });
+}
+
+smax_status smax_kernel_register_A_bcrs(smax_kernel k, uint64_t n_rows, uint64_t n_cols, uint64_t n_blocks,
+                                        uint64_t b_height, uint64_t b_width, uint64_t height_pad,
+                                        uint64_t width_pad, void *col, void *row_ptr, void *val) {
+    return guarded([&] {
+        smax_kernel_s *kk = K(k);
+        require(row_ptr != nullptr, SMAX_ERR_BAD_ARG, "null row_ptr");
+        require(n_blocks == 0 || (col && val), SMAX_ERR_BAD_ARG, "null col/val");
+        kk->A_bcrs = RegBCRS{true, n_rows, n_cols, n_blocks, b_height, b_width, height_pad, width_pad,
+                             col, row_ptr, val};
         kk->a_dirty = true;
     });
 }

@@ -4,7 +4,7 @@
 // (KernelContext, Args, Flags, Timers: src/kernel.hpp:7-127,
 // src/kernels/<k>/<k>_common.hpp) plus this platform's device-resident state:
 // the matrix is uploaded once and kept in HBM across run() calls, and every
-// launch goes to the kernel's own stream.
+// launch goes to the kernel's stream.
 #pragma once
 
 #include <map>
@@ -14,6 +14,7 @@
 
 #include "common.cuh"
 #include "spmv_crs.cuh"
+#include "spmv_formats.cuh"
 
 struct smax_ctx_s {
     // UtilitiesContainer (src/common.hpp:187-195): written by generate_perm,
@@ -31,6 +32,20 @@ struct RegCRS {
     void *col = nullptr, *row_ptr = nullptr, *val = nullptr;
 };
 
+// register_A with 13 SELL-C-sigma arguments (src/kernels/spmv.hpp:25-53)
+struct RegSCS {
+    bool set = false;
+    uint64_t C = 0, sigma = 0, n_rows = 0, n_rows_padded = 0, n_cols = 0, n_chunks = 0, n_elements = 0, nnz = 0;
+    void *chunk_ptr = nullptr, *chunk_lengths = nullptr, *col = nullptr, *val = nullptr, *perm = nullptr;
+};
+
+// register_A with 10 BCRS arguments (src/kernels/spmv.hpp:54-76)
+struct RegBCRS {
+    bool set = false;
+    uint64_t n_rows = 0, n_cols = 0, n_blocks = 0, bh = 0, bw = 0, hpad = 0, wpad = 0;
+    void *col = nullptr, *row_ptr = nullptr, *val = nullptr;
+};
+
 struct RegDense {
     bool set = false;
     uint64_t n_rows = 0, n_cols = 0;
@@ -38,16 +53,8 @@ struct RegDense {
     uint64_t elems() const { return n_rows * (n_cols ? n_cols : 1); }
 };
 
-// Device copy of a CRS matrix (int32 indices).
-struct DevCRS {
-    int64_t n_rows = 0, n_cols = 0, nnz = 0;
-    DevBuf row_ptr, col, val;
-    // pad: col/val are allocated and zero-filled up to a multiple of `pad` entries
-    void upload(const RegCRS &r, int vbytes, cudaStream_t st, int64_t pad = 1);
-    const int *rp() const { return row_ptr.as<int>(); }
-    const int *ci() const { return col.as<int>(); }
-};
-
+// pad: col/val are allocated and zero-filled up to a multiple of `pad` entries
+void upload_crs(DevCRS &d, const RegCRS &r, int vbytes, cudaStream_t st, int64_t pad = 1);
 void validate_crs(const DevCRS &m, DevStatus *st, cudaStream_t s);
 
 struct PendingEvents {
@@ -56,6 +63,8 @@ struct PendingEvents {
     double drain();  // waits for and sums all live intervals (seconds)
     ~PendingEvents();
 };
+
+double wall_s();
 
 }  // namespace smax
 
@@ -71,6 +80,8 @@ struct smax_kernel_s {
 
     // Args as registered (host pointers unless f_device for B/C)
     smax::RegCRS A;
+    smax::RegSCS A_scs;
+    smax::RegBCRS A_bcrs;
     smax::RegDense B, C;
     bool a_dirty = true;
 
@@ -78,11 +89,13 @@ struct smax_kernel_s {
     cudaStream_t stream = nullptr;      // current stream (own or the caller's)
     cudaStream_t own_stream = nullptr;  // created with the kernel
     smax::DevCRS dA;
+    smax::DevSCS dS;
+    smax::DevBCRS dBc;
     smax::DevBuf dB, dC;
     smax::CrsTilePlan crs_plan;
     smax::CrsStreamPlan crs_stream;
     int spmv_variant = 0;  // 0 auto, 1 warp-stream, 2 row-tile
-    smax::DevBuf status;  // smax::DevStatus
+    smax::DevBuf status;   // smax::DevStatus
 
     // stopwatches
     std::map<std::string, double> timers;

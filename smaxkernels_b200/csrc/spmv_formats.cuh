@@ -1,0 +1,48 @@
+// spmv_formats.cuh -- device-resident SELL-C-sigma and BCRS matrices, their
+// SpMV launchers and the GPU conversions from CRS; SpMM launchers.
+#pragma once
+
+#include "common.cuh"
+
+namespace smax {
+
+// Device copy of a CRS matrix (int32 indices); col/val may be padded.
+struct DevCRS {
+    int64_t n_rows = 0, n_cols = 0, nnz = 0;
+    DevBuf row_ptr, col, val;
+    const int *rp() const { return row_ptr.as<int>(); }
+    const int *ci() const { return col.as<int>(); }
+};
+
+// SELL-C-sigma (src/common.hpp:62-88)
+struct DevSCS {
+    int64_t C = 0, sigma = 0, n_rows = 0, n_rows_padded = 0, n_cols = 0, n_chunks = 0, n_elements = 0, nnz = 0;
+    DevBuf chunk_ptr, chunk_len, col, val;
+};
+
+// BCRS (src/common.hpp:90-111): n_rows/n_cols count blocks
+struct DevBCRS {
+    int64_t n_rows = 0, n_cols = 0, n_blocks = 0, bh = 0, bw = 0, hpad = 0, wpad = 0;
+    bool col_major = false;
+    DevBuf row_ptr, col, val;
+};
+
+void validate_scs(const DevSCS &m, DevStatus *st, cudaStream_t s);
+void validate_bcrs(const DevBCRS &m, DevStatus *st, cudaStream_t s);
+
+template <typename VT> void scs_spmv(const DevSCS &m, const VT *x, VT *y, cudaStream_t st);
+bool scs_vector_path(int64_t C, int vbytes);
+// perm (device, n_rows ints) receives perm[old] = new
+void crs_to_scs(const DevCRS &a, int vbytes, int64_t C, int64_t sigma, DevSCS &out, DevBuf &perm, cudaStream_t st);
+
+template <typename VT> void bcrs_spmv(const DevBCRS &m, const VT *x, VT *y, cudaStream_t st);
+void crs_to_bcrs(const DevCRS &a, int vbytes, int64_t bh, int64_t bw, int64_t hpad, int64_t wpad, bool col_major,
+                 DevBCRS &out, cudaStream_t st);
+
+// Y = A X with k right-hand sides.  Row-major: X[col*k+v], Y[row*k+v].
+// Column-major: X[ldx*v+col], Y[row+ldy*v] (the reference uses A's n_rows as
+// the leading dimension of X and Y, src/kernels/spmm/spmm_cpu/spmm_cpu_crs_impl.hpp:29,44).
+template <typename VT>
+void crs_spmm_row_major(const DevCRS &a, int64_t k, const VT *X, VT *Y, cudaStream_t st);
+
+}  // namespace smax

@@ -1,0 +1,310 @@
+// spmv_scs.cu -- SELL-C-sigma SpMV and CRS -> SELL-C-sigma conversion on sm_100a.
+//
+// Layout (the reference's, src/common.hpp:62-88 and src/utils/convert_formats.hpp:16-132):
+// chunk c holds rows c*C .. c*C+C-1 of the sigma-sorted order; entry j of
+// chunk-row i sits at chunk_ptr[c] + j*C + i; padded entries are col 0 / val 0;
+// y is produced in the permuted order (y[perm[r]] is row r of the CRS product).
+//
+// SpMV (SPMV::CPU::naive_scs_spmv, src/kernels/spmv/spmv_cpu/spmv_cpu_scs_impl.hpp:9-49):
+//   * C a multiple of VEC = 16 / sizeof(VT) and C/VEC <= 32: one warp per chunk;
+//     each lane owns VEC adjacent rows and reads them with one 128-bit load per
+//     chunk column, so C/VEC lanes cover a chunk column and the warp covers
+//     32*VEC/C columns per instruction (chunk-column-major, fully coalesced);
+//     the lanes holding the same rows combine with shuffles at the end and y is
+//     stored with 128-bit stores.
+//   * any other C: one thread per row, consecutive threads on consecutive rows.
+//
+// Conversion (Utils::convert_crs_to_scs): row lengths, a per-sigma-window sort
+// by descending length with ties broken by ascending row (a segmented radix
+// sort of (length, row) keys), chunk lengths as the chunk's maximum, chunk_ptr
+// by scan, perm[old] = new, and a scatter of col/val into the zero-filled
+// chunk-column-major arrays -- all on the GPU.
+#include "spmv_formats.cuh"
+
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_segmented_radix_sort.cuh>
+
+namespace smax {
+
+namespace {
+
+template <typename VT> struct Vec;
+template <> struct Vec<double> { using T = double2; static constexpr int N = 2; };
+template <> struct Vec<float> { using T = float4; static constexpr int N = 4; };
+
+template <typename VT> __device__ __forceinline__ void vec_get(const typename Vec<VT>::T &v, VT *o);
+template <> __device__ __forceinline__ void vec_get<double>(const double2 &v, double *o) { o[0] = v.x; o[1] = v.y; }
+template <> __device__ __forceinline__ void vec_get<float>(const float4 &v, float *o) {
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+
+// one warp per chunk; LPC = C / VEC lanes per chunk column
+template <typename VT, int LPC>
+__global__ void __launch_bounds__(256) scs_warp_kernel(const int *__restrict__ chunk_ptr,
+                                                       const int *__restrict__ chunk_len, int64_t n_chunks,
+                                                       const int *__restrict__ col, const VT *__restrict__ val,
+                                                       const VT *__restrict__ x, VT *__restrict__ y) {
+    constexpr int VEC = Vec<VT>::N;
+    constexpr int C = LPC * VEC;
+    constexpr int CPI = 32 / LPC;  // chunk columns per warp instruction
+    using VV = typename Vec<VT>::T;
+    const int lane = threadIdx.x & 31;
+    const int64_t c = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (c >= n_chunks) return;
+    const int64_t cs = chunk_ptr[c];
+    const int len = chunk_len[c];
+    const int sub = lane % LPC;  // which VEC rows of the chunk
+    const int j0 = lane / LPC;   // first chunk column of this lane
+    VT acc[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) acc[i] = VT(0);
+    for (int j = j0; j < len; j += CPI) {
+        const int64_t idx = cs + (int64_t)j * C + sub * VEC;
+        VT v[VEC];
+        vec_get<VT>(__ldcs(reinterpret_cast<const VV *>(val + idx)), v);
+        int cc[VEC];
+        if constexpr (VEC == 2) {
+            int2 t = __ldcs(reinterpret_cast<const int2 *>(col + idx));
+            cc[0] = t.x; cc[1] = t.y;
+        } else {
+            int4 t = __ldcs(reinterpret_cast<const int4 *>(col + idx));
+            cc[0] = t.x; cc[1] = t.y; cc[2] = t.z; cc[3] = t.w;
+        }
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) acc[i] += v[i] * ld_keep(x + cc[i]);
+    }
+    // lanes with the same `sub` hold partial sums of the same rows
+#pragma unroll
+    for (int o = LPC; o < 32; o <<= 1)
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+    if (j0 == 0) {
+        VV out;
+        if constexpr (VEC == 2) { out.x = acc[0]; out.y = acc[1]; }
+        else { out.x = acc[0]; out.y = acc[1]; out.z = acc[2]; out.w = acc[3]; }
+        __stcs(reinterpret_cast<VV *>(y + c * C + sub * VEC), out);
+    }
+}
+
+// generic: one thread per (padded) row
+template <typename VT>
+__global__ void scs_thread_kernel(const int *__restrict__ chunk_ptr, const int *__restrict__ chunk_len, int64_t C,
+                                  int64_t n_rows_padded, const int *__restrict__ col, const VT *__restrict__ val,
+                                  const VT *__restrict__ x, VT *__restrict__ y) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rows_padded) return;
+    const int64_t c = r / C, i = r % C;
+    const int64_t cs = chunk_ptr[c];
+    const int len = chunk_len[c];
+    VT acc = VT(0);
+    for (int j = 0; j < len; ++j) {
+        const int64_t idx = cs + (int64_t)j * C + i;
+        acc += ld_stream(val + idx) * ld_keep(x + ld_stream(col + idx));
+    }
+    y[r] = acc;
+}
+
+// ----------------------------------------------------------- conversion ----
+__global__ void scs_keys_kernel(const int *__restrict__ row_ptr, int64_t n, int64_t npad,
+                                unsigned long long *__restrict__ keys) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npad) return;
+    const unsigned cnt = i < n ? (unsigned)(row_ptr[i + 1] - row_ptr[i]) : 0u;
+    // ascending key order == longer rows first, then lower original row
+    keys[i] = ((unsigned long long)(0x7fffffffu - cnt) << 32) | (unsigned long long)i;
+}
+
+__global__ void scs_window_offsets(int64_t npad, int64_t sigma, int64_t n_windows, int *__restrict__ off) {
+    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w > n_windows) return;
+    const int64_t o = w * sigma;
+    off[w] = (int)(o < npad ? o : npad);
+}
+
+// chunk lengths (max row length in the chunk) and perm[old] = new
+__global__ void scs_chunks_kernel(const unsigned long long *__restrict__ sorted, int64_t n, int64_t C,
+                                  int64_t n_chunks, int *__restrict__ chunk_len, int *__restrict__ perm) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_chunks) return;
+    unsigned mx = 0;
+    for (int64_t i = c * C; i < (c + 1) * C; ++i) {
+        const unsigned long long k = sorted[i];
+        const unsigned cnt = 0x7fffffffu - (unsigned)(k >> 32);
+        const int64_t old = (int64_t)(k & 0xffffffffull);
+        if (cnt > mx) mx = cnt;
+        if (old < n) perm[old] = (int)i;
+    }
+    chunk_len[c] = (int)mx;
+}
+
+__global__ void scs_chunk_sizes(const int *__restrict__ chunk_len, int64_t n_chunks, int64_t C,
+                                long long *__restrict__ sizes) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n_chunks) sizes[c] = (long long)chunk_len[c] * C;
+}
+
+__global__ void scs_ptr_kernel(const long long *__restrict__ incl, int64_t n_chunks, int *__restrict__ chunk_ptr) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > n_chunks) return;
+    chunk_ptr[c] = c == 0 ? 0 : (int)incl[c - 1];
+}
+
+// one warp per original row: its entries go to chunk-column j of its new row
+template <typename VT>
+__global__ void scs_scatter_kernel(const int *__restrict__ row_ptr, const int *__restrict__ col,
+                                   const VT *__restrict__ val, int64_t n, int64_t C, const int *__restrict__ perm,
+                                   const int *__restrict__ chunk_ptr, int *__restrict__ o_col, VT *__restrict__ o_val) {
+    const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= n) return;
+    const int64_t nr = perm[r];
+    const int64_t base = (int64_t)chunk_ptr[nr / C] + nr % C;
+    const int s = row_ptr[r], e = row_ptr[r + 1];
+    for (int j = s + lane; j < e; j += 32) {
+        const int64_t dst = base + (int64_t)(j - s) * C;
+        o_col[dst] = col[j];
+        o_val[dst] = val[j];
+    }
+}
+
+}  // namespace
+
+bool scs_vector_path(int64_t C, int vbytes) {
+    const int vec = 16 / vbytes;
+    return C % vec == 0 && C / vec >= 1 && C / vec <= 32 && ((C / vec) & (C / vec - 1)) == 0;
+}
+
+template <typename VT>
+void scs_spmv(const DevSCS &m, const VT *x, VT *y, cudaStream_t st) {
+    if (m.n_chunks == 0) return;
+    const int vec = Vec<VT>::N;
+    // y is written with 16-byte stores: an offset given to apply() may unalign it
+    const bool y_aligned = (reinterpret_cast<uintptr_t>(y) & 15) == 0;
+    if (y_aligned && scs_vector_path(m.C, sizeof(VT))) {
+        const unsigned grid = ceil_div_u(m.n_chunks, 8);
+        const int *cp = m.chunk_ptr.as<int>(), *cl = m.chunk_len.as<int>(), *ci = m.col.as<int>();
+        const VT *v = m.val.as<VT>();
+        switch (m.C / vec) {
+        case 1: scs_warp_kernel<VT, 1><<<grid, 256, 0, st>>>(cp, cl, m.n_chunks, ci, v, x, y); break;
+        case 2: scs_warp_kernel<VT, 2><<<grid, 256, 0, st>>>(cp, cl, m.n_chunks, ci, v, x, y); break;
+        case 4: scs_warp_kernel<VT, 4><<<grid, 256, 0, st>>>(cp, cl, m.n_chunks, ci, v, x, y); break;
+        case 8: scs_warp_kernel<VT, 8><<<grid, 256, 0, st>>>(cp, cl, m.n_chunks, ci, v, x, y); break;
+        case 16: scs_warp_kernel<VT, 16><<<grid, 256, 0, st>>>(cp, cl, m.n_chunks, ci, v, x, y); break;
+        case 32: scs_warp_kernel<VT, 32><<<grid, 256, 0, st>>>(cp, cl, m.n_chunks, ci, v, x, y); break;
+        default: fail(SMAX_ERR_STATE, "unexpected SELL chunk width");
+        }
+    } else {
+        scs_thread_kernel<VT><<<ceil_div_u(m.n_rows_padded, 256), 256, 0, st>>>(
+            m.chunk_ptr.as<int>(), m.chunk_len.as<int>(), m.C, m.n_rows_padded, m.col.as<int>(), m.val.as<VT>(),
+            x, y);
+    }
+    SMAX_CUDA(cudaGetLastError());
+}
+
+template void scs_spmv<double>(const DevSCS &, const double *, double *, cudaStream_t);
+template void scs_spmv<float>(const DevSCS &, const float *, float *, cudaStream_t);
+
+void crs_to_scs(const DevCRS &a, int vbytes, int64_t C, int64_t sigma, DevSCS &out, DevBuf &perm, cudaStream_t st) {
+    if (C <= 0 || sigma <= 0) fail(SMAX_ERR_BAD_ARG, "C and sigma must be positive");
+    const int64_t n = a.n_rows;
+    const int64_t n_chunks = (n + C - 1) / C;
+    const int64_t npad = n_chunks * C;
+    out.C = C;
+    out.sigma = sigma;
+    out.n_rows = n;
+    out.n_rows_padded = npad;
+    out.n_cols = a.n_cols;
+    out.n_chunks = n_chunks;
+    out.nnz = a.nnz;
+    perm.alloc(sizeof(int) * (n > 0 ? n : 1));
+    out.chunk_ptr.alloc(sizeof(int) * (n_chunks + 1));
+    out.chunk_len.alloc(sizeof(int) * (n_chunks > 0 ? n_chunks : 1));
+    if (npad == 0) {
+        SMAX_CUDA(cudaMemsetAsync(out.chunk_ptr.p, 0, sizeof(int), st));
+        out.n_elements = 0;
+        return;
+    }
+    DevBuf keys(sizeof(unsigned long long) * npad), sorted(sizeof(unsigned long long) * npad);
+    scs_keys_kernel<<<ceil_div_u(npad, 256), 256, 0, st>>>(a.rp(), n, npad, keys.as<unsigned long long>());
+    SMAX_CUDA(cudaGetLastError());
+    const int64_t n_windows = (npad + sigma - 1) / sigma;
+    DevBuf woff(sizeof(int) * (n_windows + 1));
+    scs_window_offsets<<<ceil_div_u(n_windows + 1, 256), 256, 0, st>>>(npad, sigma, n_windows, woff.as<int>());
+    SMAX_CUDA(cudaGetLastError());
+    size_t tb = 0;
+    SMAX_CUDA(cub::DeviceSegmentedRadixSort::SortKeys(nullptr, tb, keys.as<unsigned long long>(),
+                                                      sorted.as<unsigned long long>(), (int)npad, (int)n_windows,
+                                                      woff.as<int>(), woff.as<int>() + 1, 0, 64, st));
+    DevBuf tmp(tb);
+    SMAX_CUDA(cub::DeviceSegmentedRadixSort::SortKeys(tmp.p, tb, keys.as<unsigned long long>(),
+                                                      sorted.as<unsigned long long>(), (int)npad, (int)n_windows,
+                                                      woff.as<int>(), woff.as<int>() + 1, 0, 64, st));
+    scs_chunks_kernel<<<ceil_div_u(n_chunks, 256), 256, 0, st>>>(sorted.as<unsigned long long>(), n, C, n_chunks,
+                                                                 out.chunk_len.as<int>(), perm.as<int>());
+    SMAX_CUDA(cudaGetLastError());
+    DevBuf sizes(sizeof(long long) * n_chunks), incl(sizeof(long long) * n_chunks);
+    scs_chunk_sizes<<<ceil_div_u(n_chunks, 256), 256, 0, st>>>(out.chunk_len.as<int>(), n_chunks, C,
+                                                               sizes.as<long long>());
+    SMAX_CUDA(cudaGetLastError());
+    size_t tb2 = 0;
+    SMAX_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb2, sizes.as<long long>(), incl.as<long long>(),
+                                            (int)n_chunks, st));
+    DevBuf tmp2(tb2);
+    SMAX_CUDA(cub::DeviceScan::InclusiveSum(tmp2.p, tb2, sizes.as<long long>(), incl.as<long long>(),
+                                            (int)n_chunks, st));
+    long long ne = 0;
+    SMAX_CUDA(cudaMemcpyAsync(&ne, incl.as<long long>() + n_chunks - 1, sizeof(long long), cudaMemcpyDeviceToHost,
+                              st));
+    SMAX_CUDA(cudaStreamSynchronize(st));
+    if (ne >= (1ll << 31)) fail(SMAX_ERR_UNSUPPORTED, "SELL-C-sigma matrix exceeds int32 indexing");
+    out.n_elements = ne;
+    scs_ptr_kernel<<<ceil_div_u(n_chunks + 1, 256), 256, 0, st>>>(incl.as<long long>(), n_chunks,
+                                                                  out.chunk_ptr.as<int>());
+    SMAX_CUDA(cudaGetLastError());
+    out.col.alloc(sizeof(int) * (ne > 0 ? ne : 1));
+    out.val.alloc((size_t)vbytes * (ne > 0 ? ne : 1));
+    SMAX_CUDA(cudaMemsetAsync(out.col.p, 0, sizeof(int) * ne, st));
+    SMAX_CUDA(cudaMemsetAsync(out.val.p, 0, (size_t)vbytes * ne, st));
+    if (n > 0 && a.nnz > 0) {
+        const unsigned grid = ceil_div_u((uint64_t)n * 32, 256);
+        if (vbytes == 8)
+            scs_scatter_kernel<double><<<grid, 256, 0, st>>>(a.rp(), a.ci(), a.val.as<double>(), n, C, perm.as<int>(),
+                                                             out.chunk_ptr.as<int>(), out.col.as<int>(),
+                                                             out.val.as<double>());
+        else
+            scs_scatter_kernel<float><<<grid, 256, 0, st>>>(a.rp(), a.ci(), a.val.as<float>(), n, C, perm.as<int>(),
+                                                            out.chunk_ptr.as<int>(), out.col.as<int>(),
+                                                            out.val.as<float>());
+        SMAX_CUDA(cudaGetLastError());
+    }
+    SMAX_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace smax
+
+namespace smax {
+namespace {
+// chunk_ptr[0] == 0, chunk_ptr[c+1] - chunk_ptr[c] == chunk_len[c]*C (so every
+// chunk start is a multiple of C, which the vector loads rely on),
+// chunk_ptr[n_chunks] == n_elements, every column in [0, n_cols).
+__global__ void validate_scs_kernel(const int *__restrict__ cp, const int *__restrict__ cl,
+                                    const int *__restrict__ col, int64_t n_chunks, int64_t C, int64_t n_elements,
+                                    int64_t n_cols, DevStatus *st) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0 && (cp[0] != 0 || cp[n_chunks] != n_elements)) report(st, SMAX_ERR_BAD_ARG, 0);
+    for (int64_t c = t; c < n_chunks; c += stride)
+        if (cl[c] < 0 || (int64_t)cp[c + 1] - cp[c] != (int64_t)cl[c] * C) report(st, SMAX_ERR_BAD_ARG, c);
+    for (int64_t j = t; j < n_elements; j += stride) {
+        const int c = col[j];
+        if (c < 0 || c >= n_cols) report(st, SMAX_ERR_COL_OOB, j);
+    }
+}
+}  // namespace
+
+void validate_scs(const DevSCS &m, DevStatus *st, cudaStream_t s) {
+    validate_scs_kernel<<<4 * sm_count(), 256, 0, s>>>(m.chunk_ptr.as<int>(), m.chunk_len.as<int>(), m.col.as<int>(),
+                                                       m.n_chunks, m.C, m.n_elements, m.n_cols, st);
+    SMAX_CUDA(cudaGetLastError());
+}
+}  // namespace smax

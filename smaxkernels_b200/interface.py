@@ -96,17 +96,41 @@ class Kernel:
         self.float_type = ftype
         self._keep = {}  # registered arrays stay alive while registered
         self._device = None
+        self._scs = False
+        self._bcrs = False
 
     # -- registration -----------------------------------------------------
     def register_A(self, *args):
+        """CRS (6 args), BCRS (10 args, after set_mat_bcrs) or SELL-C-sigma (13 args,
+        after set_mat_scs), in the reference's argument orders (src/kernels/spmv.hpp:25-91)."""
         n = len(args)
+        if self._scs:
+            if n != 13:
+                raise RuntimeError("SpMVKernel register_A expects 13 Sell-C-sigma args")
+            (C_, sigma, n_rows, n_rows_padded, n_cols, n_chunks, n_elements, nnz, chunk_ptr, chunk_lengths, col,
+             val, perm) = args
+            self._keep["A"] = (chunk_ptr, chunk_lengths, col, val, perm)
+            check(lib.smax_kernel_register_A_scs(self._h, int(C_), int(sigma), int(n_rows), int(n_rows_padded),
+                                                 int(n_cols), int(n_chunks), int(n_elements), int(nnz),
+                                                 _ptr(chunk_ptr), _ptr(chunk_lengths), _ptr(col), _ptr(val),
+                                                 _ptr(perm)))
+            return 0
+        if self._bcrs:
+            if n != 10:
+                raise RuntimeError("SpMVKernel register_A expects 10 BCRS args")
+            n_rows, n_cols, n_blocks, bh, bw, hpad, wpad, col, row_ptr, val = args
+            self._keep["A"] = (col, row_ptr, val)
+            check(lib.smax_kernel_register_A_bcrs(self._h, int(n_rows), int(n_cols), int(n_blocks), int(bh),
+                                                  int(bw), int(hpad), int(wpad), _ptr(col), _ptr(row_ptr),
+                                                  _ptr(val)))
+            return 0
         if n == 6:
             n_rows, n_cols, nnz, col, row_ptr, val = args
             self._keep["A"] = (col, row_ptr, val)
             check(lib.smax_kernel_register_A_crs(self._h, int(n_rows), int(n_cols), int(nnz), _ptr(col),
                                                  _ptr(row_ptr), _ptr(val)))
             return 0
-        raise RuntimeError(f"{self.kernel_type.name} register_A: unsupported argument count {n}")
+        raise RuntimeError(f"{self.kernel_type.name} register_A expects 6 args")
 
     def _register_dense(self, slot: int, args):
         if len(args) == 2:
@@ -150,9 +174,11 @@ class Kernel:
         return self._flag("vec_row_major", v)
 
     def set_mat_scs(self, v):
+        self._scs = bool(v)
         return self._flag("mat_scs", v)
 
     def set_mat_bcrs(self, v):
+        self._bcrs = bool(v)
         return self._flag("mat_bcrs", v)
 
     def set_block_column_major(self, v):
@@ -207,6 +233,68 @@ class Kernel:
             self._h = None
 
 
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _ftype(dtype) -> int:
+    if np.dtype(dtype) == np.float64:
+        return int(FloatType.FLOAT64)
+    if np.dtype(dtype) == np.float32:
+        return int(FloatType.FLOAT32)
+    raise TypeError("values must be float32 or float64")
+
+
+def _take(p, n, dtype):
+    """Copies n elements of a library-allocated host array into numpy and frees it."""
+    if not p:
+        return np.zeros(0, dtype)
+    out = np.empty(n, dtype=dtype)
+    if n:
+        C.memmove(out.ctypes.data, p, n * out.itemsize)
+    lib.smax_free_host(p)
+    return out
+
+
+class Utils:
+    """SMAX::Utils (src/utils.hpp:12-87): the work runs on the GPU; inputs and
+    outputs are host numpy arrays, as the reference's are host arrays."""
+
+    def __init__(self, iface: "Interface"):
+        self._iface = iface
+
+    def convert_crs_to_scs(self, n_rows, n_cols, nnz, col, row_ptr, val, C_, sigma) -> dict:
+        """Returns the 13 SELL-C-sigma fields of convert_crs_to_scs as a dict."""
+        col, row_ptr = _i32(col), _i32(row_ptr)
+        val = np.ascontiguousarray(val)
+        meta = (C.c_uint64 * 6)()
+        ptrs = [C.c_void_p() for _ in range(5)]
+        check(lib.smax_utils_convert_crs_to_scs(int(IntType.INT32), _ftype(val.dtype), int(n_rows), int(n_cols),
+                                                int(nnz), _ptr(col), _ptr(row_ptr), _ptr(val), int(C_),
+                                                int(sigma), meta, *[C.byref(p) for p in ptrs]))
+        nr, npad, nc, nch, ne, nz = (int(v) for v in meta)
+        return dict(C=int(C_), sigma=int(sigma), n_rows=nr, n_rows_padded=npad, n_cols=nc, n_chunks=nch,
+                    n_elements=ne, nnz=nz, chunk_ptr=_take(ptrs[0].value, nch + 1, np.int32),
+                    chunk_lengths=_take(ptrs[1].value, nch, np.int32), col=_take(ptrs[2].value, ne, np.int32),
+                    val=_take(ptrs[3].value, ne, val.dtype), perm=_take(ptrs[4].value, nr, np.int32))
+
+    def convert_crs_to_bcrs(self, n_rows, n_cols, nnz, col, row_ptr, val, b_height, b_width, height_pad,
+                            width_pad, block_column_major) -> dict:
+        col, row_ptr = _i32(col), _i32(row_ptr)
+        val = np.ascontiguousarray(val)
+        meta = (C.c_uint64 * 7)()
+        ptrs = [C.c_void_p() for _ in range(3)]
+        check(lib.smax_utils_convert_crs_to_bcrs(int(IntType.INT32), _ftype(val.dtype), int(n_rows), int(n_cols),
+                                                 int(nnz), _ptr(col), _ptr(row_ptr), _ptr(val), int(b_height),
+                                                 int(b_width), int(height_pad), int(width_pad),
+                                                 int(bool(block_column_major)), meta,
+                                                 *[C.byref(p) for p in ptrs]))
+        nr, nc, nb, bh, bw, hp, wp = (int(v) for v in meta)
+        return dict(n_rows=nr, n_cols=nc, n_blocks=nb, b_height=bh, b_width=bw, height_pad=hp, width_pad=wp,
+                    col=_take(ptrs[0].value, nb, np.int32), row_ptr=_take(ptrs[1].value, nr + 1, np.int32),
+                    val=_take(ptrs[2].value, nb * hp * wp, val.dtype))
+
+
 class Interface:
     """SMAX::Interface for the CUDA platform (src/interface.hpp:21-48)."""
 
@@ -215,6 +303,7 @@ class Interface:
         check(lib.smax_ctx_create(C.byref(h)))
         self._ctx = h
         self._kernels: dict[str, Kernel] = {}
+        self.utils = Utils(self)
 
     def register_kernel(self, name: str, kernel_type: KernelType, platform: PlatformType = PlatformType.CUDA,
                         int_type: IntType = IntType.INT32, float_type: FloatType = FloatType.FLOAT64) -> int:
