@@ -88,6 +88,14 @@ typedef int smax_status;
 #define SMAX_FLAG_DEVICE_POINTERS 8    /* B and C registered as device pointers */
 #define SMAX_FLAG_A_DIRTY 9            /* re-upload A at the next initialize */
 #define SMAX_FLAG_SPMV_VARIANT 10      /* CRS SpMV kernel: 0 auto, 1 warp-stream, 2 row-tile */
+#define SMAX_FLAG_SOLVE_MODE 11        /* SpTRSV/SpTRSM launch scheme, one of SMAX_SOLVE_* */
+#define SMAX_FLAG_LEVEL_MERGE 12       /* levels with <= this many rows*rhs run merged in one CTA (0: never) */
+
+/* SpTRSV / SpTRSM launch schemes (SMAX_FLAG_SOLVE_MODE) */
+#define SMAX_SOLVE_AUTO 0        /* graph-captured, narrow levels merged (the default) */
+#define SMAX_SOLVE_PER_LEVEL 1   /* one kernel launch per level, no merging, no graph */
+#define SMAX_SOLVE_MERGED 2      /* narrow levels merged into single-CTA runs, no graph */
+#define SMAX_SOLVE_GRAPH 3       /* the merged launch sequence captured into a CUDA graph */
 
 typedef struct smax_ctx_s *smax_ctx;
 typedef struct smax_kernel_s *smax_kernel;
@@ -185,6 +193,33 @@ smax_status smax_utils_convert_crs_to_bcrs(int int_type, int float_type, uint64_
                                            uint64_t b_height, uint64_t b_width, uint64_t height_pad,
                                            uint64_t width_pad, int block_column_major, uint64_t *meta,
                                            void **col_out, void **row_ptr_out, void **val_out);
+
+/* Utils::build_symmetric_crs (src/utils/permutations.hpp:236-392): the
+ * pattern of A + A^T; row c is A's row c followed by the missing transposes in
+ * ascending row order.  Arrays allocated with new[]. */
+smax_status smax_utils_build_symmetric_crs(int int_type, uint64_t n_rows, const void *row_ptr, const void *col,
+                                           void **sym_row_ptr, void **sym_col, uint64_t *sym_nnz);
+
+/* Utils::generate_perm (src/utils/permutations.hpp:485-584) for types "BFS"
+ * (the default of the reference; queue order of its one-thread BFS), "RS"
+ * (rows stably sorted by level) and "NONE"; computed on the GPU.  perm and
+ * inv_perm are caller arrays of n_rows ints; the level pointer is stored in
+ * ctx (smax_ctx_get_n_levels / smax_ctx_get_level_ptr_at).  The colourings
+ * "SC", "PC", "PC_BAL" return SMAX_ERR_UNSUPPORTED. */
+smax_status smax_utils_generate_perm(smax_ctx ctx, int int_type, uint64_t n_rows, const void *row_ptr,
+                                     const void *col, int *perm, int *inv_perm, const char *type);
+
+/* Utils::apply_mat_perm (src/utils/permutations.hpp:820-861): row r of the
+ * result is row perm[r], columns mapped through inv_perm; output arrays are the
+ * caller's (n_rows+1, nnz, nnz). */
+smax_status smax_utils_apply_mat_perm(int int_type, int float_type, uint64_t n_rows, const void *row_ptr,
+                                      const void *col, const void *val, void *perm_row_ptr, void *perm_col,
+                                      void *perm_val, const int *perm, const int *inv_perm);
+
+/* Utils::apply_vec_perm (src/utils/permutations.hpp:863-874):
+ * vec_perm[i] = vec[perm[i]]. */
+smax_status smax_utils_apply_vec_perm(int float_type, uint64_t n_rows, const void *vec, void *vec_perm,
+                                      const int *perm);
 
 /* Releases an array returned by an smax_utils_* function. */
 void smax_free_host(void *p);

@@ -49,6 +49,10 @@ SIGNATURES = {
     "smax_utils_convert_crs_to_scs": (I32, [I32, I32, U64, U64, U64, P, P, P, U64, U64, PU64] + [PP] * 5),
     "smax_utils_convert_crs_to_bcrs": (I32, [I32, I32, U64, U64, U64, P, P, P, U64, U64, U64, U64, I32, PU64]
                                        + [PP] * 3),
+    "smax_utils_build_symmetric_crs": (I32, [I32, U64, P, P, PP, PP, PU64]),
+    "smax_utils_generate_perm": (I32, [P, I32, U64, P, P, P, P, C.c_char_p]),
+    "smax_utils_apply_mat_perm": (I32, [I32, I32, U64, P, P, P, P, P, P, P, P]),
+    "smax_utils_apply_vec_perm": (I32, [I32, U64, P, P, P]),
     "smax_free_host": (None, [P]),
     "smax_spmv_crs_noalloc": (I32, [I32, U64, U64, U64, P, P, P, P, P, P]),
 }

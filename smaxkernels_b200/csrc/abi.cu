@@ -138,6 +138,62 @@ template <typename VT> void spmm_apply_t(smax_kernel_s *k, const VT *X, VT *Y) {
     }
 }
 
+// ------------------------------------------------------- SpTRSV / SpTRSM --
+// register_B is the solution x (X), register_C the right-hand side b (B)
+// (src/kernels/sptrsv.hpp:40-58, sptrsm.hpp:40-60).
+bool is_tri(const smax_kernel_s *k) { return k->ktype == SMAX_KERNEL_SPTRSV || k->ktype == SMAX_KERNEL_SPTRSM; }
+
+constexpr int kDefaultLevelMerge = 4096;
+
+void tri_upload(smax_kernel_s *k) {
+    require(k->A.set, SMAX_ERR_STATE, "register_A before initialize");
+    require(k->A.n_rows == k->A.n_cols, SMAX_ERR_BAD_ARG, "triangular solves need a square matrix");
+    cudaStream_t st = k->stream;
+    upload_crs(k->dA, k->A, k->vbytes, st);
+    validate_crs(k->dA, dstatus(k), st);
+    read_status(k);
+    peel_diag(k->dA, k->vbytes, k->D, dstatus(k), st);
+    read_status(k);
+    // the reference moves each diagonal entry to the end of its row in the
+    // caller's arrays (sptrsv_cpu_core.hpp:21-38); mirror that
+    if (k->A.nnz) {
+        SMAX_CUDA(cudaMemcpyAsync(k->A.col, k->dA.col.p, sizeof(int) * k->A.nnz, cudaMemcpyDeviceToHost, st));
+        SMAX_CUDA(cudaMemcpyAsync(k->A.val, k->dA.val.p, (size_t)k->vbytes * k->A.nnz, cudaMemcpyDeviceToHost, st));
+    }
+    SMAX_CUDA(cudaStreamSynchronize(st));
+    k->tri_plan_valid = false;
+}
+
+void tri_plan(smax_kernel_s *k) {
+    if (k->f_perm) {
+        require(k->ctx != nullptr && k->ctx->n_levels > 0, SMAX_ERR_STATE,
+                "level-scheduled solve needs the levels of generate_perm in the context");
+        if (!k->tri_plan_valid || k->tri_levels_version != k->ctx->levels_version) {
+            k->tri.release_graph();
+            k->tri.build_given(k->ctx->lvl_ptr, k->dA.n_rows, k->f_upper, k->stream);
+            k->tri_levels_version = k->ctx->levels_version;
+            k->tri_plan_valid = true;
+        }
+    } else if (!k->tri_plan_valid) {
+        k->tri.release_graph();
+        k->tri.build_own(k->dA, k->f_upper, k->stream);
+        k->tri_plan_valid = true;
+    }
+}
+
+template <typename VT> void tri_apply_t(smax_kernel_s *k, const VT *Bv, VT *Xv) {
+    tri_plan(k);
+    const int64_t kk = k->ktype == SMAX_KERNEL_SPTRSM ? (int64_t)(k->B.n_cols ? k->B.n_cols : 1) : 1;
+    const bool rm = k->ktype == SMAX_KERNEL_SPTRSM ? k->f_row_major : true;
+    const int64_t ld = k->dA.n_rows;  // column-major blocks use A's n_rows (sptrsm_cpu_crs_impl.hpp:44-50)
+    const int merge = k->solve_mode == SMAX_SOLVE_PER_LEVEL ? 0
+                      : (k->level_merge >= 0 ? k->level_merge : kDefaultLevelMerge);
+    if (k->solve_mode == SMAX_SOLVE_AUTO || k->solve_mode == SMAX_SOLVE_GRAPH)
+        tri_solve_graph<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, kk, rm, ld, merge, k->stream);
+    else
+        tri_solve<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, kk, rm, ld, merge, k->stream);
+}
+
 // Device addresses of B and C (+ element offsets).
 const void *dev_b(smax_kernel_s *k, uint64_t off) {
     const char *base = k->f_device ? static_cast<const char *>(k->B.val) : static_cast<const char *>(k->dB.p);
@@ -164,6 +220,17 @@ void check_extents(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
         else { need_b = (kk - 1) * k->A.n_rows + k->A.n_cols; need_c = k->A.n_rows * kk; }
         break;
     }
+    case SMAX_KERNEL_SPTRSV:
+        need_b = k->A.n_rows;
+        need_c = k->A.n_rows;
+        break;
+    case SMAX_KERNEL_SPTRSM: {
+        const uint64_t kk = k->B.n_cols ? k->B.n_cols : 1;
+        require(k->C.n_cols == k->B.n_cols, SMAX_ERR_BAD_ARG, "X and B must have the same number of vectors");
+        need_b = k->A.n_rows * kk;
+        need_c = k->A.n_rows * kk;
+        break;
+    }
     default: break;
     }
     require(b_off + need_b <= k->B.elems(), SMAX_ERR_BAD_ARG, "B (with offset) is smaller than the operator needs");
@@ -177,6 +244,8 @@ void do_initialize(smax_kernel_s *k) {
         switch (k->ktype) {
         case SMAX_KERNEL_SPMV: spmv_upload(k); break;
         case SMAX_KERNEL_SPMM: spmm_upload(k); break;
+        case SMAX_KERNEL_SPTRSV:
+        case SMAX_KERNEL_SPTRSM: tri_upload(k); break;
         default: fail(SMAX_ERR_UNSUPPORTED, "kernel type not available in this build");
         }
         k->a_dirty = false;
@@ -185,7 +254,12 @@ void do_initialize(smax_kernel_s *k) {
         size_t bb = (size_t)k->B.elems() * k->vbytes, cb = (size_t)k->C.elems() * k->vbytes;
         k->dB.ensure(bb);
         k->dC.ensure(cb);
-        if (bb) SMAX_CUDA(cudaMemcpyAsync(k->dB.p, k->B.val, bb, cudaMemcpyHostToDevice, k->stream));
+        // the kernel's input: B (x / X) for SpMV and SpMM, C (b / B) for solves
+        if (is_tri(k)) {
+            if (cb) SMAX_CUDA(cudaMemcpyAsync(k->dC.p, k->C.val, cb, cudaMemcpyHostToDevice, k->stream));
+        } else {
+            if (bb) SMAX_CUDA(cudaMemcpyAsync(k->dB.p, k->B.val, bb, cudaMemcpyHostToDevice, k->stream));
+        }
     }
     SMAX_CUDA(cudaStreamSynchronize(k->stream));
     k->timers["initialize"] += wall_s() - t0;
@@ -208,6 +282,15 @@ void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
         if (f64) spmm_apply_t<double>(k, static_cast<const double *>(b), static_cast<double *>(c));
         else spmm_apply_t<float>(k, static_cast<const float *>(b), static_cast<float *>(c));
         break;
+    case SMAX_KERNEL_SPTRSV:
+    case SMAX_KERNEL_SPTRSM: {
+        // solves read C (right-hand sides) and write B (solution)
+        void *x = const_cast<void *>(b);
+        const void *rhs = c;
+        if (f64) tri_apply_t<double>(k, static_cast<const double *>(rhs), static_cast<double *>(x));
+        else tri_apply_t<float>(k, static_cast<const float *>(rhs), static_cast<float *>(x));
+        break;
+    }
     default: fail(SMAX_ERR_UNSUPPORTED, "kernel type not available in this build");
     }
     SMAX_CUDA(cudaEventRecord(ev.second, k->stream));
@@ -216,8 +299,13 @@ void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
 void do_finalize(smax_kernel_s *k) {
     double t0 = wall_s();
     if (!k->f_device) {
-        size_t cb = (size_t)k->C.elems() * k->vbytes;
-        if (cb) SMAX_CUDA(cudaMemcpyAsync(k->C.val, k->dC.p, cb, cudaMemcpyDeviceToHost, k->stream));
+        if (is_tri(k)) {
+            size_t bb = (size_t)k->B.elems() * k->vbytes;
+            if (bb) SMAX_CUDA(cudaMemcpyAsync(k->B.val, k->dB.p, bb, cudaMemcpyDeviceToHost, k->stream));
+        } else {
+            size_t cb = (size_t)k->C.elems() * k->vbytes;
+            if (cb) SMAX_CUDA(cudaMemcpyAsync(k->C.val, k->dC.p, cb, cudaMemcpyDeviceToHost, k->stream));
+        }
     }
     SMAX_CUDA(cudaStreamSynchronize(k->stream));
     read_status(k);
@@ -287,8 +375,14 @@ smax_status smax_kernel_set_flag(smax_kernel k, int flag, int value) {
         smax_kernel_s *kk = K(k);
         bool v = value != 0;
         switch (flag) {
-        case SMAX_FLAG_MAT_PERM: kk->f_perm = v; break;
-        case SMAX_FLAG_MAT_UPPER_TRIANG: kk->f_upper = v; break;
+        case SMAX_FLAG_MAT_PERM:
+            if (v != kk->f_perm) kk->tri_plan_valid = false;
+            kk->f_perm = v;
+            break;
+        case SMAX_FLAG_MAT_UPPER_TRIANG:
+            if (v != kk->f_upper) kk->tri_plan_valid = false;
+            kk->f_upper = v;
+            break;
         case SMAX_FLAG_MAT_LOWER_TRIANG: kk->f_lower = v; break;
         case SMAX_FLAG_VEC_ROW_MAJOR:
             if (v != kk->f_row_major) kk->a_dirty = true;
@@ -310,6 +404,14 @@ smax_status smax_kernel_set_flag(smax_kernel k, int flag, int value) {
             require(value >= 0 && value <= 2, SMAX_ERR_BAD_ARG, "SpMV variant must be 0, 1 or 2");
             if (value != kk->spmv_variant) kk->a_dirty = true;  // plans differ per variant
             kk->spmv_variant = value;
+            break;
+        case SMAX_FLAG_SOLVE_MODE:
+            require(value >= SMAX_SOLVE_AUTO && value <= SMAX_SOLVE_GRAPH, SMAX_ERR_BAD_ARG, "unknown solve mode");
+            kk->solve_mode = value;
+            break;
+        case SMAX_FLAG_LEVEL_MERGE:
+            require(value >= 0, SMAX_ERR_BAD_ARG, "level merge threshold must be >= 0");
+            kk->level_merge = value;
             break;
         default: fail(SMAX_ERR_BAD_ARG, "unknown flag");
         }

@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "spmv_crs.cuh"
 #include "spmv_formats.cuh"
+#include "sptrsv.cuh"
 
 struct smax_ctx_s {
     // UtilitiesContainer (src/common.hpp:187-195): written by generate_perm,
@@ -96,6 +97,14 @@ struct smax_kernel_s {
     smax::CrsStreamPlan crs_stream;
     int spmv_variant = 0;  // 0 auto, 1 warp-stream, 2 row-tile
     smax::DevBuf status;   // smax::DevStatus
+
+    // triangular solves (SpTRSV / SpTRSM)
+    smax::DevBuf D;                 // peeled diagonal
+    smax::TriPlan tri;
+    bool tri_plan_valid = false;
+    uint64_t tri_levels_version = 0;
+    int solve_mode = 0;             // SMAX_SOLVE_*
+    int level_merge = -1;           // rows*k of levels merged into one-CTA runs; -1 = default
 
     // stopwatches
     std::map<std::string, double> timers;

@@ -73,7 +73,8 @@ void upload_crs(DevCRS &d, const RegCRS &r, int vbytes, cudaStream_t st, int64_t
     SMAX_CUDA(cudaMemcpyAsync(d.row_ptr.p, r.row_ptr, sizeof(int) * (r.n_rows + 1), cudaMemcpyHostToDevice, st));
     if (r.nnz) {
         SMAX_CUDA(cudaMemcpyAsync(d.col.p, r.col, sizeof(int) * r.nnz, cudaMemcpyHostToDevice, st));
-        SMAX_CUDA(cudaMemcpyAsync(d.val.p, r.val, (size_t)vbytes * r.nnz, cudaMemcpyHostToDevice, st));
+        // a pattern-only upload (val == nullptr) leaves the values unset
+        if (r.val) SMAX_CUDA(cudaMemcpyAsync(d.val.p, r.val, (size_t)vbytes * r.nnz, cudaMemcpyHostToDevice, st));
     }
 }
 

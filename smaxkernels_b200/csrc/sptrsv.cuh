@@ -1,0 +1,65 @@
+// sptrsv.cuh -- level-scheduled triangular solves (sptrsv.cu).
+#pragma once
+
+#include <vector>
+
+#include "levels.cuh"
+#include "spmv_formats.cuh"
+
+namespace smax {
+
+// Copies the diagonal into D and swaps it to the last slot of each row (in
+// place on the device copy); missing / |d| < 1e-16 diagonals are reported.
+void peel_diag(DevCRS &a, int vbytes, DevBuf &D, DevStatus *st, cudaStream_t s);
+
+// The level schedule of one triangular matrix and its launch plan.
+struct TriPlan {
+    int64_t n_rows = 0;
+    std::vector<int> lvl_ptr;  // host copy, n_levels + 1 entries
+    DevBuf order;              // rows sorted by level (own levels) or unused
+    bool has_order = false;
+    bool descending = false;   // sweep levels last to first
+
+    // launch plan: steps of single wide levels (kind 0) or merged runs (kind 1)
+    struct Step {
+        int kind = 0;
+        int row0 = 0, m = 0;
+        int seg_first = 0, seg_count = 0;
+    };
+    std::vector<Step> steps;
+    std::vector<int2> seg_ranges;
+    DevBuf d_ranges;
+    bool ranges_uploaded = false;
+    int64_t scheduled_k = -1;
+    int scheduled_merge = -1;
+
+    // CUDA graph of the launch sequence (bound to the operand addresses)
+    cudaGraphExec_t graph = nullptr;
+    bool graph_valid = false;
+    const void *graph_key[3] = {nullptr, nullptr, nullptr};
+    bool graph_row_major = false;
+    int64_t graph_ld = 0;
+
+    // dependency levels of the matrix itself (plain solve)
+    void build_own(const DevCRS &a, bool upper, cudaStream_t st);
+    // caller-given contiguous levels (permuted, level-scheduled solve)
+    void build_given(const std::vector<int> &lvl_ptr, int64_t n, bool upper, cudaStream_t st);
+    void finish(cudaStream_t st);
+    void schedule(int64_t k, int merge_rows);
+    void release_graph();
+    int n_levels() const { return lvl_ptr.empty() ? 0 : (int)lvl_ptr.size() - 1; }
+    ~TriPlan();
+};
+
+// X = A^{-1} B for k right-hand sides (row-major: element (r, v) at r*k+v;
+// column-major: at r + v*ld).  merge_rows: levels with at most this many
+// (row, vector) pairs are merged into single-CTA runs (0 disables merging).
+template <typename VT>
+void tri_solve(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int64_t k, bool row_major, int64_t ld,
+               int merge_rows, cudaStream_t st);
+// The same launch sequence, captured once into a CUDA graph and replayed.
+template <typename VT>
+void tri_solve_graph(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int64_t k, bool row_major,
+                     int64_t ld, int merge_rows, cudaStream_t st);
+
+}  // namespace smax

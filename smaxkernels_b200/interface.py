@@ -63,7 +63,9 @@ class SpMVType(enum.IntEnum):
 
 FLAG = dict(mat_perm=0, mat_upper_triang=1, mat_lower_triang=2, vec_row_major=3, mat_scs=4, mat_bcrs=5,
             block_column_major=6, kernel_impl=7, device_pointers=8, a_dirty=9,
-            spmv_variant=10)
+            spmv_variant=10, solve_mode=11, level_merge=12)
+
+SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED, SOLVE_GRAPH = 0, 1, 2, 3
 
 
 def _is_torch_cuda(a) -> bool:
@@ -191,6 +193,14 @@ class Kernel:
         """CRS SpMV kernel: 0 auto, 1 warp-stream, 2 row-tile."""
         return self._flag("spmv_variant", v)
 
+    def set_solve_mode(self, mode: int):
+        """SpTRSV/SpTRSM launch scheme: SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED or SOLVE_GRAPH."""
+        return self._flag("solve_mode", mode)
+
+    def set_level_merge(self, rows: int):
+        """Levels with at most `rows` (row, right-hand side) pairs run merged in one CTA."""
+        return self._flag("level_merge", rows)
+
     def mark_A_dirty(self):
         return self._flag("a_dirty", 1)
 
@@ -293,6 +303,45 @@ class Utils:
         return dict(n_rows=nr, n_cols=nc, n_blocks=nb, b_height=bh, b_width=bw, height_pad=hp, width_pad=wp,
                     col=_take(ptrs[0].value, nb, np.int32), row_ptr=_take(ptrs[1].value, nr + 1, np.int32),
                     val=_take(ptrs[2].value, nb * hp * wp, val.dtype))
+
+
+    # -- level sets and permutations (src/utils/permutations.hpp) --------------
+    def build_symmetric_crs(self, row_ptr, col, n_rows):
+        """Pattern of A + A^T: returns (sym_row_ptr, sym_col, sym_nnz)."""
+        row_ptr, col = _i32(row_ptr), _i32(col)
+        pr, pc, nz = C.c_void_p(), C.c_void_p(), C.c_uint64(0)
+        check(lib.smax_utils_build_symmetric_crs(int(IntType.INT32), int(n_rows), _ptr(row_ptr), _ptr(col),
+                                                 C.byref(pr), C.byref(pc), C.byref(nz)))
+        return _take(pr.value, int(n_rows) + 1, np.int32), _take(pc.value, nz.value, np.int32), nz.value
+
+    def generate_perm(self, n_rows, row_ptr, col, perm, inv_perm, type_="BFS"):
+        """Fills perm / inv_perm (int32 arrays of n_rows) and stores the level
+        pointer in the Interface (get_n_levels / get_level_ptr_at)."""
+        for a in (perm, inv_perm):
+            if not (isinstance(a, np.ndarray) and a.dtype == np.int32 and a.flags["C_CONTIGUOUS"]):
+                raise TypeError("perm and inv_perm must be C-contiguous int32 numpy arrays")
+        row_ptr, col = _i32(row_ptr), _i32(col)
+        check(lib.smax_utils_generate_perm(self._iface._ctx, int(IntType.INT32), int(n_rows), _ptr(row_ptr),
+                                           _ptr(col), _ptr(perm), _ptr(inv_perm), type_.encode()))
+
+    def apply_mat_perm(self, n_rows, row_ptr, col, val, perm_row_ptr, perm_col, perm_val, perm, inv_perm):
+        row_ptr, col, perm, inv_perm = _i32(row_ptr), _i32(col), _i32(perm), _i32(inv_perm)
+        val = np.ascontiguousarray(val)
+        check(lib.smax_utils_apply_mat_perm(int(IntType.INT32), _ftype(val.dtype), int(n_rows), _ptr(row_ptr),
+                                            _ptr(col), _ptr(val), _ptr(perm_row_ptr), _ptr(perm_col),
+                                            _ptr(perm_val), _ptr(perm), _ptr(inv_perm)))
+
+    def apply_vec_perm(self, n_rows, vec, vec_perm, perm):
+        perm = _i32(perm)
+        vec = np.ascontiguousarray(vec)
+        check(lib.smax_utils_apply_vec_perm(_ftype(vec.dtype), int(n_rows), _ptr(vec), _ptr(vec_perm), _ptr(perm)))
+
+    def level_aware_copy(self, src_row_ptr, dest_row_ptr, src_col, dest_col, src_val, dest_val):
+        """src/utils/permutations.hpp:876-897: a first-touch (NUMA) copy on the
+        CPU platform; on this platform a plain copy of the three arrays."""
+        dest_row_ptr[...] = src_row_ptr
+        dest_col[...] = src_col
+        dest_val[...] = src_val
 
 
 class Interface:
