@@ -143,6 +143,16 @@ smax_status smax_kernel_register_A_bcrs(smax_kernel k, uint64_t n_rows, uint64_t
                                         uint64_t b_height, uint64_t b_width, uint64_t height_pad,
                                         uint64_t width_pad, void *col, void *row_ptr, void *val);
 
+/* SpGEMM: register_B of the CRS matrix B (src/kernels/spgemm.hpp:51-66) and
+ * register_C of the output references (src/kernels/spgemm.hpp:68-83): after
+ * finalize, *n_rows/*n_cols/*nnz hold C's sizes and *col/*row_ptr/*val point
+ * to new[]-allocated arrays owned by the caller (int32 indices, values of the
+ * kernel's float type), columns of each row in first-touch order. */
+smax_status smax_kernel_register_B_crs(smax_kernel k, uint64_t n_rows, uint64_t n_cols, uint64_t nnz, void *col,
+                                       void *row_ptr, void *val);
+smax_status smax_kernel_register_C_crs_ref(smax_kernel k, uint64_t *n_rows, uint64_t *n_cols, uint64_t *nnz,
+                                           void **col, void **row_ptr, void **val);
+
 /* register_B / register_C of a dense operand: (n_rows, val) for vectors
  * (spmv.hpp:97-115, sptrsv.hpp:40-58) or (n_rows, n_cols, val) for blocks of
  * vectors (spmm.hpp:40-61, sptrsm.hpp:40-60).  slot 1 = B, slot 2 = C. */

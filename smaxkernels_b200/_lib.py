@@ -37,6 +37,8 @@ SIGNATURES = {
     "smax_kernel_register_A_crs": (I32, [P, U64, U64, U64, P, P, P]),
     "smax_kernel_register_A_scs": (I32, [P] + [U64] * 8 + [P] * 5),
     "smax_kernel_register_A_bcrs": (I32, [P] + [U64] * 7 + [P] * 3),
+    "smax_kernel_register_B_crs": (I32, [P, U64, U64, U64, P, P, P]),
+    "smax_kernel_register_C_crs_ref": (I32, [P, PU64, PU64, PU64, PP, PP, PP]),
     "smax_kernel_register_dense": (I32, [P, I32, U64, U64, P]),
     "smax_kernel_initialize": (I32, [P, U64, U64, U64]),
     "smax_kernel_apply": (I32, [P, U64, U64, U64]),

@@ -194,6 +194,41 @@ template <typename VT> void tri_apply_t(smax_kernel_s *k, const VT *Bv, VT *Xv) 
         tri_solve<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, kk, rm, ld, merge, k->stream);
 }
 
+// ------------------------------------------------------------------ SpGEMM --
+void spgemm_upload(smax_kernel_s *k) {
+    require(k->A.set && k->Bm.set, SMAX_ERR_STATE, "register_A and register_B before initialize");
+    require(k->A.n_cols == k->Bm.n_rows, SMAX_ERR_BAD_ARG, "A.n_cols must equal B.n_rows");
+    upload_crs(k->dA, k->A, k->vbytes, k->stream);
+    validate_crs(k->dA, dstatus(k), k->stream);
+    read_status(k);
+    upload_crs(k->dBm, k->Bm, k->vbytes, k->stream);
+    validate_crs(k->dBm, dstatus(k), k->stream);
+    read_status(k);
+}
+
+void spgemm_finalize(smax_kernel_s *k) {
+    // the reference allocates C with new[] and hands it to the caller
+    // (symbolic_phase_impl.hpp:132-151); so does this platform
+    require(k->spgemm_done, SMAX_ERR_STATE, "apply before finalize");
+    const DevCRS &c = k->dCm;
+    int *rp = new int[c.n_rows + 1];
+    int *col = new int[c.nnz > 0 ? c.nnz : 1];
+    void *val = k->vbytes == 8 ? static_cast<void *>(new double[c.nnz > 0 ? c.nnz : 1])
+                               : static_cast<void *>(new float[c.nnz > 0 ? c.nnz : 1]);
+    SMAX_CUDA(cudaMemcpyAsync(rp, c.row_ptr.p, sizeof(int) * (c.n_rows + 1), cudaMemcpyDeviceToHost, k->stream));
+    if (c.nnz) {
+        SMAX_CUDA(cudaMemcpyAsync(col, c.col.p, sizeof(int) * c.nnz, cudaMemcpyDeviceToHost, k->stream));
+        SMAX_CUDA(cudaMemcpyAsync(val, c.val.p, (size_t)k->vbytes * c.nnz, cudaMemcpyDeviceToHost, k->stream));
+    }
+    SMAX_CUDA(cudaStreamSynchronize(k->stream));
+    *k->Cref.n_rows = (uint64_t)c.n_rows;
+    *k->Cref.n_cols = (uint64_t)c.n_cols;
+    *k->Cref.nnz = (uint64_t)c.nnz;
+    *k->Cref.row_ptr = rp;
+    *k->Cref.col = col;
+    *k->Cref.val = val;
+}
+
 // Device addresses of B and C (+ element offsets).
 const void *dev_b(smax_kernel_s *k, uint64_t off) {
     const char *base = k->f_device ? static_cast<const char *>(k->B.val) : static_cast<const char *>(k->dB.p);
@@ -239,6 +274,15 @@ void check_extents(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
 
 void do_initialize(smax_kernel_s *k) {
     double t0 = wall_s();
+    if (k->ktype == SMAX_KERNEL_SPGEMM) {
+        require(k->Cref.set, SMAX_ERR_STATE, "register_C before initialize");
+        if (k->a_dirty) {
+            spgemm_upload(k);
+            k->a_dirty = false;
+        }
+        k->timers["initialize"] += wall_s() - t0;
+        return;
+    }
     require(k->B.set && k->C.set, SMAX_ERR_STATE, "register_B and register_C before initialize");
     if (k->a_dirty) {
         switch (k->ktype) {
@@ -267,6 +311,23 @@ void do_initialize(smax_kernel_s *k) {
 
 void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
     require(!k->a_dirty, SMAX_ERR_STATE, "initialize before apply");
+    if (k->ktype == SMAX_KERNEL_SPGEMM) {
+        // offsets are ignored, as in the reference (src/kernels/spgemm.hpp:108-130)
+        auto ev = k->apply_events.acquire();
+        SMAX_CUDA(cudaEventRecord(ev.first, k->stream));
+        if (k->vbytes == 8) spgemm<double>(k->dA, k->dBm, k->dCm, &k->spgemm_times, k->stream);
+        else spgemm<float>(k->dA, k->dBm, k->dCm, &k->spgemm_times, k->stream);
+        SMAX_CUDA(cudaEventRecord(ev.second, k->stream));
+        const SpgemmTimes &t = k->spgemm_times;
+        k->timers["Symbolic_Setup"] += t.setup;
+        k->timers["Fused_Gustavson"] += t.fused;
+        k->timers["Alloc_C"] += t.alloc;
+        k->timers["Compress"] += t.compress;
+        k->timers["symbolic_phase"] += t.setup + t.alloc;
+        k->timers["numerical_phase"] += t.fused + t.compress;
+        k->spgemm_done = true;
+        return;
+    }
     check_extents(k, b_off, c_off);
     auto ev = k->apply_events.acquire();
     SMAX_CUDA(cudaEventRecord(ev.first, k->stream));
@@ -298,6 +359,12 @@ void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
 
 void do_finalize(smax_kernel_s *k) {
     double t0 = wall_s();
+    if (k->ktype == SMAX_KERNEL_SPGEMM) {
+        spgemm_finalize(k);
+        k->timers["apply"] += k->apply_events.drain();
+        k->timers["finalize"] += wall_s() - t0;
+        return;
+    }
     if (!k->f_device) {
         if (is_tri(k)) {
             size_t bb = (size_t)k->B.elems() * k->vbytes;
@@ -453,6 +520,26 @@ smax_status smax_kernel_register_A_bcrs(smax_kernel k, uint64_t n_rows, uint64_t
         kk->A_bcrs = RegBCRS{true, n_rows, n_cols, n_blocks, b_height, b_width, height_pad, width_pad,
                              col, row_ptr, val};
         kk->a_dirty = true;
+    });
+}
+
+smax_status smax_kernel_register_B_crs(smax_kernel k, uint64_t n_rows, uint64_t n_cols, uint64_t nnz, void *col,
+                                       void *row_ptr, void *val) {
+    return guarded([&] {
+        smax_kernel_s *kk = K(k);
+        require(row_ptr != nullptr, SMAX_ERR_BAD_ARG, "null row_ptr");
+        require(nnz == 0 || (col && val), SMAX_ERR_BAD_ARG, "null col/val");
+        kk->Bm = RegCRS{true, n_rows, n_cols, nnz, col, row_ptr, val};
+        kk->a_dirty = true;
+    });
+}
+
+smax_status smax_kernel_register_C_crs_ref(smax_kernel k, uint64_t *n_rows, uint64_t *n_cols, uint64_t *nnz,
+                                           void **col, void **row_ptr, void **val) {
+    return guarded([&] {
+        smax_kernel_s *kk = K(k);
+        require(n_rows && n_cols && nnz && col && row_ptr && val, SMAX_ERR_BAD_ARG, "null output reference");
+        kk->Cref = RegCRSRef{true, n_rows, n_cols, nnz, col, row_ptr, val};
     });
 }
 

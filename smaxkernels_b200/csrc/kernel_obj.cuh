@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "spmv_crs.cuh"
 #include "spmv_formats.cuh"
+#include "spgemm.cuh"
 #include "sptrsv.cuh"
 
 struct smax_ctx_s {
@@ -45,6 +46,14 @@ struct RegBCRS {
     bool set = false;
     uint64_t n_rows = 0, n_cols = 0, n_blocks = 0, bh = 0, bw = 0, hpad = 0, wpad = 0;
     void *col = nullptr, *row_ptr = nullptr, *val = nullptr;
+};
+
+// register_C of SpGEMM: where the result's sizes and arrays are written
+// (src/kernels/spgemm.hpp:68-83)
+struct RegCRSRef {
+    bool set = false;
+    uint64_t *n_rows = nullptr, *n_cols = nullptr, *nnz = nullptr;
+    void **col = nullptr, **row_ptr = nullptr, **val = nullptr;
 };
 
 struct RegDense {
@@ -84,6 +93,8 @@ struct smax_kernel_s {
     smax::RegSCS A_scs;
     smax::RegBCRS A_bcrs;
     smax::RegDense B, C;
+    smax::RegCRS Bm;       // SpGEMM's B
+    smax::RegCRSRef Cref;  // SpGEMM's C
     bool a_dirty = true;
 
     // device state
@@ -97,6 +108,11 @@ struct smax_kernel_s {
     smax::CrsStreamPlan crs_stream;
     int spmv_variant = 0;  // 0 auto, 1 warp-stream, 2 row-tile
     smax::DevBuf status;   // smax::DevStatus
+
+    // SpGEMM
+    smax::DevCRS dBm, dCm;
+    smax::SpgemmTimes spgemm_times;
+    bool spgemm_done = false;
 
     // triangular solves (SpTRSV / SpTRSM)
     smax::DevBuf D;                 // peeled diagonal

@@ -1,0 +1,349 @@
+// spgemm.cu -- Gustavson SpGEMM C = A*B on sm_100a.
+//
+// Reference semantics (src/kernels/spgemm/spgemm_cpu/): padded_symbolic_phase
+// (symbolic_phase_impl.hpp:9-177) stores each row's distinct columns of B in
+// FIRST-TOUCH order -- the order in which the products (j over A's row, k over
+// B's row col[j]) first reach them; basic_numerical_phase
+// (numerical_phase_impl.hpp:9-91) accumulates every product in that (j, k)
+// order.  C_n_rows = A_n_rows, C_n_cols = B_n_cols.
+//
+// Design.  One fused pass per row of A, binned by its product count P_i:
+//   * P_i <= 256:   one warp, hash table in shared memory (512 slots);
+//   * P_i <= 4096:  one CTA, hash table in shared memory (8192 slots);
+//   * larger:       one CTA, hash table in a global workspace (2*P_i slots).
+// The row's products are visited B-row by B-row in the reference's order; the
+// columns of one B row are distinct, so the lanes of one step never collide
+// and every table slot accumulates its products in (j, k) order --
+// deterministic, and the same summation order as the reference.  A column's
+// slot records the product index p of its first touch; since these indices
+// are distinct, posmap[p] = slot followed by an ordered compaction of posmap
+// yields the columns in first-touch order without a comparison sort.  Each row
+// writes its columns/values at its product offset (an upper bound, as the
+// reference's padded buffer), then a scan of the counts gives C's row_ptr and
+// a compaction pass packs C_col / C_val.
+#include "spgemm.cuh"
+
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
+namespace smax {
+
+namespace {
+
+constexpr int kWarpP = 256, kWarpTS = 512;     // warp path: products, table slots
+constexpr int kCtaP = 4096, kCtaTS = 8192;     // CTA path
+constexpr int kCtaThreads = 512;
+constexpr int kWarpsPerCta = 4;
+
+__device__ __forceinline__ unsigned hash_col(int c) { return (unsigned)c * 0x9E3779B1u; }
+
+// product count of every row of A
+__global__ void row_products(const int *__restrict__ arp, const int *__restrict__ acol, const int *__restrict__ brp,
+                             int64_t n, long long *__restrict__ P) {
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    long long s = 0;
+    for (int j = arp[i] + lane; j < arp[i + 1]; j += 32) {
+        const int c = acol[j];
+        s += brp[c + 1] - brp[c];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) P[i] = s;
+}
+
+__global__ void bin_flags(const long long *__restrict__ P, int64_t n, unsigned char *__restrict__ fw,
+                          unsigned char *__restrict__ fc, unsigned char *__restrict__ fg) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long p = P[i];
+    fw[i] = p <= kWarpP;
+    fc[i] = p > kWarpP && p <= kCtaP;
+    fg[i] = p > kCtaP;
+}
+
+// The body shared by all three paths: a team of `tsize` threads (`t` its
+// rank) fills a table of `TS` slots for row i.  sync() orders the steps.
+template <typename VT, typename Sync>
+__device__ __forceinline__ void gustavson_row(int i, int t, int tsize, const int *__restrict__ arp,
+                                              const int *__restrict__ acol, const VT *__restrict__ aval,
+                                              const int *__restrict__ brp, const int *__restrict__ bcol,
+                                              const VT *__restrict__ bval, int *keys, int *first, VT *vals,
+                                              int *posmap, unsigned TS, long long P, long long out_off,
+                                              int *__restrict__ pcol, VT *__restrict__ pval, int *__restrict__ count,
+                                              Sync sync) {
+    for (unsigned h = t; h < TS; h += tsize) {
+        keys[h] = -1;
+        vals[h] = VT(0);
+    }
+    for (long long q = t; q < P; q += tsize) posmap[q] = -1;
+    sync();
+    long long base = 0;  // product index of the first product of the current B row
+    for (int j = arp[i]; j < arp[i + 1]; ++j) {
+        const int c = acol[j];
+        const VT av = aval[j];
+        const int bs = brp[c], be = brp[c + 1];
+        for (int k = bs + t; k < be; k += tsize) {
+            const int col = bcol[k];
+            const VT prod = av * bval[k];
+            unsigned h = hash_col(col) & (TS - 1);
+            while (true) {
+                const int old = atomicCAS(keys + h, -1, col);
+                if (old == -1) {
+                    first[h] = (int)(base + (k - bs));
+                    break;
+                }
+                if (old == col) break;
+                h = (h + 1) & (TS - 1);
+            }
+            vals[h] += prod;  // one product per slot per step: the (j, k) order
+        }
+        base += be - bs;
+        sync();
+    }
+    for (unsigned h = t; h < TS; h += tsize)
+        if (keys[h] != -1) posmap[first[h]] = (int)h;
+    sync();
+    // ordered compaction of posmap: entries in first-touch order
+    __shared__ int team_total[kCtaThreads / 32];
+    int written = 0;
+    for (long long q0 = 0; q0 < P; q0 += tsize) {
+        const long long q = q0 + t;
+        const int h = q < P ? posmap[q] : -1;
+        const int take = h >= 0;
+        // team-wide exclusive scan of `take` (warp ballots, then warps in order)
+        const unsigned bal = __ballot_sync(0xffffffffu, take);
+        const int lane = t & 31, warp = t >> 5;
+        const int before_in_warp = __popc(bal & ((1u << lane) - 1u));
+        int before = before_in_warp, total = __popc(bal);
+        if (tsize > 32) {
+            if (lane == 0) team_total[warp] = total;
+            sync();
+            before = before_in_warp;
+            total = 0;
+            for (int w = 0; w < tsize / 32; ++w) {
+                if (w < warp) before += team_total[w];
+                total += team_total[w];
+            }
+            sync();
+        }
+        if (take) {
+            pcol[out_off + written + before] = keys[h];
+            pval[out_off + written + before] = vals[h];
+        }
+        written += total;
+    }
+    if (t == 0) count[i] = written;
+}
+
+struct WarpSync {
+    __device__ void operator()() const { __syncwarp(); }
+};
+struct CtaSync {
+    __device__ void operator()() const { __syncthreads(); }
+};
+
+template <typename VT>
+__global__ void __launch_bounds__(kWarpsPerCta * 32) gustavson_warp(
+    const int *__restrict__ rows, int n_rows_bin, const long long *__restrict__ P, const long long *__restrict__ Poff,
+    const int *__restrict__ arp, const int *__restrict__ acol, const VT *__restrict__ aval,
+    const int *__restrict__ brp, const int *__restrict__ bcol, const VT *__restrict__ bval, int *__restrict__ pcol,
+    VT *__restrict__ pval, int *__restrict__ count) {
+    __shared__ int keys[kWarpsPerCta][kWarpTS];
+    __shared__ int first[kWarpsPerCta][kWarpTS];
+    __shared__ VT vals[kWarpsPerCta][kWarpTS];
+    __shared__ int posmap[kWarpsPerCta][kWarpP];
+    const int w = threadIdx.x >> 5;
+    const int64_t r = (int64_t)blockIdx.x * kWarpsPerCta + w;
+    if (r >= n_rows_bin) return;  // uniform per warp; the warp path never touches CTA barriers
+    const int i = rows[r];
+    gustavson_row<VT>(i, threadIdx.x & 31, 32, arp, acol, aval, brp, bcol, bval, keys[w], first[w], vals[w],
+                      posmap[w], kWarpTS, P[i], Poff[i], pcol, pval, count, WarpSync());
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(kCtaThreads) gustavson_cta(
+    const int *__restrict__ rows, int n_rows_bin, const long long *__restrict__ P, const long long *__restrict__ Poff,
+    const int *__restrict__ arp, const int *__restrict__ acol, const VT *__restrict__ aval,
+    const int *__restrict__ brp, const int *__restrict__ bcol, const VT *__restrict__ bval, int *__restrict__ pcol,
+    VT *__restrict__ pval, int *__restrict__ count) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    VT *vals = reinterpret_cast<VT *>(smem);
+    int *keys = reinterpret_cast<int *>(vals + kCtaTS);
+    int *first = keys + kCtaTS;
+    int *posmap = first + kCtaTS;
+    const int i = rows[blockIdx.x];
+    gustavson_row<VT>(i, threadIdx.x, kCtaThreads, arp, acol, aval, brp, bcol, bval, keys, first, vals, posmap,
+                      kCtaTS, P[i], Poff[i], pcol, pval, count, CtaSync());
+}
+
+// rows with more than kCtaP products: tables in a global workspace
+template <typename VT>
+__global__ void __launch_bounds__(kCtaThreads) gustavson_global(
+    const int *__restrict__ rows, const long long *__restrict__ ws_off, const unsigned *__restrict__ ws_ts,
+    const long long *__restrict__ P, const long long *__restrict__ Poff, const int *__restrict__ arp,
+    const int *__restrict__ acol, const VT *__restrict__ aval, const int *__restrict__ brp,
+    const int *__restrict__ bcol, const VT *__restrict__ bval, int *__restrict__ pcol, VT *__restrict__ pval,
+    int *__restrict__ count, int *ws_keys, int *ws_first, VT *ws_vals, int *ws_pos) {
+    const int b = blockIdx.x;
+    const int i = rows[b];
+    const long long o = ws_off[b];
+    gustavson_row<VT>(i, threadIdx.x, kCtaThreads, arp, acol, aval, brp, bcol, bval, ws_keys + o, ws_first + o,
+                      ws_vals + o, ws_pos + Poff[i], ws_ts[b], P[i], Poff[i], pcol, pval, count, CtaSync());
+}
+
+__global__ void ws_sizes(const int *__restrict__ rows, int m, const long long *__restrict__ P,
+                         unsigned *__restrict__ ts, long long *__restrict__ sz) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= m) return;
+    unsigned t = 1;
+    while ((long long)t < 2 * P[rows[b]]) t <<= 1;
+    ts[b] = t;
+    sz[b] = t;
+}
+
+template <typename VT>
+__global__ void compact_kernel(const int *__restrict__ crp, const long long *__restrict__ Poff, int64_t n,
+                               const int *__restrict__ pcol, const VT *__restrict__ pval, int *__restrict__ ccol,
+                               VT *__restrict__ cval) {
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const int s = crp[i], len = crp[i + 1] - s;
+    const long long o = Poff[i];
+    for (int t = lane; t < len; t += 32) {
+        ccol[s + t] = pcol[o + t];
+        cval[s + t] = pval[o + t];
+    }
+}
+
+template <typename T> void excl_scan(const T *in, T *out, int64_t n, cudaStream_t st) {
+    SMAX_CUDA(cudaMemsetAsync(out, 0, sizeof(T), st));
+    if (n == 0) return;
+    size_t tb = 0;
+    SMAX_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, in, out + 1, (int)n, st));
+    DevBuf tmp(tb);
+    SMAX_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tb, in, out + 1, (int)n, st));
+}
+
+int select_rows(const unsigned char *flags, int64_t n, DevBuf &out, DevBuf &cnt, cudaStream_t st) {
+    out.alloc(sizeof(int) * (n ? n : 1));
+    thrust::counting_iterator<int> it(0);
+    size_t tb = 0;
+    SMAX_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, it, flags, out.as<int>(), cnt.as<int>(), (int)n, st));
+    DevBuf tmp(tb);
+    SMAX_CUDA(cub::DeviceSelect::Flagged(tmp.p, tb, it, flags, out.as<int>(), cnt.as<int>(), (int)n, st));
+    int h = 0;
+    SMAX_CUDA(cudaMemcpyAsync(&h, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SMAX_CUDA(cudaStreamSynchronize(st));
+    return h;
+}
+
+}  // namespace
+
+template <typename VT>
+void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmTimes *times, cudaStream_t st) {
+    if (A.n_cols != B.n_rows) fail(SMAX_ERR_BAD_ARG, "A.n_cols must equal B.n_rows");
+    const int64_t n = A.n_rows;
+    C.n_rows = n;
+    C.n_cols = B.n_cols;
+    C.row_ptr.alloc(sizeof(int) * (n + 1));
+    cudaEvent_t ev[5];
+    for (auto &e : ev) SMAX_CUDA(cudaEventCreate(&e));
+    SMAX_CUDA(cudaEventRecord(ev[0], st));
+    // --- setup: product counts, their offsets, row bins
+    DevBuf P(sizeof(long long) * (n ? n : 1)), Poff(sizeof(long long) * (n + 1));
+    if (n > 0) {
+        row_products<<<ceil_div_u((uint64_t)n * 32, 256), 256, 0, st>>>(A.rp(), A.ci(), B.rp(), n, P.as<long long>());
+        SMAX_CUDA(cudaGetLastError());
+    }
+    excl_scan<long long>(P.as<long long>(), Poff.as<long long>(), n, st);
+    long long total_p = 0;
+    SMAX_CUDA(cudaMemcpyAsync(&total_p, Poff.as<long long>() + n, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    DevBuf fw(n ? n : 1), fc(n ? n : 1), fg(n ? n : 1), cnt(sizeof(int)), rw, rc, rg;
+    if (n > 0) {
+        bin_flags<<<ceil_div_u(n, 256), 256, 0, st>>>(P.as<long long>(), n, fw.as<unsigned char>(),
+                                                       fc.as<unsigned char>(), fg.as<unsigned char>());
+        SMAX_CUDA(cudaGetLastError());
+    }
+    const int nw = n ? select_rows(fw.as<unsigned char>(), n, rw, cnt, st) : 0;
+    const int nc = n ? select_rows(fc.as<unsigned char>(), n, rc, cnt, st) : 0;
+    const int ng = n ? select_rows(fg.as<unsigned char>(), n, rg, cnt, st) : 0;
+    SMAX_CUDA(cudaStreamSynchronize(st));
+    SMAX_CUDA(cudaEventRecord(ev[1], st));
+    // --- fused Gustavson pass into product-offset (padded) buffers
+    DevBuf pcol(sizeof(int) * (total_p ? total_p : 1)), pval(sizeof(VT) * (total_p ? total_p : 1));
+    DevBuf count(sizeof(int) * (n ? n : 1));
+    if (nw > 0)
+        gustavson_warp<VT><<<ceil_div_u(nw, kWarpsPerCta), kWarpsPerCta * 32, 0, st>>>(
+            rw.as<int>(), nw, P.as<long long>(), Poff.as<long long>(), A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(),
+            B.val.as<VT>(), pcol.as<int>(), pval.as<VT>(), count.as<int>());
+    if (nc > 0) {
+        const size_t sm = (size_t)kCtaTS * (sizeof(VT) + 2 * sizeof(int)) + sizeof(int) * kCtaP;
+        SMAX_CUDA(cudaFuncSetAttribute(gustavson_cta<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        gustavson_cta<VT><<<nc, kCtaThreads, sm, st>>>(rc.as<int>(), nc, P.as<long long>(), Poff.as<long long>(),
+                                                       A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(),
+                                                       pcol.as<int>(), pval.as<VT>(), count.as<int>());
+    }
+    DevBuf wts, wsz, woff, wkeys, wfirst, wvals, wpos;
+    if (ng > 0) {
+        wts.alloc(sizeof(unsigned) * ng);
+        wsz.alloc(sizeof(long long) * ng);
+        woff.alloc(sizeof(long long) * (ng + 1));
+        ws_sizes<<<ceil_div_u(ng, 256), 256, 0, st>>>(rg.as<int>(), ng, P.as<long long>(), wts.as<unsigned>(),
+                                                      wsz.as<long long>());
+        SMAX_CUDA(cudaGetLastError());
+        excl_scan<long long>(wsz.as<long long>(), woff.as<long long>(), ng, st);
+        long long wtot = 0;
+        SMAX_CUDA(cudaMemcpyAsync(&wtot, woff.as<long long>() + ng, sizeof(long long), cudaMemcpyDeviceToHost, st));
+        SMAX_CUDA(cudaStreamSynchronize(st));
+        wkeys.alloc(sizeof(int) * wtot);
+        wfirst.alloc(sizeof(int) * wtot);
+        wvals.alloc(sizeof(VT) * wtot);
+        wpos.alloc(sizeof(int) * total_p);
+        gustavson_global<VT><<<ng, kCtaThreads, 0, st>>>(rg.as<int>(), woff.as<long long>(), wts.as<unsigned>(),
+                                                         P.as<long long>(), Poff.as<long long>(), A.rp(), A.ci(),
+                                                         A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(),
+                                                         pcol.as<int>(), pval.as<VT>(), count.as<int>(),
+                                                         wkeys.as<int>(), wfirst.as<int>(), wvals.as<VT>(),
+                                                         wpos.as<int>());
+    }
+    SMAX_CUDA(cudaGetLastError());
+    SMAX_CUDA(cudaEventRecord(ev[2], st));
+    // --- C's row pointer and arrays
+    excl_scan<int>(count.as<int>(), C.row_ptr.as<int>(), n, st);
+    int nnz = 0;
+    SMAX_CUDA(cudaMemcpyAsync(&nnz, C.row_ptr.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SMAX_CUDA(cudaStreamSynchronize(st));
+    C.nnz = nnz;
+    C.col.alloc(sizeof(int) * (nnz ? nnz : 1));
+    C.val.alloc(sizeof(VT) * (nnz ? nnz : 1));
+    SMAX_CUDA(cudaEventRecord(ev[3], st));
+    if (n > 0) {
+        compact_kernel<VT><<<ceil_div_u((uint64_t)n * 32, 256), 256, 0, st>>>(
+            C.rp(), Poff.as<long long>(), n, pcol.as<int>(), pval.as<VT>(), C.col.as<int>(), C.val.as<VT>());
+        SMAX_CUDA(cudaGetLastError());
+    }
+    SMAX_CUDA(cudaEventRecord(ev[4], st));
+    SMAX_CUDA(cudaStreamSynchronize(st));
+    if (times) {
+        float a = 0, b = 0, c = 0, d = 0;
+        cudaEventElapsedTime(&a, ev[0], ev[1]);
+        cudaEventElapsedTime(&b, ev[1], ev[2]);
+        cudaEventElapsedTime(&c, ev[2], ev[3]);
+        cudaEventElapsedTime(&d, ev[3], ev[4]);
+        times->setup = a * 1e-3;
+        times->fused = b * 1e-3;
+        times->alloc = c * 1e-3;
+        times->compress = d * 1e-3;
+        times->products = total_p;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+}
+
+template void spgemm<double>(const DevCRS &, const DevCRS &, DevCRS &, SpgemmTimes *, cudaStream_t);
+template void spgemm<float>(const DevCRS &, const DevCRS &, DevCRS &, SpgemmTimes *, cudaStream_t);
+
+}  // namespace smax

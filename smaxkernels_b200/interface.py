@@ -153,10 +153,36 @@ class Kernel:
         return 0
 
     def register_B(self, *args):
+        if self.kernel_type == KernelType.SPGEMM:
+            if len(args) != 6:
+                raise RuntimeError("SpGEMMKernel register_B expects 6 args")
+            n_rows, n_cols, nnz, col, row_ptr, val = args
+            self._keep["B"] = (col, row_ptr, val)
+            check(lib.smax_kernel_register_B_crs(self._h, int(n_rows), int(n_cols), int(nnz), _ptr(col),
+                                                 _ptr(row_ptr), _ptr(val)))
+            return 0
         return self._register_dense(1, args)
 
     def register_C(self, *args):
+        if self.kernel_type == KernelType.SPGEMM:
+            if len(args) != 0:
+                raise RuntimeError("SpGEMMKernel register_C takes no arguments here: read the result with "
+                                   "result() after run(); the references are owned by the kernel")
+            self._cref = [C.c_uint64(0), C.c_uint64(0), C.c_uint64(0), C.c_void_p(), C.c_void_p(), C.c_void_p()]
+            r = self._cref
+            check(lib.smax_kernel_register_C_crs_ref(self._h, C.byref(r[0]), C.byref(r[1]), C.byref(r[2]),
+                                                     C.byref(r[3]), C.byref(r[4]), C.byref(r[5])))
+            return 0
         return self._register_dense(2, args)
+
+    def result(self):
+        """SpGEMM: C as (n_rows, n_cols, nnz, row_ptr, col, val) numpy copies of
+        the arrays finalize() allocated (which are then released)."""
+        r = self._cref
+        n_rows, n_cols, nnz = r[0].value, r[1].value, r[2].value
+        vt = np.float64 if self.float_type == FloatType.FLOAT64 else np.float32
+        return (n_rows, n_cols, nnz, _take(r[4].value, n_rows + 1, np.int32), _take(r[3].value, nnz, np.int32),
+                _take(r[5].value, nnz, vt))
 
     # -- flags ------------------------------------------------------------
     def _flag(self, name, v):

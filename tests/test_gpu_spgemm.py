@@ -1,0 +1,88 @@
+"""Parity of the GPU Gustavson SpGEMM with the oracle and the reference's golden
+vectors: C's pattern (row_ptr and the FIRST-TOUCH column order in each row) is
+bit-exact, values within the normwise tolerance."""
+import numpy as np
+import pytest
+
+import golden_cases as G
+from helpers import normwise, rand_crs, tol
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+O = Oracle()
+
+
+def gpu_spgemm(A, B, a_n_cols, b_n_cols):
+    from smaxkernels_b200 import FloatType, Interface, IntType, KernelType, PlatformType
+    (arp, acol, aval), (brp, bcol, bval) = A, B
+    ft = FloatType.FLOAT32 if aval.dtype == np.float32 else FloatType.FLOAT64
+    smax = Interface()
+    smax.register_kernel("g", KernelType.SPGEMM, PlatformType.CUDA, IntType.INT32, ft)
+    k = smax.kernel("g")
+    k.register_A(len(arp) - 1, a_n_cols, len(acol), acol.astype(np.int32), arp.astype(np.int32), aval)
+    k.register_B(len(brp) - 1, b_n_cols, len(bcol), bcol.astype(np.int32), brp.astype(np.int32), bval)
+    k.register_C()
+    k.run()
+    res = k.result()
+    smax.close()
+    return res
+
+
+@pytest.mark.parametrize("name", ["spgemmAA_test", "spgemmAB_test"])
+def test_spgemm_golden(name):
+    """spgemmAA_test uses uint16 indices in the reference; this platform runs
+    int32 indices, the pattern and values are the same."""
+    c = G.spgemm_case(name)
+    n_rows, n_cols, nnz, rp, col, val = gpu_spgemm(c["A"], c["B"], c["b_n_cols"], c["b_n_cols"])
+    assert (n_rows, n_cols, nnz) == (len(c["C"][0]) - 1, c["b_n_cols"], len(c["C"][1]))
+    np.testing.assert_array_equal(rp, c["C"][0])
+    np.testing.assert_array_equal(col, c["C"][1])
+    assert G.almost_equal(val, c["C"][2], np.float32)
+
+
+@pytest.mark.parametrize("vt", [np.float64, np.float32])
+@pytest.mark.parametrize("shape", ["square", "rect", "empty_rows"])
+def test_spgemm_random_vs_oracle(vt, shape):
+    if shape == "square":
+        A = rand_crs(2000, 12, 101, vt=vt)
+        B = rand_crs(2000, 12, 102, vt=vt)
+        a_nc, b_nc = 2000, 2000
+    elif shape == "rect":
+        A = rand_crs(1500, 10, 103, vt=vt, n_cols=800)
+        B = rand_crs(800, 15, 104, vt=vt, n_cols=3000)
+        a_nc, b_nc = 800, 3000
+    else:
+        A = rand_crs(2000, 8, 105, vt=vt, empty_frac=0.5)
+        B = rand_crs(2000, 8, 106, vt=vt, empty_frac=0.5)
+        a_nc, b_nc = 2000, 2000
+    n_rows, n_cols, nnz, rp, col, val = gpu_spgemm(A, B, a_nc, b_nc)
+    orp, ocol, oval = O.spgemm(*A, *B, b_nc)
+    assert (n_rows, n_cols) == (len(A[0]) - 1, b_nc)
+    np.testing.assert_array_equal(rp, orp)
+    np.testing.assert_array_equal(col, ocol)
+    assert normwise(val, oval) <= tol(vt)
+
+
+@pytest.mark.parametrize("maxlen", [40, 90, 300])
+def test_spgemm_heavy_rows(maxlen):
+    """Rows with hundreds to tens of thousands of products: the CTA and the
+    global-workspace paths."""
+    A = rand_crs(600, maxlen, 111, long_rows=(590, 599))
+    B = rand_crs(600, maxlen, 112, long_rows=(580,))
+    n_rows, n_cols, nnz, rp, col, val = gpu_spgemm(A, B, 600, 600)
+    orp, ocol, oval = O.spgemm(*A, *B, 600)
+    np.testing.assert_array_equal(rp, orp)
+    np.testing.assert_array_equal(col, ocol)
+    assert normwise(val, oval) <= 1e-12
+
+
+@pytest.mark.slow
+def test_spgemm_config2_laplace96():
+    from smaxkernels_b200 import matrices as M
+    A = M.laplace3d_7pt(96)
+    n_rows, n_cols, nnz, rp, col, val = gpu_spgemm(A, A, 96 ** 3, 96 ** 3)
+    orp, ocol, oval = O.spgemm(*A, *A, 96 ** 3)
+    assert nnz == 21_732_480
+    np.testing.assert_array_equal(rp, orp)
+    np.testing.assert_array_equal(col, ocol)
+    assert normwise(val, oval) <= 1e-12
