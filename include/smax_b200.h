@@ -90,12 +90,15 @@ typedef int smax_status;
 #define SMAX_FLAG_SPMV_VARIANT 10      /* CRS SpMV kernel: 0 auto, 1 warp-stream, 2 row-tile */
 #define SMAX_FLAG_SOLVE_MODE 11        /* SpTRSV/SpTRSM launch scheme, one of SMAX_SOLVE_* */
 #define SMAX_FLAG_LEVEL_MERGE 12       /* levels with <= this many rows*rhs run merged in one CTA (0: never) */
+#define SMAX_FLAG_SPIN_LIMIT 13        /* polls (x 1000) before a persistent solve's grid barrier times out */
+#define SMAX_FLAG_TEST_FORCE_TIMEOUT 14 /* test only: the persistent solve's barrier waits for a missing arrival */
 
 /* SpTRSV / SpTRSM launch schemes (SMAX_FLAG_SOLVE_MODE) */
 #define SMAX_SOLVE_AUTO 0        /* graph-captured, narrow levels merged (the default) */
 #define SMAX_SOLVE_PER_LEVEL 1   /* one kernel launch per level, no merging, no graph */
 #define SMAX_SOLVE_MERGED 2      /* narrow levels merged into single-CTA runs, no graph */
 #define SMAX_SOLVE_GRAPH 3       /* the merged launch sequence captured into a CUDA graph */
+#define SMAX_SOLVE_PERSISTENT 4  /* one cooperative launch, bounded grid barrier per level (SpTRSV, k = 1) */
 
 typedef struct smax_ctx_s *smax_ctx;
 typedef struct smax_kernel_s *smax_kernel;
@@ -183,6 +186,27 @@ void *smax_kernel_stream(smax_kernel k);
  * current stream of a framework) instead of its own; NULL restores its own.
  * The caller keeps ownership of the stream. */
 smax_status smax_kernel_set_stream(smax_kernel k, void *stream);
+
+/* -------------------------------------------------------- batched SpTRSV */
+/* A batch of independent lower-triangular CRS matrices (host arrays, each with
+ * its diagonal; no counterpart in the reference, which solves one matrix per
+ * kernel) solved together: one persistent kernel whose CTAs take matrices from
+ * a device work queue (longest critical path first) and sweep each matrix's
+ * dependency levels with the CTA barrier as the level barrier.  The batch owns
+ * device copies; the caller's arrays are not modified. */
+typedef struct smax_batch_s *smax_batch;
+smax_status smax_batch_sptrsv_create(smax_batch *out, int float_type, int n_mats, const uint64_t *n_rows,
+                                     const uint64_t *nnz, void *const *row_ptr, void *const *col, void *const *val);
+/* rhs and x are DEVICE arrays of the packed rows (matrix m at row offset
+ * smax_batch_row_offset(b, m)); mode: SMAX_SOLVE_GRAPH (persistent kernel
+ * replayed from a CUDA graph), SMAX_SOLVE_MERGED (persistent kernel, direct
+ * launch) or SMAX_SOLVE_PER_LEVEL (one launch per level of every matrix, the
+ * plain baseline).  stream: a cudaStream_t (NULL = legacy default stream). */
+smax_status smax_batch_sptrsv_solve(smax_batch b, const void *rhs, void *x, int mode, void *stream);
+uint64_t smax_batch_row_offset(smax_batch b, int m);
+/* total packed rows, sum of the matrices' level counts, largest level count */
+smax_status smax_batch_info(smax_batch b, uint64_t *n_rows, int *total_levels, int *max_levels);
+smax_status smax_batch_destroy(smax_batch b);
 
 /* ------------------------------------------------------------------ utils */
 /* Utils::convert_crs_to_scs (src/utils/convert_formats.hpp:16-132), computed on

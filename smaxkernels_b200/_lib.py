@@ -48,6 +48,11 @@ SIGNATURES = {
     "smax_kernel_get_timer": (I32, [P, C.c_char_p, C.POINTER(C.c_double)]),
     "smax_kernel_stream": (P, [P]),
     "smax_kernel_set_stream": (I32, [P, P]),
+    "smax_batch_sptrsv_create": (I32, [PP, I32, I32, PU64, PU64, PP, PP, PP]),
+    "smax_batch_sptrsv_solve": (I32, [P, P, P, I32, P]),
+    "smax_batch_row_offset": (U64, [P, I32]),
+    "smax_batch_info": (I32, [P, PU64, C.POINTER(I32), C.POINTER(I32)]),
+    "smax_batch_destroy": (I32, [P]),
     "smax_utils_convert_crs_to_scs": (I32, [I32, I32, U64, U64, U64, P, P, P, U64, U64, PU64] + [PP] * 5),
     "smax_utils_convert_crs_to_bcrs": (I32, [I32, I32, U64, U64, U64, P, P, P, U64, U64, U64, U64, I32, PU64]
                                        + [PP] * 3),

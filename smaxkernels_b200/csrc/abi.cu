@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "kernel_obj.cuh"
+#include "sptrsv_batch.cuh"
 
 smax_kernel_s::~smax_kernel_s() {
     if (stream) cudaStreamSynchronize(stream);
@@ -188,6 +189,12 @@ template <typename VT> void tri_apply_t(smax_kernel_s *k, const VT *Bv, VT *Xv) 
     const int64_t ld = k->dA.n_rows;  // column-major blocks use A's n_rows (sptrsm_cpu_crs_impl.hpp:44-50)
     const int merge = k->solve_mode == SMAX_SOLVE_PER_LEVEL ? 0
                       : (k->level_merge >= 0 ? k->level_merge : kDefaultLevelMerge);
+    if (k->solve_mode == SMAX_SOLVE_PERSISTENT) {
+        require(kk == 1, SMAX_ERR_UNSUPPORTED, "the persistent solve handles one right-hand side");
+        tri_solve_persistent<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, dstatus(k), k->persist_scratch,
+                                 k->force_timeout, k->spin_limit, k->stream);
+        return;
+    }
     if (k->solve_mode == SMAX_SOLVE_AUTO || k->solve_mode == SMAX_SOLVE_GRAPH)
         tri_solve_graph<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, kk, rm, ld, merge, k->stream);
     else
@@ -472,8 +479,14 @@ smax_status smax_kernel_set_flag(smax_kernel k, int flag, int value) {
             if (value != kk->spmv_variant) kk->a_dirty = true;  // plans differ per variant
             kk->spmv_variant = value;
             break;
+        case SMAX_FLAG_SPIN_LIMIT:
+            require(value > 0, SMAX_ERR_BAD_ARG, "spin limit must be positive");
+            kk->spin_limit = (long long)value * 1000;
+            break;
+        case SMAX_FLAG_TEST_FORCE_TIMEOUT: kk->force_timeout = v; break;
         case SMAX_FLAG_SOLVE_MODE:
-            require(value >= SMAX_SOLVE_AUTO && value <= SMAX_SOLVE_GRAPH, SMAX_ERR_BAD_ARG, "unknown solve mode");
+            require(value >= SMAX_SOLVE_AUTO && value <= SMAX_SOLVE_PERSISTENT, SMAX_ERR_BAD_ARG,
+                    "unknown solve mode");
             kk->solve_mode = value;
             break;
         case SMAX_FLAG_LEVEL_MERGE:

@@ -121,6 +121,9 @@ struct smax_kernel_s {
     uint64_t tri_levels_version = 0;
     int solve_mode = 0;             // SMAX_SOLVE_*
     int level_merge = -1;           // rows*k of levels merged into one-CTA runs; -1 = default
+    bool force_timeout = false;     // test knob of the persistent solve's grid barrier
+    long long spin_limit = 20000000; // polls before a grid barrier gives up
+    smax::DevBuf persist_scratch;
 
     // stopwatches
     std::map<std::string, double> timers;

@@ -63,9 +63,9 @@ class SpMVType(enum.IntEnum):
 
 FLAG = dict(mat_perm=0, mat_upper_triang=1, mat_lower_triang=2, vec_row_major=3, mat_scs=4, mat_bcrs=5,
             block_column_major=6, kernel_impl=7, device_pointers=8, a_dirty=9,
-            spmv_variant=10, solve_mode=11, level_merge=12)
+            spmv_variant=10, solve_mode=11, level_merge=12, spin_limit=13, test_force_timeout=14)
 
-SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED, SOLVE_GRAPH = 0, 1, 2, 3
+SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED, SOLVE_GRAPH, SOLVE_PERSISTENT = 0, 1, 2, 3, 4
 
 
 def _is_torch_cuda(a) -> bool:
@@ -223,6 +223,10 @@ class Kernel:
         """SpTRSV/SpTRSM launch scheme: SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED or SOLVE_GRAPH."""
         return self._flag("solve_mode", mode)
 
+    def set_spin_limit(self, kilo_polls: int):
+        """Polls (x 1000) before a persistent solve's grid barrier gives up with TIMEOUT."""
+        return self._flag("spin_limit", kilo_polls)
+
     def set_level_merge(self, rows: int):
         """Levels with at most `rows` (row, right-hand side) pairs run merged in one CTA."""
         return self._flag("level_merge", rows)
@@ -267,6 +271,49 @@ class Kernel:
         if self._h:
             lib.smax_kernel_destroy(self._h)
             self._h = None
+
+
+class TriangularBatch:
+    """Batched SpTRSV over independent lower-triangular matrices (C ABI
+    smax_batch_sptrsv_*): one persistent kernel with a device work queue."""
+
+    def __init__(self, mats, float_type: FloatType = FloatType.FLOAT64):
+        """mats: list of (row_ptr, col, val) numpy CRS arrays (square, with diagonal)."""
+        n = len(mats)
+        self._keep = [(_i32(rp), _i32(c), np.ascontiguousarray(v)) for rp, c, v in mats]
+        nr = (C.c_uint64 * n)(*[len(m[0]) - 1 for m in self._keep])
+        nz = (C.c_uint64 * n)(*[len(m[1]) for m in self._keep])
+        rps = (C.c_void_p * n)(*[m[0].ctypes.data for m in self._keep])
+        cls = (C.c_void_p * n)(*[m[1].ctypes.data for m in self._keep])
+        vls = (C.c_void_p * n)(*[m[2].ctypes.data for m in self._keep])
+        h = C.c_void_p()
+        check(lib.smax_batch_sptrsv_create(C.byref(h), int(float_type), n, nr, nz, rps, cls, vls))
+        self._h = h
+        self.n_mats = n
+
+    def row_offset(self, m: int) -> int:
+        return int(lib.smax_batch_row_offset(self._h, m))
+
+    def info(self):
+        nr, tl, ml = C.c_uint64(0), C.c_int(0), C.c_int(0)
+        check(lib.smax_batch_info(self._h, C.byref(nr), C.byref(tl), C.byref(ml)))
+        return nr.value, tl.value, ml.value
+
+    def solve(self, rhs, x, mode: int = 0, stream: int = 0):
+        """rhs, x: CUDA tensors of the packed rows."""
+        check(lib.smax_batch_sptrsv_solve(self._h, _ptr(rhs), _ptr(x), int(mode),
+                                          C.c_void_p(stream) if stream else None))
+
+    def close(self):
+        if self._h:
+            lib.smax_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _i32(a):
