@@ -252,7 +252,10 @@ def main():
     k.register_A(N_ROWS, n_cols, nnz, col, rp, val)
     k.register_B(n_cols, x_glob)
     k.register_C(N_ROWS, y)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the kernels, the all-gather and the timing events
+    # all run on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     k.set_stream(stream.cuda_stream)
     k.initialize()
     torch.cuda.synchronize()

@@ -320,6 +320,7 @@ void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
     require(!k->a_dirty, SMAX_ERR_STATE, "initialize before apply");
     if (k->ktype == SMAX_KERNEL_SPGEMM) {
         // offsets are ignored, as in the reference (src/kernels/spgemm.hpp:108-130)
+        k->timers["apply"] += k->apply_events.trim(512);
         auto ev = k->apply_events.acquire();
         SMAX_CUDA(cudaEventRecord(ev.first, k->stream));
         if (k->vbytes == 8) spgemm<double>(k->dA, k->dBm, k->dCm, &k->spgemm_times, k->stream);
@@ -336,6 +337,7 @@ void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
         return;
     }
     check_extents(k, b_off, c_off);
+    k->timers["apply"] += k->apply_events.trim(512);
     auto ev = k->apply_events.acquire();
     SMAX_CUDA(cudaEventRecord(ev.first, k->stream));
     const void *b = dev_b(k, b_off);

@@ -106,6 +106,45 @@ inline unsigned ceil_div_u(uint64_t a, uint64_t b) { return (unsigned)((a + b - 
 // number of SMs of the current device (148 on B200), cached per device
 int sm_count();
 
+// The legacy default stream (NULL / cudaStreamLegacy) and the per-thread
+// default stream cannot be captured into a CUDA graph.
+inline bool is_capturable(cudaStream_t s) {
+    return s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread;
+}
+
+// A private stream fenced to a caller's stream with events: work issued on it
+// between enter() and leave() is ordered after everything queued on the
+// caller's stream before enter() and before everything queued after leave().
+struct AuxStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t in = nullptr, out = nullptr;
+    cudaStream_t enter(cudaStream_t caller) {
+        if (!s) {
+            cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+            cuda_check(cudaEventCreateWithFlags(&in, cudaEventDisableTiming), "cudaEventCreate");
+            cuda_check(cudaEventCreateWithFlags(&out, cudaEventDisableTiming), "cudaEventCreate");
+        }
+        cuda_check(cudaEventRecord(in, caller), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(s, in, 0), "cudaStreamWaitEvent");
+        return s;
+    }
+    void leave(cudaStream_t caller) {
+        cuda_check(cudaEventRecord(out, s), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(caller, out, 0), "cudaStreamWaitEvent");
+    }
+    AuxStream() = default;
+    AuxStream(const AuxStream &) = delete;
+    AuxStream &operator=(const AuxStream &) = delete;
+    ~AuxStream() {
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+        if (in) cudaEventDestroy(in);
+        if (out) cudaEventDestroy(out);
+    }
+};
+
 // ----------------------------------------------------- cache-hinted loads --
 // Matrix streams are read exactly once per product: load them with the
 // streaming (evict-first) hint so they do not displace the gathered vector,

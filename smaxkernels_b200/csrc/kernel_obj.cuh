@@ -71,6 +71,9 @@ struct PendingEvents {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> live, spare;
     std::pair<cudaEvent_t, cudaEvent_t> acquire();
     double drain();  // waits for and sums all live intervals (seconds)
+    // sums and recycles all but the newest `keep` intervals once more than
+    // 2*keep are live (bounds the event count of long apply() loops)
+    double trim(size_t keep);
     ~PendingEvents();
 };
 

@@ -91,6 +91,23 @@ std::pair<cudaEvent_t, cudaEvent_t> PendingEvents::acquire() {
     return p;
 }
 
+double PendingEvents::trim(size_t keep) {
+    if (live.size() <= 2 * keep) return 0.0;
+    // the oldest intervals finished long ago in any pipelined loop
+    const size_t n = live.size() - keep;
+    double s = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+        auto &p = live[i];
+        SMAX_CUDA(cudaEventSynchronize(p.second));
+        float ms = 0.f;
+        SMAX_CUDA(cudaEventElapsedTime(&ms, p.first, p.second));
+        s += ms * 1e-3;
+        spare.push_back(p);
+    }
+    live.erase(live.begin(), live.begin() + (ptrdiff_t)n);
+    return s;
+}
+
 double PendingEvents::drain() {
     double s = 0.0;
     for (auto &p : live) {

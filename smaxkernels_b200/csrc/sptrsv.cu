@@ -227,8 +227,22 @@ void tri_solve(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int
 
 template <typename VT>
 void tri_solve_graph(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int64_t k, bool row_major,
-                     int64_t ld, int merge_rows, cudaStream_t st) {
+                     int64_t ld, int merge_rows, cudaStream_t caller) {
     if (p.n_rows == 0) return;
+    // graphs are captured (and replayed) on a capturable stream
+    const bool fenced = !is_capturable(caller);
+    cudaStream_t st = fenced ? p.aux.enter(caller) : caller;
+    struct Leave {
+        TriPlan &p;
+        bool fenced;
+        cudaStream_t caller;
+        ~Leave() {
+            if (fenced) {
+                cudaEventRecord(p.aux.out, p.aux.s);
+                cudaStreamWaitEvent(caller, p.aux.out, 0);
+            }
+        }
+    } leave{p, fenced, caller};
     if (p.scheduled_k != k || p.scheduled_merge != merge_rows) p.schedule(k, merge_rows);
     const void *key[3] = {B, X, D};
     if (!p.graph_valid || p.graph_key[0] != key[0] || p.graph_key[1] != key[1] || p.graph_key[2] != key[2] ||

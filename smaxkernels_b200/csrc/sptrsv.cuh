@@ -39,6 +39,7 @@ struct TriPlan {
     const void *graph_key[3] = {nullptr, nullptr, nullptr};
     bool graph_row_major = false;
     int64_t graph_ld = 0;
+    AuxStream aux;  // capture stream when the caller's stream cannot be captured
 
     // dependency levels of the matrix itself (plain solve)
     void build_own(const DevCRS &a, bool upper, cudaStream_t st);

@@ -245,8 +245,21 @@ void TriBatch::solve_persistent(const VT *B, VT *X, cudaStream_t st) {
 }
 
 template <typename VT>
-void TriBatch::solve_graph(const VT *B, VT *X, cudaStream_t st) {
+void TriBatch::solve_graph(const VT *B, VT *X, cudaStream_t caller) {
     if (n_mats == 0) return;
+    const bool fenced = !is_capturable(caller);
+    cudaStream_t st = fenced ? aux.enter(caller) : caller;
+    struct Leave {
+        AuxStream &aux;
+        bool fenced;
+        cudaStream_t caller;
+        ~Leave() {
+            if (fenced) {
+                cudaEventRecord(aux.out, aux.s);
+                cudaStreamWaitEvent(caller, aux.out, 0);
+            }
+        }
+    } leave{aux, fenced, caller};
     if (!graph || graph_b != B || graph_x != X) {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;

@@ -23,6 +23,7 @@ struct TriBatch {
     DevBuf D, order, mat_lvl_off, lvl_rows, queue_order, queue;
     cudaGraphExec_t graph = nullptr;
     const void *graph_b = nullptr, *graph_x = nullptr;
+    AuxStream aux;  // capture stream when the caller's stream cannot be captured
 
     void build(int vbytes, const std::vector<RegCRS> &mats, cudaStream_t st);
     template <typename VT> void solve_persistent(const VT *B, VT *X, cudaStream_t st);

@@ -68,6 +68,14 @@ FLAG = dict(mat_perm=0, mat_upper_triang=1, mat_lower_triang=2, vec_row_major=3,
 SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED, SOLVE_GRAPH, SOLVE_PERSISTENT = 0, 1, 2, 3, 4
 
 
+CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy: the legacy default stream as an explicit handle
+
+
+def _stream_arg(stream):
+    """A torch stream handle for the C ABI: 0 (the default stream) becomes cudaStreamLegacy."""
+    return C.c_void_p(stream if stream else CUDA_STREAM_LEGACY)
+
+
 def _is_torch_cuda(a) -> bool:
     return hasattr(a, "is_cuda") and bool(a.is_cuda)
 
@@ -264,8 +272,14 @@ class Kernel:
         return lib.smax_kernel_stream(self._h) or 0
 
     def set_stream(self, stream_ptr: int | None):
-        """Launch on the caller's CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
-        check(lib.smax_kernel_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+        """Launch on the caller's CUDA stream, e.g. torch.cuda.current_stream().cuda_stream.
+        0 (torch's default stream) means the legacy default stream; None
+        restores the kernel's own stream."""
+        if stream_ptr is None:
+            arg = None
+        else:
+            arg = C.c_void_p(stream_ptr if stream_ptr else CUDA_STREAM_LEGACY)
+        check(lib.smax_kernel_set_stream(self._h, arg))
 
     def _destroy(self):
         if self._h:
@@ -300,9 +314,9 @@ class TriangularBatch:
         return nr.value, tl.value, ml.value
 
     def solve(self, rhs, x, mode: int = 0, stream: int = 0):
-        """rhs, x: CUDA tensors of the packed rows."""
-        check(lib.smax_batch_sptrsv_solve(self._h, _ptr(rhs), _ptr(x), int(mode),
-                                          C.c_void_p(stream) if stream else None))
+        """rhs, x: CUDA tensors of the packed rows; stream: a torch stream handle
+        (0, the default, is torch's default stream)."""
+        check(lib.smax_batch_sptrsv_solve(self._h, _ptr(rhs), _ptr(x), int(mode), _stream_arg(stream)))
 
     def close(self):
         if self._h:
