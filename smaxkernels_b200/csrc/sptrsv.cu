@@ -155,8 +155,35 @@ void TriPlan::build_given(const std::vector<int> &lp, int64_t n, bool upper, cud
     finish(st);
 }
 
+void TriPlan::assign_reverse(const TriPlan &src, cudaStream_t st) {
+    release_graph();
+    n_rows = src.n_rows;
+    lvl_ptr = src.lvl_ptr;
+    has_order = src.has_order;
+    descending = !src.descending;
+    if (src.has_order) {
+        order.alloc(sizeof(int) * (n_rows > 0 ? n_rows : 1));
+        if (n_rows) SMAX_CUDA(cudaMemcpyAsync(order.p, src.order.p, sizeof(int) * n_rows, cudaMemcpyDeviceToDevice, st));
+    } else {
+        order.release();
+    }
+    scheduled_k = -1;
+    scheduled_merge = -1;
+    finish(st);
+}
+
 void TriPlan::finish(cudaStream_t) {
     graph_valid = false;
+}
+
+void TriPlan::prepare(int64_t k, int merge_rows, cudaStream_t st) {
+    if (scheduled_k != k || scheduled_merge != merge_rows) schedule(k, merge_rows);
+    if (!ranges_uploaded && !seg_ranges.empty()) {
+        SMAX_CUDA(cudaMemcpyAsync(d_ranges.p, seg_ranges.data(), sizeof(int2) * seg_ranges.size(),
+                                  cudaMemcpyHostToDevice, st));
+        ranges_uploaded = true;
+        SMAX_CUDA(cudaStreamSynchronize(st));
+    }
 }
 
 // Sequence of steps: wide levels alone, runs of narrow levels merged.
@@ -201,6 +228,12 @@ void TriPlan::schedule(int64_t k, int merge_rows) {
 template <typename VT>
 void tri_solve(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int64_t k, bool row_major, int64_t ld,
                int merge_rows, cudaStream_t st) {
+    tri_solve_raw<VT>(p, a.rp(), a.ci(), a.val.as<VT>(), D, B, X, k, row_major, ld, merge_rows, st);
+}
+
+template <typename VT>
+void tri_solve_raw(TriPlan &p, const int *rp, const int *ci, const VT *val, const VT *D, const VT *B, VT *X,
+                   int64_t k, bool row_major, int64_t ld, int merge_rows, cudaStream_t st) {
     if (p.n_rows == 0) return;
     if (p.scheduled_k != k || p.scheduled_merge != merge_rows) p.schedule(k, merge_rows);
     if (!p.ranges_uploaded && !p.seg_ranges.empty()) {
@@ -214,12 +247,11 @@ void tri_solve(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int
     for (const auto &s : p.steps) {
         if (s.kind == 0) {
             const int64_t work = (int64_t)s.m * k;
-            level_kernel<VT><<<ceil_div_u(work, 256), 256, 0, st>>>(a.rp(), a.ci(), a.val.as<VT>(), D, order, s.row0,
-                                                                    s.m, k, row_major, rs, vs, B, X);
+            level_kernel<VT><<<ceil_div_u(work, 256), 256, 0, st>>>(rp, ci, val, D, order, s.row0, s.m, k, row_major,
+                                                                    rs, vs, B, X);
         } else {
-            segment_kernel<VT><<<1, kSegThreads, 0, st>>>(a.rp(), a.ci(), a.val.as<VT>(), D, order,
-                                                          ranges + s.seg_first, s.seg_count, k, row_major, rs, vs, B,
-                                                          X);
+            segment_kernel<VT><<<1, kSegThreads, 0, st>>>(rp, ci, val, D, order, ranges + s.seg_first, s.seg_count, k,
+                                                          row_major, rs, vs, B, X);
         }
     }
     SMAX_CUDA(cudaGetLastError());
@@ -291,6 +323,10 @@ template void tri_solve<double>(TriPlan &, const DevCRS &, const double *, const
                                 int64_t, int, cudaStream_t);
 template void tri_solve<float>(TriPlan &, const DevCRS &, const float *, const float *, float *, int64_t, bool,
                                int64_t, int, cudaStream_t);
+template void tri_solve_raw<double>(TriPlan &, const int *, const int *, const double *, const double *,
+                                    const double *, double *, int64_t, bool, int64_t, int, cudaStream_t);
+template void tri_solve_raw<float>(TriPlan &, const int *, const int *, const float *, const float *, const float *,
+                                   float *, int64_t, bool, int64_t, int, cudaStream_t);
 template void tri_solve_graph<double>(TriPlan &, const DevCRS &, const double *, const double *, double *, int64_t,
                                       bool, int64_t, int, cudaStream_t);
 template void tri_solve_graph<float>(TriPlan &, const DevCRS &, const float *, const float *, float *, int64_t, bool,

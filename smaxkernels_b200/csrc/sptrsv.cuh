@@ -45,8 +45,13 @@ struct TriPlan {
     void build_own(const DevCRS &a, bool upper, cudaStream_t st);
     // caller-given contiguous levels (permuted, level-scheduled solve)
     void build_given(const std::vector<int> &lvl_ptr, int64_t n, bool upper, cudaStream_t st);
+    // the same level sets swept in the opposite direction (the schedule of
+    // the transposed solve)
+    void assign_reverse(const TriPlan &src, cudaStream_t st);
     void finish(cudaStream_t st);
     void schedule(int64_t k, int merge_rows);
+    // schedules and uploads the merged-run ranges ahead of a stream capture
+    void prepare(int64_t k, int merge_rows, cudaStream_t st);
     void release_graph();
     int n_levels() const { return lvl_ptr.empty() ? 0 : (int)lvl_ptr.size() - 1; }
     ~TriPlan();
@@ -58,6 +63,11 @@ struct TriPlan {
 template <typename VT>
 void tri_solve(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int64_t k, bool row_major, int64_t ld,
                int merge_rows, cudaStream_t st);
+// tri_solve on raw arrays (rp/ci of the matrix the plan was built for, with
+// any values of type VT, e.g. a float copy of double values).
+template <typename VT>
+void tri_solve_raw(TriPlan &p, const int *rp, const int *ci, const VT *val, const VT *D, const VT *B, VT *X,
+                   int64_t k, bool row_major, int64_t ld, int merge_rows, cudaStream_t st);
 // The same launch sequence, captured once into a CUDA graph and replayed.
 template <typename VT>
 void tri_solve_graph(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int64_t k, bool row_major,
