@@ -92,6 +92,8 @@ typedef int smax_status;
 #define SMAX_FLAG_LEVEL_MERGE 12       /* levels with <= this many rows*rhs run merged in one CTA (0: never) */
 #define SMAX_FLAG_SPIN_LIMIT 13        /* polls (x 1000) before a persistent solve's grid barrier times out */
 #define SMAX_FLAG_TEST_FORCE_TIMEOUT 14 /* test only: the persistent solve's barrier waits for a missing arrival */
+#define SMAX_FLAG_REFINE 15            /* float64 SpTRSV: solve in FP32, then this many FP64-residual corrections (0: off) */
+#define SMAX_FLAG_REFINE_TOL 16        /* stop refining once max|dx| <= 10^-value * max|x| (host check per step; 0: run all) */
 
 /* SpTRSV / SpTRSM launch schemes (SMAX_FLAG_SOLVE_MODE) */
 #define SMAX_SOLVE_AUTO 0        /* graph-captured, narrow levels merged (the default) */
@@ -186,6 +188,68 @@ void *smax_kernel_stream(smax_kernel k);
  * current stream of a framework) instead of its own; NULL restores its own.
  * The caller keeps ownership of the stream. */
 smax_status smax_kernel_set_stream(smax_kernel k, void *stream);
+
+/* ------------------------------------------------- reverse-mode derivatives */
+/* Adjoint of an initialized kernel (no counterpart in the reference), for a
+ * loss gradient g:
+ *   SpMV (CRS, y = A x):  d_in = A^T g (n_cols values),
+ *                         d_val[k] = g[row(k)] * x[col(k)]   (nnz values)
+ *   SpTRSV (L x = b):     L^T lambda = g;  d_in = lambda = dLoss/db (n values),
+ *                         d_val[k] = -lambda[row(k)] * x[col(k)]
+ * d_val follows the entry order of the device copy of A: the registered order
+ * for SpMV; for SpTRSV the order after initialize moved each diagonal to the
+ * end of its row (the order the caller's arrays then hold).  x is the SpMV
+ * input or the SpTRSV solution; NULL means the registered B.  g, x, d_in and
+ * d_val are device pointers when SMAX_FLAG_DEVICE_POINTERS is set, host
+ * pointers otherwise (the call then returns when the outputs are written).
+ * d_in or d_val may be NULL to skip that output.  A^T (L^T) is built on the
+ * first call and kept with the kernel. */
+smax_status smax_kernel_adjoint(smax_kernel k, const void *x, const void *g, void *d_in, void *d_val);
+
+/* Replaces the values of the device copy of a CRS A (SpMV, SpMM, SpTRSV,
+ * SpTRSM) in place, keeping the pattern and every plan; val holds nnz values
+ * in the entry order described for d_val above.  For solves the diagonal is
+ * re-read and checked (ZERO_DIAG).  Host or device pointer as above. */
+smax_status smax_kernel_update_A_values(smax_kernel k, const void *val);
+
+/* Refinement statistics of the last solve with SMAX_FLAG_REFINE: corrections
+ * applied and max|dx| / max|x| of the last one. */
+smax_status smax_kernel_get_refine_stats(smax_kernel k, int *steps, double *last_rel_correction);
+
+/* --------------------------------------------------------------- autotuning */
+/* Times the launch variants of an initialized kernel on its registered
+ * operands and keeps the fastest: the CRS SpMV kernel for SpMV; the solve
+ * mode and the level-merge threshold for SpTRSV / SpTRSM.  Choices are cached
+ * for the life of the process per matrix (kernel type, value type, sizes and
+ * a hash of the pattern); a later kernel with the same matrix takes them from
+ * the cache.  Overwrites the output operand (C for SpMV, B for solves). */
+typedef struct smax_tuning {
+    int spmv_variant; /* SMAX_FLAG_SPMV_VARIANT chosen (SpMV) */
+    int solve_mode;   /* SMAX_SOLVE_* chosen (SpTRSV / SpTRSM) */
+    int level_merge;  /* SMAX_FLAG_LEVEL_MERGE chosen (SpTRSV / SpTRSM) */
+    int from_cache;   /* 1: taken from the process-wide cache */
+    int n_candidates; /* configurations timed (0 from the cache) */
+    double seconds;   /* one apply with the choice */
+} smax_tuning;
+smax_status smax_kernel_autotune(smax_kernel k, smax_tuning *out);
+
+/* Chooses the storage format of a CRS matrix for SpMV by converting it on the
+ * GPU and timing each candidate: CRS (both kernels), SELL-C-sigma with
+ * C in {8, 16, 32, 64} and sigma in {1, C*8, 1024}, and BCRS with square
+ * blocks of 2 and 4 where the dimensions divide and the fill stays below
+ * twice the nonzeros.  Host arrays. */
+typedef struct smax_format_choice {
+    int format;             /* 0 CRS, 1 SELL-C-sigma, 2 BCRS */
+    int spmv_variant;       /* CRS kernel (format 0) */
+    int C, sigma;           /* SELL-C-sigma parameters (format 1) */
+    int b_height, b_width;  /* BCRS block (format 2) */
+    int n_candidates;       /* configurations timed */
+    double seconds;         /* one SpMV with the choice */
+    double crs_seconds;     /* one SpMV with the best CRS kernel */
+} smax_format_choice;
+smax_status smax_utils_tune_spmv_format(int float_type, uint64_t n_rows, uint64_t n_cols, uint64_t nnz,
+                                        const void *row_ptr, const void *col, const void *val,
+                                        smax_format_choice *out);
 
 /* -------------------------------------------------------- batched SpTRSV */
 /* A batch of independent lower-triangular CRS matrices (host arrays, each with

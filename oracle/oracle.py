@@ -165,6 +165,42 @@ class Oracle:
                 int(bool(lower)), len(lp) - 1, _p(lp), _p(pcol), _p(rp), _p(pval), _p(D), _p(x), _p(bb))
         return x
 
+    # -- adjoints (no reference counterpart) ----------------------------------
+    @staticmethod
+    def transpose(row_ptr, col, val, n_cols):
+        """CRS of A^T with each row in ascending row order of A (a stable
+        counting sort of the entries by column)."""
+        rp = _i32(row_ptr)
+        col = _i32(col)
+        n = len(rp) - 1
+        rows = np.repeat(np.arange(n, dtype=np.int32), np.diff(rp))
+        order = np.argsort(col, kind="stable")
+        t_rp = np.zeros(n_cols + 1, dtype=np.int32)
+        np.cumsum(np.bincount(col, minlength=n_cols), out=t_rp[1:])
+        return t_rp, rows[order].astype(np.int32), np.ascontiguousarray(val[order])
+
+    def spmv_adjoint(self, row_ptr, col, val, x, g, n_cols=None):
+        """y = A x, loss gradient g = dL/dy: returns (A^T g, dval) with
+        dval[k] = g[row(k)] * x[col(k)], A^T formed on the host."""
+        n = len(row_ptr) - 1
+        n_cols = n if n_cols is None else n_cols
+        t_rp, t_col, t_val = self.transpose(row_ptr, col, val, n_cols)
+        dx = self.spmv_crs(t_rp, t_col, t_val, np.ascontiguousarray(g, val.dtype))
+        rows = np.repeat(np.arange(n), np.diff(_i32(row_ptr)))
+        dval = np.asarray(g, val.dtype)[rows] * np.asarray(x, val.dtype)[_i32(col)]
+        return dx, dval
+
+    def sptrsv_adjoint(self, row_ptr, col, val, x, g, lower=True):
+        """L x = b, loss gradient g = dL/dx: returns (lambda, dval) with
+        L^T lambda = g (an upper solve for lower L, through the reference
+        semantics) and dval[k] = -lambda[row(k)] * x[col(k)]."""
+        n = len(row_ptr) - 1
+        t_rp, t_col, t_val = self.transpose(row_ptr, col, val, n)
+        lam = self.sptrsv(t_rp, t_col, t_val, np.ascontiguousarray(g, val.dtype), lower=not lower)
+        rows = np.repeat(np.arange(n), np.diff(_i32(row_ptr)))
+        dval = -lam[rows] * np.asarray(x, val.dtype)[_i32(col)]
+        return lam, dval
+
     def sptrsm(self, row_ptr, col, val, B, k, lower=True, row_major=True):
         pcol, pval, D = self.peel_diag(row_ptr, col, val)
         rp = _i32(row_ptr)

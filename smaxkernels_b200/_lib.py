@@ -48,6 +48,11 @@ SIGNATURES = {
     "smax_kernel_get_timer": (I32, [P, C.c_char_p, C.POINTER(C.c_double)]),
     "smax_kernel_stream": (P, [P]),
     "smax_kernel_set_stream": (I32, [P, P]),
+    "smax_kernel_adjoint": (I32, [P, P, P, P, P]),
+    "smax_kernel_update_A_values": (I32, [P, P]),
+    "smax_kernel_get_refine_stats": (I32, [P, C.POINTER(I32), C.POINTER(C.c_double)]),
+    "smax_kernel_autotune": (I32, [P, P]),
+    "smax_utils_tune_spmv_format": (I32, [I32, U64, U64, U64, P, P, P, P]),
     "smax_batch_sptrsv_create": (I32, [PP, I32, I32, PU64, PU64, PP, PP, PP]),
     "smax_batch_sptrsv_solve": (I32, [P, P, P, I32, P]),
     "smax_batch_row_offset": (U64, [P, I32]),
@@ -63,6 +68,25 @@ SIGNATURES = {
     "smax_free_host": (None, [P]),
     "smax_spmv_crs_noalloc": (I32, [I32, U64, U64, U64, P, P, P, P, P, P]),
 }
+
+
+
+class Tuning(C.Structure):
+    """struct smax_tuning"""
+    _fields_ = [("spmv_variant", C.c_int), ("solve_mode", C.c_int), ("level_merge", C.c_int),
+                ("from_cache", C.c_int), ("n_candidates", C.c_int), ("seconds", C.c_double)]
+
+
+class FormatChoice(C.Structure):
+    """struct smax_format_choice"""
+    _fields_ = [("format", C.c_int), ("spmv_variant", C.c_int), ("C", C.c_int), ("sigma", C.c_int),
+                ("b_height", C.c_int), ("b_width", C.c_int), ("n_candidates", C.c_int), ("seconds", C.c_double),
+                ("crs_seconds", C.c_double)]
+
+
+def struct_dict(s) -> dict:
+    return {name: getattr(s, name) for name, _ in s._fields_}
+
 
 for _name, (_res, _args) in SIGNATURES.items():
     _f = getattr(lib, _name)

@@ -5,7 +5,7 @@
 // spmm.hpp:68-100): the kernel type and the flags pick the format and kernel.
 #include <cstring>
 
-#include "kernel_obj.cuh"
+#include "abi_internal.cuh"
 #include "sptrsv_batch.cuh"
 
 smax_kernel_s::~smax_kernel_s() {
@@ -15,7 +15,7 @@ smax_kernel_s::~smax_kernel_s() {
 
 using namespace smax;
 
-namespace {
+namespace smax {
 
 void require(bool c, int code, const char *msg) {
     if (!c) fail(code, msg);
@@ -39,6 +39,42 @@ void read_status(smax_kernel_s *k) {
 }
 
 DevStatus *dstatus(smax_kernel_s *k) { return k->status.as<DevStatus>(); }
+
+bool is_tri(const smax_kernel_s *k) { return k->ktype == SMAX_KERNEL_SPTRSV || k->ktype == SMAX_KERNEL_SPTRSM; }
+
+void tri_plan(smax_kernel_s *k) {
+    if (k->f_perm) {
+        require(k->ctx != nullptr && k->ctx->n_levels > 0, SMAX_ERR_STATE,
+                "level-scheduled solve needs the levels of generate_perm in the context");
+        if (!k->tri_plan_valid || k->tri_levels_version != k->ctx->levels_version) {
+            k->tri.release_graph();
+            k->tri.build_given(k->ctx->lvl_ptr, k->dA.n_rows, k->f_upper, k->stream);
+            k->tri_levels_version = k->ctx->levels_version;
+            k->tri_plan_valid = true;
+            ++k->tri_plan_serial;
+        }
+    } else if (!k->tri_plan_valid) {
+        k->tri.release_graph();
+        k->tri.build_own(k->dA, k->f_upper, k->stream);
+        k->tri_plan_valid = true;
+        ++k->tri_plan_serial;
+    }
+}
+
+// Device addresses of B and C (+ element offsets).
+const void *dev_b(smax_kernel_s *k, uint64_t off) {
+    const char *base = k->f_device ? static_cast<const char *>(k->B.val) : static_cast<const char *>(k->dB.p);
+    return base + off * k->vbytes;
+}
+
+void *dev_c(smax_kernel_s *k, uint64_t off) {
+    char *base = k->f_device ? static_cast<char *>(k->C.val) : static_cast<char *>(k->dC.p);
+    return base + off * k->vbytes;
+}
+
+}  // namespace smax
+
+namespace {
 
 template <typename T> T *up(DevBuf &d, const void *h, uint64_t n, cudaStream_t st) {
     d.alloc(sizeof(T) * (n ? n : 1));
@@ -142,9 +178,6 @@ template <typename VT> void spmm_apply_t(smax_kernel_s *k, const VT *X, VT *Y) {
 // ------------------------------------------------------- SpTRSV / SpTRSM --
 // register_B is the solution x (X), register_C the right-hand side b (B)
 // (src/kernels/sptrsv.hpp:40-58, sptrsm.hpp:40-60).
-bool is_tri(const smax_kernel_s *k) { return k->ktype == SMAX_KERNEL_SPTRSV || k->ktype == SMAX_KERNEL_SPTRSM; }
-
-constexpr int kDefaultLevelMerge = 4096;
 
 void tri_upload(smax_kernel_s *k) {
     require(k->A.set, SMAX_ERR_STATE, "register_A before initialize");
@@ -165,30 +198,21 @@ void tri_upload(smax_kernel_s *k) {
     k->tri_plan_valid = false;
 }
 
-void tri_plan(smax_kernel_s *k) {
-    if (k->f_perm) {
-        require(k->ctx != nullptr && k->ctx->n_levels > 0, SMAX_ERR_STATE,
-                "level-scheduled solve needs the levels of generate_perm in the context");
-        if (!k->tri_plan_valid || k->tri_levels_version != k->ctx->levels_version) {
-            k->tri.release_graph();
-            k->tri.build_given(k->ctx->lvl_ptr, k->dA.n_rows, k->f_upper, k->stream);
-            k->tri_levels_version = k->ctx->levels_version;
-            k->tri_plan_valid = true;
-        }
-    } else if (!k->tri_plan_valid) {
-        k->tri.release_graph();
-        k->tri.build_own(k->dA, k->f_upper, k->stream);
-        k->tri_plan_valid = true;
-    }
-}
 
 template <typename VT> void tri_apply_t(smax_kernel_s *k, const VT *Bv, VT *Xv) {
     tri_plan(k);
+    if constexpr (sizeof(VT) == 8) {
+        if (k->refine_steps > 0) {
+            require(k->ktype == SMAX_KERNEL_SPTRSV, SMAX_ERR_UNSUPPORTED,
+                    "refinement is available for SpTRSV (one right-hand side)");
+            refine_solve(k, Bv, Xv);
+            return;
+        }
+    }
     const int64_t kk = k->ktype == SMAX_KERNEL_SPTRSM ? (int64_t)(k->B.n_cols ? k->B.n_cols : 1) : 1;
     const bool rm = k->ktype == SMAX_KERNEL_SPTRSM ? k->f_row_major : true;
     const int64_t ld = k->dA.n_rows;  // column-major blocks use A's n_rows (sptrsm_cpu_crs_impl.hpp:44-50)
-    const int merge = k->solve_mode == SMAX_SOLVE_PER_LEVEL ? 0
-                      : (k->level_merge >= 0 ? k->level_merge : kDefaultLevelMerge);
+    const int merge = tri_merge_rows(k);
     if (k->solve_mode == SMAX_SOLVE_PERSISTENT) {
         require(kk == 1, SMAX_ERR_UNSUPPORTED, "the persistent solve handles one right-hand side");
         tri_solve_persistent<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, dstatus(k), k->persist_scratch,
@@ -236,15 +260,6 @@ void spgemm_finalize(smax_kernel_s *k) {
     *k->Cref.val = val;
 }
 
-// Device addresses of B and C (+ element offsets).
-const void *dev_b(smax_kernel_s *k, uint64_t off) {
-    const char *base = k->f_device ? static_cast<const char *>(k->B.val) : static_cast<const char *>(k->dB.p);
-    return base + off * k->vbytes;
-}
-void *dev_c(smax_kernel_s *k, uint64_t off) {
-    char *base = k->f_device ? static_cast<char *>(k->C.val) : static_cast<char *>(k->dC.p);
-    return base + off * k->vbytes;
-}
 
 // Operand extents the kernel reads (B) and writes (C), in elements.
 void check_extents(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
@@ -286,6 +301,8 @@ void do_initialize(smax_kernel_s *k) {
         if (k->a_dirty) {
             spgemm_upload(k);
             k->a_dirty = false;
+            ++k->a_version;
+            ++k->vals_version;
         }
         k->timers["initialize"] += wall_s() - t0;
         return;
@@ -300,6 +317,8 @@ void do_initialize(smax_kernel_s *k) {
         default: fail(SMAX_ERR_UNSUPPORTED, "kernel type not available in this build");
         }
         k->a_dirty = false;
+        ++k->a_version;
+        ++k->vals_version;
     }
     if (!k->f_device) {
         size_t bb = (size_t)k->B.elems() * k->vbytes, cb = (size_t)k->C.elems() * k->vbytes;
@@ -340,6 +359,14 @@ void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
     k->timers["apply"] += k->apply_events.trim(512);
     auto ev = k->apply_events.acquire();
     SMAX_CUDA(cudaEventRecord(ev.first, k->stream));
+    apply_core(k, b_off, c_off);
+    SMAX_CUDA(cudaEventRecord(ev.second, k->stream));
+}
+
+}  // namespace
+
+// The launches of one apply (no stopwatch events).
+void smax::apply_core(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
     const void *b = dev_b(k, b_off);
     void *c = dev_c(k, c_off);
     const bool f64 = k->vbytes == 8;
@@ -363,8 +390,17 @@ void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
     }
     default: fail(SMAX_ERR_UNSUPPORTED, "kernel type not available in this build");
     }
-    SMAX_CUDA(cudaEventRecord(ev.second, k->stream));
 }
+
+void smax::build_crs_plans(smax_kernel_s *k) {
+    k->crs_plan = CrsTilePlan();
+    k->crs_plan.build(k->dA.rp(), k->dA.n_rows, crs_default_cap(k->vbytes * 8), k->stream);
+    k->crs_stream = CrsStreamPlan();
+    k->crs_stream.build(k->dA.rp(), k->dA.n_rows, k->dA.nnz, k->vbytes, k->stream);
+    SMAX_CUDA(cudaStreamSynchronize(k->stream));
+}
+
+namespace {
 
 void do_finalize(smax_kernel_s *k) {
     double t0 = wall_s();
@@ -490,6 +526,16 @@ smax_status smax_kernel_set_flag(smax_kernel k, int flag, int value) {
             require(value >= SMAX_SOLVE_AUTO && value <= SMAX_SOLVE_PERSISTENT, SMAX_ERR_BAD_ARG,
                     "unknown solve mode");
             kk->solve_mode = value;
+            break;
+        case SMAX_FLAG_REFINE:
+            require(value >= 0 && value <= 64, SMAX_ERR_BAD_ARG, "refinement steps must be in [0, 64]");
+            require(value == 0 || kk->ftype == SMAX_FLOAT64, SMAX_ERR_UNSUPPORTED_TYPE,
+                    "refinement needs a float64 kernel (the FP32 copy is made internally)");
+            kk->refine_steps = value;
+            break;
+        case SMAX_FLAG_REFINE_TOL:
+            require(value >= 0 && value <= 16, SMAX_ERR_BAD_ARG, "refinement tolerance exponent must be in [0, 16]");
+            kk->refine_tol = value;
             break;
         case SMAX_FLAG_LEVEL_MERGE:
             require(value >= 0, SMAX_ERR_BAD_ARG, "level merge threshold must be >= 0");

@@ -17,6 +17,8 @@
 #include "spmv_formats.cuh"
 #include "spgemm.cuh"
 #include "sptrsv.cuh"
+#include "adjoint.cuh"
+#include "refine.cuh"
 
 struct smax_ctx_s {
     // UtilitiesContainer (src/common.hpp:187-195): written by generate_perm,
@@ -121,12 +123,27 @@ struct smax_kernel_s {
     smax::DevBuf D;                 // peeled diagonal
     smax::TriPlan tri;
     bool tri_plan_valid = false;
+    uint64_t tri_plan_serial = 0;   // bumped whenever tri is rebuilt
     uint64_t tri_levels_version = 0;
     int solve_mode = 0;             // SMAX_SOLVE_*
     int level_merge = -1;           // rows*k of levels merged into one-CTA runs; -1 = default
     bool force_timeout = false;     // test knob of the persistent solve's grid barrier
     long long spin_limit = 20000000; // polls before a grid barrier gives up
     smax::DevBuf persist_scratch;
+
+    // versions of the device copy of A: pattern + values (each upload), values
+    // alone (each upload or value update)
+    uint64_t a_version = 0, vals_version = 0;
+
+    // reverse mode (adjoint_abi.cu): A^T or L^T and the reversed level plan
+    smax::DevTranspose adj;
+    smax::TriPlan adj_plan;
+    uint64_t adj_version = ~0ull, adj_plan_serial = ~0ull;
+    smax::DevBuf adj_stage[4];      // device staging of host operands (x, g, d_in, d_val)
+
+    // FP32 solve + FP64 residual refinement (refine.cu); 0 steps = off
+    int refine_steps = 0, refine_tol = 0;
+    smax::RefineState refine;
 
     // stopwatches
     std::map<std::string, double> timers;

@@ -201,7 +201,7 @@ template void bcrs_spmv<double>(const DevBCRS &, const double *, double *, cudaS
 template void bcrs_spmv<float>(const DevBCRS &, const float *, float *, cudaStream_t);
 
 void crs_to_bcrs(const DevCRS &a, int vbytes, int64_t bh, int64_t bw, int64_t hpad, int64_t wpad, bool col_major,
-                 DevBCRS &out, cudaStream_t st) {
+                 DevBCRS &out, cudaStream_t st, int64_t max_blocks) {
     // the reference throws for these (src/utils/convert_formats.hpp:143-160); it
     // tests the height padding twice, this platform tests both paddings
     if (bh <= 0 || bw <= 0 || a.n_rows % bh) fail(SMAX_ERR_BAD_ARG, "Target block height does not divide number of input rows");
@@ -246,6 +246,12 @@ void crs_to_bcrs(const DevCRS &a, int vbytes, int64_t bh, int64_t bw, int64_t hp
     SMAX_CUDA(cudaMemcpyAsync(&nu, nsel.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     SMAX_CUDA(cudaStreamSynchronize(st));
     out.n_blocks = nu;
+    if (max_blocks >= 0 && nu > max_blocks) {
+        // more blocks than the caller accepts: report the count, build nothing
+        out.col.release();
+        out.val.release();
+        return;
+    }
     DevBuf counts(sizeof(int) * nb), incl(sizeof(int) * nb);
     SMAX_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * nb, st));
     bcrs_count<<<ceil_div_u(nu, 256), 256, 0, st>>>(ubrow.as<int>(), nu, counts.as<int>());

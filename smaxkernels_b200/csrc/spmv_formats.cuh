@@ -36,8 +36,10 @@ bool scs_vector_path(int64_t C, int vbytes);
 void crs_to_scs(const DevCRS &a, int vbytes, int64_t C, int64_t sigma, DevSCS &out, DevBuf &perm, cudaStream_t st);
 
 template <typename VT> void bcrs_spmv(const DevBCRS &m, const VT *x, VT *y, cudaStream_t st);
+// max_blocks >= 0: when the matrix needs more blocks, only out.n_blocks is set
+// (out.val stays empty)
 void crs_to_bcrs(const DevCRS &a, int vbytes, int64_t bh, int64_t bw, int64_t hpad, int64_t wpad, bool col_major,
-                 DevBCRS &out, cudaStream_t st);
+                 DevBCRS &out, cudaStream_t st, int64_t max_blocks = -1);
 
 // Y = A X with k right-hand sides.  Row-major: X[col*k+v], Y[row*k+v].
 // Column-major: X[ldx*v+col], Y[row+ldy*v] (the reference uses A's n_rows as

@@ -60,6 +60,22 @@ __global__ void peel_diag_kernel(const int *__restrict__ rp, int *__restrict__ c
     }
 }
 
+// D[r] = the last entry of row r, which the peel made the diagonal
+template <typename VT>
+__global__ void refresh_diag_kernel(const int *__restrict__ rp, const int *__restrict__ col,
+                                    const VT *__restrict__ val, int64_t n, VT *__restrict__ D, DevStatus *st) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const int e = rp[r + 1] - 1;
+    if (e < rp[r] || col[e] != (int)r) {
+        report(st, SMAX_ERR_NO_DIAG, r);
+        return;
+    }
+    const VT d = val[e];
+    if (fabs((double)d) < 1e-16) report(st, SMAX_ERR_ZERO_DIAG, r);
+    D[r] = d;
+}
+
 // ------------------------------------------------------------ the row op ---
 // Element (row r, vector v) of X / B lives at r*rs + v*vs.
 template <typename VT>
@@ -127,6 +143,16 @@ void peel_diag(DevCRS &a, int vbytes, DevBuf &D, DevStatus *st, cudaStream_t s) 
     else
         peel_diag_kernel<float><<<g, 256, 0, s>>>(a.rp(), a.col.as<int>(), a.val.as<float>(), a.n_rows,
                                                   D.as<float>(), st);
+    SMAX_CUDA(cudaGetLastError());
+}
+
+void refresh_diag(const DevCRS &a, int vbytes, DevBuf &D, DevStatus *st, cudaStream_t s) {
+    if (a.n_rows == 0) return;
+    const unsigned g = ceil_div_u(a.n_rows, 256);
+    if (vbytes == 8)
+        refresh_diag_kernel<double><<<g, 256, 0, s>>>(a.rp(), a.ci(), a.val.as<double>(), a.n_rows, D.as<double>(), st);
+    else
+        refresh_diag_kernel<float><<<g, 256, 0, s>>>(a.rp(), a.ci(), a.val.as<float>(), a.n_rows, D.as<float>(), st);
     SMAX_CUDA(cudaGetLastError());
 }
 

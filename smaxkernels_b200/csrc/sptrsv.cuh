@@ -11,6 +11,10 @@ namespace smax {
 // Copies the diagonal into D and swaps it to the last slot of each row (in
 // place on the device copy); missing / |d| < 1e-16 diagonals are reported.
 void peel_diag(DevCRS &a, int vbytes, DevBuf &D, DevStatus *st, cudaStream_t s);
+// Re-reads D from a matrix whose diagonals already sit last in their rows
+// (after a value update); a row whose last entry is not its diagonal reports
+// NO_DIAG, |d| < 1e-16 ZERO_DIAG.
+void refresh_diag(const DevCRS &a, int vbytes, DevBuf &D, DevStatus *st, cudaStream_t s);
 
 // The level schedule of one triangular matrix and its launch plan.
 struct TriPlan {

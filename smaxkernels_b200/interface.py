@@ -63,7 +63,8 @@ class SpMVType(enum.IntEnum):
 
 FLAG = dict(mat_perm=0, mat_upper_triang=1, mat_lower_triang=2, vec_row_major=3, mat_scs=4, mat_bcrs=5,
             block_column_major=6, kernel_impl=7, device_pointers=8, a_dirty=9,
-            spmv_variant=10, solve_mode=11, level_merge=12, spin_limit=13, test_force_timeout=14)
+            spmv_variant=10, solve_mode=11, level_merge=12, spin_limit=13, test_force_timeout=14,
+            refine=15, refine_tol=16)
 
 SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED, SOLVE_GRAPH, SOLVE_PERSISTENT = 0, 1, 2, 3, 4
 
@@ -242,6 +243,49 @@ class Kernel:
     def mark_A_dirty(self):
         return self._flag("a_dirty", 1)
 
+    def set_refine(self, steps: int, tol_exp: int = 0):
+        """float64 SpTRSV: solve in FP32 and apply `steps` FP64-residual
+        corrections; with tol_exp > 0 stop once max|dx| <= 10^-tol_exp max|x|."""
+        self._flag("refine", steps)
+        return self._flag("refine_tol", tol_exp)
+
+    def refine_stats(self):
+        """(corrections applied, max|dx|/max|x| of the last one) of the last refined solve."""
+        n, r = C.c_int(0), C.c_double(0.0)
+        check(lib.smax_kernel_get_refine_stats(self._h, C.byref(n), C.byref(r)))
+        return n.value, r.value
+
+    # -- reverse mode -----------------------------------------------------
+    def _same_space(self, *arrs):
+        dev = bool(self._device)
+        for a in arrs:
+            if a is not None and _is_torch_cuda(a) != dev:
+                raise RuntimeError("adjoint operands must live where B and C were registered "
+                                   f"({'device tensors' if dev else 'host arrays'})")
+
+    def adjoint(self, g, d_in=None, d_val=None, x=None):
+        """Reverse mode of an initialized CRS SpMV or SpTRSV kernel for the loss
+        gradient g: d_in = A^T g (SpMV) or lambda = L^-T g (SpTRSV, = dLoss/db);
+        d_val = g[row] x[col] (SpMV) or -lambda[row] x[col] (SpTRSV) in the
+        device copy's entry order; x defaults to the registered B."""
+        self._same_space(g, d_in, d_val, x)
+        check(lib.smax_kernel_adjoint(self._h, _ptr(x), _ptr(g), _ptr(d_in), _ptr(d_val)))
+        return 0
+
+    def update_A_values(self, val):
+        """New values for the device copy of A (same pattern and entry order)."""
+        self._same_space(val)
+        check(lib.smax_kernel_update_A_values(self._h, _ptr(val)))
+        return 0
+
+    # -- tuning -----------------------------------------------------------
+    def autotune(self) -> dict:
+        """Times the launch variants on the registered operands, keeps the
+        fastest (cached per matrix for the process) and returns the choice."""
+        t = _lib.Tuning()
+        check(lib.smax_kernel_autotune(self._h, C.byref(t)))
+        return _lib.struct_dict(t)
+
     # -- execution --------------------------------------------------------
     def initialize(self, A_offset=0, B_offset=0, C_offset=0):
         check(lib.smax_kernel_initialize(self._h, A_offset, B_offset, C_offset))
@@ -359,6 +403,19 @@ class Utils:
 
     def __init__(self, iface: "Interface"):
         self._iface = iface
+
+    def tune_spmv_format(self, n_rows, n_cols, nnz, col, row_ptr, val) -> dict:
+        """Times CRS (both kernels), SELL-C-sigma and BCRS candidates of this
+        matrix on the GPU and returns the fastest (smax_utils_tune_spmv_format)."""
+        col, row_ptr = _i32(col), _i32(row_ptr)
+        val = np.ascontiguousarray(val)
+        ft = FloatType.FLOAT64 if val.dtype == np.float64 else FloatType.FLOAT32
+        out = _lib.FormatChoice()
+        check(lib.smax_utils_tune_spmv_format(int(ft), int(n_rows), int(n_cols), int(nnz), _ptr(row_ptr),
+                                              _ptr(col), _ptr(val), C.byref(out)))
+        d = _lib.struct_dict(out)
+        d["format_name"] = ("CRS", "SELL-C-sigma", "BCRS")[d["format"]]
+        return d
 
     def convert_crs_to_scs(self, n_rows, n_cols, nnz, col, row_ptr, val, C_, sigma) -> dict:
         """Returns the 13 SELL-C-sigma fields of convert_crs_to_scs as a dict."""
