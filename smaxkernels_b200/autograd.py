@@ -11,7 +11,7 @@ reverse-mode entry (``smax_kernel_adjoint``):
 
 A :class:`SparsePattern` owns one kernel object with the pattern resident in
 HBM; values are differentiable tensors that are copied into the device copy
-(``smax_kernel_update_A_values``) when they change.  Every call runs on
+(``smax_kernel_update_A_values``) on every call.  Every call runs on
 torch's current stream, and the kernel object's operand buffers stay fixed so
 the solves' CUDA graphs are captured once.
 
@@ -101,7 +101,6 @@ class SparsePattern:
         self._dval = torch.zeros(self.nnz, **opts)
         self._bind_stream()
         self.k.initialize()
-        self._vals_key = None
 
     # -- plumbing ---------------------------------------------------------
     def _bind_stream(self):
@@ -110,16 +109,11 @@ class SparsePattern:
     def _set_values(self, val: torch.Tensor):
         if val.shape != (self.nnz,):
             raise ValueError(f"expected {self.nnz} values, got shape {tuple(val.shape)}")
-        # the last value tensor is held, so an equal (address, version) key
-        # means the same, unmodified values
-        key = (val.data_ptr(), val._version, val.dtype)
-        if key == self._vals_key:
-            return
+        # copied on every call (an nnz-sized device copy): edits through
+        # .data leave no trace a cache could check
         v = val.detach().to(device=self.device, dtype=self.dtype)
         v = (v[self._order] if self._order is not None else v).contiguous()
         self.k.update_A_values(v)
-        self._vals_key = key
-        self._last_val = val
         self._keep = v  # the copy is asynchronous on the stream: keep the source alive
 
     def _to_user_order(self, dval_dev: torch.Tensor) -> torch.Tensor:

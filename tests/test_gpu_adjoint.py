@@ -211,12 +211,12 @@ def _fd_check(fwd, params, t, entries_of, h=1e-6, rel=1e-6):
     worst = 0.0
     for p, idx in entries_of:
         for i in idx:
-            old = p.data[i].item()
-            p.data[i] = old + h
+            old = p[i].item()
+            p[i] = old + h
             yp = fwd().detach()
-            p.data[i] = old - h
+            p[i] = old - h
             ym = fwd().detach()
-            p.data[i] = old
+            p[i] = old
             fd = float((0.5 * (yp - ym) * (yp + ym - 2 * t)).sum()) / (2 * h)
             ad = float(p.grad[i])
             err = abs(fd - ad) / max(1.0, abs(ad))
