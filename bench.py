@@ -199,6 +199,503 @@ def config_dict(nnz, vbytes, world):
             "l2": "inputs larger than L2 (no flush)", "parallelism": f"row blocks x {world} ranks"}
 
 
+# ---------------------------------------------------------------------------
+# The other workloads of the hot path (--workload NAME, or "all"): one JSON
+# line per case, same keys as the headline line.  Single GPU.
+# ---------------------------------------------------------------------------
+EXTRA_WORKLOADS = ("spmv_laplace64", "scs_spmv", "bcrs_spmv", "spmm", "spgemm", "sptrsv", "sptrsv_batch",
+                   "sptrsv_refine", "adjoint")
+
+
+class Bench:
+    """Timing and reporting shared by the extra workloads."""
+
+    def __init__(self, args):
+        import torch
+        self.torch = torch
+        self.args = args
+        self.stream = torch.cuda.Stream()
+        torch.cuda.set_stream(self.stream)
+        self.peak, self.peak_kind = measured_peaks()
+        self.gpu = gpu_id_for_nvsmi(0)
+        self._flush_buf = None
+        self._flip = 0
+        self.ref = None
+        if not args.no_cpu_baseline:
+            from oracle.oracle import Reference, reference_available
+            if reference_available():
+                self.ref = Reference()
+                self.threads = self.ref.set_threads(os.cpu_count() or 1)
+
+    # -- timing -----------------------------------------------------------
+    def flush(self):
+        """Writes 256 MB (twice the L2) so the next launch starts cold."""
+        if self._flush_buf is None:
+            self._flush_buf = self.torch.empty(256 << 20, dtype=self.torch.uint8, device="cuda")
+        self._flip ^= 1
+        self._flush_buf.fill_(self._flip)
+
+    def time(self, fn, flush=False, budget_s=2.0, max_reps=None):
+        """(seconds per call, calls timed): CUDA events on the bench stream,
+        3 warm-up calls; with flush, each call is timed alone after an L2 flush."""
+        torch = self.torch
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(self.stream)
+        fn()
+        e1.record(self.stream)
+        torch.cuda.synchronize()
+        t1 = max(e0.elapsed_time(e1) * 1e-3, 1e-7)
+        reps = int(min(max_reps or self.args.steps, max(3, budget_s / t1)))
+        if not flush:
+            e0.record(self.stream)
+            for _ in range(reps):
+                fn()
+            e1.record(self.stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) * 1e-3 / reps, reps
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        for a, b in evs:
+            self.flush()
+            a.record(self.stream)
+            fn()
+            b.record(self.stream)
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs) * 1e-3 / reps, reps
+
+    def clocks(self):
+        return ClockSampler(self.gpu)
+
+    # -- reporting --------------------------------------------------------
+    def hbm(self, nbytes, t, kernel, workload=None):
+        a = nbytes / t / 1e9
+        return {"bound": "hbm", "achieved": round(a, 2), "peak": self.peak, "unit": "GB/s",
+                "frac": round(a / self.peak, 4), "peak_source": f"{self.peak_kind} hbm_gbs",
+                "traffic": ncu_traffic(workload) if workload else None,
+                "algorithmic_bytes_per_launch": int(nbytes), "kernel": kernel}
+
+    def cpu(self, timer, nbytes, sample, unit="GB/s"):
+        if self.ref is None:
+            return None
+        t = timer()
+        return {"value": round(nbytes / t / 1e9, 3), "unit": unit, "cores": self.threads, "kind": "reference",
+                "sample": sample, "ms_per_call": round(t * 1e3, 4)}
+
+    def emit(self, workload, metric, value, unit, t, reps, dtype, config, clocks, roofline=None, cpu=None,
+             launches=None, higher=True, **extra):
+        d = {"metric": metric, "value": round(value, 4), "unit": unit, "n_gpus": 1, "steps": reps, "warmup": 3,
+             "ms_per_step": round(t * 1e3, 5), "higher_is_better": higher, "scaling": "weak", "vs_baseline": None,
+             "dtype": dtype, "data": "synthetic (seeded, generated on the host)",
+             "config": dict({"workload": workload}, **config), "roofline": roofline, "cpu_baseline": cpu,
+             "e2e": None, "gpu_launches": launches, "clocks": clocks}
+        d.update(extra)
+        print(json.dumps(d), flush=True)
+        return d
+
+    # -- kernels with device operands ---------------------------------------
+    def kernel(self, ktype, vt, setup=None):
+        from smaxkernels_b200 import FloatType, Interface, IntType, PlatformType
+        smax = Interface()
+        smax.register_kernel("k", ktype, PlatformType.CUDA, IntType.INT32,
+                             FloatType.FLOAT64 if vt == np.float64 else FloatType.FLOAT32)
+        k = smax.kernel("k")
+        if setup:
+            setup(k)
+        return smax, k
+
+    def dev(self, a):
+        return self.torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+    def zeros(self, n, vt):
+        return self.torch.zeros(int(n), dtype=self.torch.float64 if vt == np.float64 else self.torch.float32,
+                                device="cuda")
+
+
+def _dt(vt):
+    return "f64" if vt == np.float64 else "f32"
+
+
+def wl_spmv_laplace64(b: Bench):
+    """CRS SpMV, 7-point 64^3 Laplacian (n = 262,144, nnz = 1,810,432): the
+    27 MB working set is L2-resident, so report L2-flushed and hot."""
+    from smaxkernels_b200 import KernelType
+    from smaxkernels_b200 import matrices as M
+    from smaxkernels_b200.matrices import crs_bytes
+    rp, col, val = M.laplace3d_7pt(64)
+    n, nnz = len(rp) - 1, len(col)
+    x = M.uniform_vector(n, 0)
+    smax, k = b.kernel(KernelType.SPMV, np.float64)
+    xd, yd = b.dev(x), b.zeros(n, np.float64)
+    k.register_A(n, n, nnz, col, rp, val)
+    k.register_B(n, xd)
+    k.register_C(n, yd)
+    k.set_stream(b.stream.cuda_stream)
+    k.initialize()
+    nbytes = crs_bytes(n, nnz, n, 8)
+    with b.clocks() as clk:
+        t_fl, reps = b.time(k.apply, flush=True, budget_s=1.0, max_reps=200)
+        t_hot, _ = b.time(k.apply)
+    cpu = b.cpu(lambda: b.ref.time_spmv_crs(rp, col, val, x, warm=3, reps=100)[0], nbytes,
+                "100 applies after 3 warm-ups (reference OpenMP CRS kernel)")
+    b.emit("crs_spmv_f64_laplace3d_64", "CRS SpMV GB/s (L2-flushed)", nbytes / t_fl / 1e9, "GB/s", t_fl, reps,
+           "f64", {"n_rows": n, "nnz": nnz, "l2": "flushed (256 MB write) before every timed launch"},
+           clk.summary(), b.hbm(nbytes, t_fl, "crs_stream_kernel"), cpu, launches=2 * reps,
+           hot={"value": round(nbytes / t_hot / 1e9, 3), "ms_per_step": round(t_hot * 1e3, 5),
+                "l2": "hot (repeated launches, matrix L2-resident)"})
+    smax.close()
+
+
+def wl_scs_spmv(b: Bench):
+    """SELL-32-1024 SpMV of the lognormal 2^22 matrix, FP64 and FP32."""
+    from smaxkernels_b200 import KernelType
+    from smaxkernels_b200 import matrices as M
+    from smaxkernels_b200.matrices import crs_bytes
+    for vt in (np.float64, np.float32):
+        vb = np.dtype(vt).itemsize
+        rp, col, val = M.lognormal_random(1 << 22, seed=1, dtype=vt)
+        n, nnz = len(rp) - 1, len(col)
+        x = M.uniform_vector(n, 100, vt)
+        smax, k = b.kernel(KernelType.SPMV, vt, lambda k: k.set_mat_scs(True))
+        s = smax.utils.convert_crs_to_scs(n, n, nnz, col, rp, val, 32, 1024)
+        vs = max(s["n_rows_padded"], n)
+        xd = b.zeros(vs, vt)
+        xd[:n] = b.dev(x)
+        yd = b.zeros(vs, vt)
+        k.register_A(32, 1024, s["n_rows"], s["n_rows_padded"], n, s["n_chunks"], s["n_elements"], s["nnz"],
+                     s["chunk_ptr"], s["chunk_lengths"], s["col"], s["val"], s["perm"])
+        k.register_B(vs, xd)
+        k.register_C(vs, yd)
+        k.set_stream(b.stream.cuda_stream)
+        k.initialize()
+        ne, nch, npad = s["n_elements"], s["n_chunks"], s["n_rows_padded"]
+        nbytes = (vb + 4) * ne + 4 * (nch + 1) + 4 * nch + vb * n + vb * npad
+        with b.clocks() as clk:
+            t, reps = b.time(k.apply)
+        cpu = b.cpu(lambda: b.ref.time_spmv_scs(s, x, warm=1, reps=20), nbytes,
+                    "20 applies after 1 warm-up (reference OpenMP SELL-C-sigma kernel)")
+        b.emit(f"scs_spmv_{_dt(vt)}_lognormal_4194304", "SELL-C-sigma SpMV GB/s (stored bytes)",
+               nbytes / t / 1e9, "GB/s", t, reps, _dt(vt),
+               {"C": 32, "sigma": 1024, "n_rows": n, "nnz": nnz, "n_elements": ne,
+                "l2": "inputs larger than L2 (no flush)"},
+               clk.summary(), b.hbm(nbytes, t, "scs_warp_kernel"), cpu, launches=reps,
+               crs_equivalent_gbs=round(crs_bytes(n, nnz, n, vb) / t / 1e9, 3),
+               gflops=round(2 * nnz / t / 1e9, 3))
+        smax.close()
+        del xd, yd
+        b.torch.cuda.empty_cache()
+
+
+def wl_bcrs_spmv(b: Bench):
+    """4x4 BCRS SpMV of the lognormal 2^22 matrix, FP64 (n_blocks ~ nnz)."""
+    from smaxkernels_b200 import KernelType
+    from smaxkernels_b200 import matrices as M
+    from smaxkernels_b200.matrices import crs_bytes
+    vt, vb = np.float64, 8
+    rp, col, val = M.lognormal_random(1 << 22, seed=1, dtype=vt)
+    n, nnz = len(rp) - 1, len(col)
+    x = M.uniform_vector(n, 100, vt)
+    smax, k = b.kernel(KernelType.SPMV, vt, lambda k: k.set_mat_bcrs(True))
+    bc = smax.utils.convert_crs_to_bcrs(n, n, nnz, col, rp, val, 4, 4, 4, 4, False)
+    del rp, col, val
+    xd, yd = b.dev(x), b.zeros(n, vt)
+    k.register_A(bc["n_rows"], bc["n_cols"], bc["n_blocks"], 4, 4, 4, 4, bc["col"], bc["row_ptr"], bc["val"])
+    k.register_B(n, xd)
+    k.register_C(n, yd)
+    k.set_stream(b.stream.cuda_stream)
+    k.initialize()
+    nb = bc["n_blocks"]
+    nbytes = (16 * vb + 4) * nb + 4 * (bc["n_rows"] + 1) + vb * n + vb * n
+    with b.clocks() as clk:
+        t, reps = b.time(k.apply, budget_s=3.0)
+    cpu = b.cpu(lambda: b.ref.time_spmv_bcrs(bc, x, False, warm=1, reps=5), nbytes,
+                "5 applies after 1 warm-up (reference OpenMP BCRS kernel)")
+    b.emit("bcrs4x4_spmv_f64_lognormal_4194304", "BCRS SpMV GB/s (stored bytes)", nbytes / t / 1e9, "GB/s", t,
+           reps, "f64", {"block": "4x4", "n_blocks": nb, "nnz": nnz, "l2": "inputs larger than L2 (no flush)"},
+           clk.summary(), b.hbm(nbytes, t, "bcrs_stream_kernel"), cpu, launches=reps,
+           crs_equivalent_gbs=round(crs_bytes(n, nnz, n, vb) / t / 1e9, 3), gflops=round(2 * nnz / t / 1e9, 3))
+    smax.close()
+
+
+def wl_spmm(b: Bench):
+    """Row-major SpMM with the 27-point 128^3 stencil (n = 2,097,152,
+    nnz = 55,742,968), k = 16 and 64 vectors, FP64 and FP32."""
+    from smaxkernels_b200 import KernelType
+    from smaxkernels_b200 import matrices as M
+    for vt in (np.float64, np.float32):
+        vb = np.dtype(vt).itemsize
+        rp, col, val = M.stencil27(128, dtype=vt)
+        n, nnz = len(rp) - 1, len(col)
+        for kv in (16, 64):
+            X = np.random.default_rng(2).uniform(-1, 1, n * kv).astype(vt)
+            smax, k = b.kernel(KernelType.SPMM, vt, lambda k: k.set_vec_row_major(True))
+            Xd, Yd = b.dev(X), b.zeros(n * kv, vt)
+            k.register_A(n, n, nnz, col, rp, val)
+            k.register_B(n, kv, Xd)
+            k.register_C(n, kv, Yd)
+            k.set_stream(b.stream.cuda_stream)
+            k.initialize()
+            nbytes = (vb + 4) * nnz + 4 * (n + 1) + 2 * vb * n * kv
+            with b.clocks() as clk:
+                t, reps = b.time(k.apply)
+            cpu = b.cpu(lambda: b.ref.time_spmm(rp, col, val, X, kv, True, warm=1, reps=5), nbytes,
+                        "5 applies after 1 warm-up (reference OpenMP row-major SpMM)")
+            b.emit(f"spmm_rowmajor_k{kv}_{_dt(vt)}_stencil27_128", "SpMM GB/s", nbytes / t / 1e9, "GB/s", t, reps,
+                   _dt(vt), {"n_rows": n, "nnz": nnz, "k": kv, "layout": "row-major X, Y",
+                             "l2": "inputs larger than L2 (no flush)"},
+                   clk.summary(), b.hbm(nbytes, t, "spmm_row_major_kernel"), cpu, launches=reps,
+                   gflops=round(2 * nnz * kv / t / 1e9, 3))
+            smax.close()
+            del Xd, Yd
+            b.torch.cuda.empty_cache()
+
+
+def wl_spgemm(b: Bench):
+    """C = A*A with the 7-point 96^3 Laplacian (n = 884,736, nnz(A) =
+    6,137,856, nnz(C) = 21,732,480), FP64: symbolic + numeric per apply."""
+    from smaxkernels_b200 import KernelType
+    from smaxkernels_b200 import matrices as M
+    rp, col, val = M.laplace3d_7pt(96)
+    n, nnz = len(rp) - 1, len(col)
+    smax, k = b.kernel(KernelType.SPGEMM, np.float64)
+    k.register_A(n, n, nnz, col, rp, val)
+    k.register_B(n, n, nnz, col, rp, val)
+    k.register_C()
+    k.set_stream(b.stream.cuda_stream)
+    k.initialize()
+    k.apply()
+    k.finalize()
+    c = k.result()
+    nnz_c = int(c[2])
+    lens = np.diff(rp)
+    products = int(lens[col].sum())  # sum over A's entries of the length of B's row
+    a_bytes = 12 * nnz + 4 * (n + 1)
+    nbytes = 2 * a_bytes + 2 * a_bytes + 12 * nnz_c + 4 * (n + 1)
+    with b.clocks() as clk:
+        t, reps = b.time(k.apply, budget_s=2.0, max_reps=200)
+    cpu = b.cpu(lambda: b.ref.time_spgemm(rp, col, val, reps=3), nbytes,
+                "3 applies (reference OpenMP symbolic + numeric phases)")
+    b.emit("spgemm_f64_laplace3d_96", "SpGEMM GB/s (2A + 2B + C bytes)", nbytes / t / 1e9, "GB/s", t, reps, "f64",
+           {"n_rows": n, "nnz_a": nnz, "nnz_c": nnz_c, "products": products,
+            "l2": "A, B (77 MB) L2-resident across the fused pass"},
+           clk.summary(), b.hbm(nbytes, t, "gustavson_warp"), cpu, launches=None,
+           gflops=round(2 * products / t / 1e9, 3), reference_gflops_2nnzC=round(2 * nnz_c / t / 1e9, 3))
+    smax.close()
+
+
+def _tri_bytes(n, nnz, vb, kv=1):
+    return (vb + 4) * nnz + 4 * (n + 1) + vb * n + 2 * vb * n * kv
+
+
+def wl_sptrsv(b: Bench):
+    """SpTRSV / SpTRSM, lower triangle of the 5-point 2048^2 Laplacian
+    (n = 4,194,304, nnz = 12,578,816): natural order (4095 levels) in every
+    launch scheme, the permuted level-scheduled flow, and k = 32 rows-major."""
+    from smaxkernels_b200 import KernelType
+    from smaxkernels_b200 import matrices as M
+    vt, vb = np.float64, 8
+    A = M.laplace2d_5pt(2048)
+    rp, col, val = M.lower_triangle(*A)
+    n, nnz = len(rp) - 1, len(col)
+    n_lv = 2 * 2048 - 1
+    rhs = M.uniform_vector(n, 3)
+    names = {1: "per_level", 2: "merged", 3: "graph", 4: "persistent"}
+    results = {}
+    for mode in (1, 2, 3, 4):
+        smax, k = b.kernel(KernelType.SPTRSV, vt, lambda k: k.set_solve_mode(mode))
+        xd, bd = b.zeros(n, vt), b.dev(rhs)
+        k.register_A(n, n, nnz, col.copy(), rp, val.copy())
+        k.register_B(n, xd)
+        k.register_C(n, bd)
+        k.set_stream(b.stream.cuda_stream)
+        k.initialize()
+        nbytes = _tri_bytes(n, nnz, vb)
+        with b.clocks() as clk:
+            t, reps = b.time(k.apply, budget_s=2.0, max_reps=100)
+        results[mode] = t
+        cpu = None
+        if mode == 3:
+            cpu = b.cpu(lambda: b.ref.time_sptrsv(rp, col, val, rhs, warm=1, reps=3)[0], nbytes,
+                        "3 solves after 1 warm-up (reference naive_crs_sptrsv, serial)")
+        b.emit(f"sptrsv_f64_laplace2d_2048_natural_{names[mode]}", "SpTRSV GB/s", nbytes / t / 1e9, "GB/s", t,
+               reps, "f64", {"n_rows": n, "nnz": nnz, "levels": n_lv, "scheme": names[mode]}, clk.summary(),
+               b.hbm(nbytes, t, "level_kernel/segment_kernel"), cpu,
+               launches=n_lv * reps if mode == 1 else (reps if mode == 4 else None),
+               us_per_level=round(t * 1e6 / n_lv, 4))
+        smax.close()
+    # permuted flow: random symmetric permutation (seed 3), RS levels, level order
+    Ar, Ac, Av, _ = M.random_symmetric_permutation(*A, seed=3)
+    smax, k = b.kernel(KernelType.SPTRSV, vt)
+    perm = np.zeros(n, np.int32)
+    inv = np.zeros(n, np.int32)
+    smax.utils.generate_perm(n, Ar, Ac, perm, inv, "RS")
+    prp = np.zeros(n + 1, np.int32)
+    pcol = np.zeros(len(Ac), np.int32)
+    pval = np.zeros(len(Ac))
+    smax.utils.apply_mat_perm(n, Ar, Ac, Av, prp, pcol, pval, perm, inv)
+    lrp, lcol, lval = M.lower_triangle(prp, pcol, pval)
+    lvl = np.array([smax.get_level_ptr_at(i) for i in range(smax.get_n_levels() + 1)], np.int32)
+    nl = len(lvl) - 1
+    for mode in (3, 4):
+        smax.register_kernel(f"p{mode}", KernelType.SPTRSV, *b_types(vt))
+        k = smax.kernel(f"p{mode}")
+        k.set_mat_perm(True)
+        k.set_solve_mode(mode)
+        xd, bd = b.zeros(n, vt), b.dev(rhs)
+        k.register_A(n, n, len(lcol), lcol.copy(), lrp, lval.copy())
+        k.register_B(n, xd)
+        k.register_C(n, bd)
+        k.set_stream(b.stream.cuda_stream)
+        k.initialize()
+        nbytes = _tri_bytes(n, len(lcol), vb)
+        with b.clocks() as clk:
+            t, reps = b.time(k.apply, budget_s=2.0, max_reps=200)
+        cpu = None
+        if mode == 3:
+            cpu = b.cpu(lambda: b.ref.time_sptrsv(lrp, lcol, lval, rhs, levels=lvl, warm=1, reps=5)[0], nbytes,
+                        "5 solves after 1 warm-up (reference crs_sptrsv_lvl, OpenMP within levels)")
+        b.emit(f"sptrsv_f64_laplace2d_2048_permuted_{names[mode]}", "SpTRSV GB/s", nbytes / t / 1e9, "GB/s", t,
+               reps, "f64", {"n_rows": n, "nnz": len(lcol), "levels": nl, "scheme": names[mode],
+                             "ordering": "random symmetric permutation (seed 3), RS level order"},
+               clk.summary(), b.hbm(nbytes, t, "level_kernel/segment_kernel"), cpu,
+               launches=reps if mode == 4 else None, us_per_level=round(t * 1e6 / max(nl, 1), 4))
+    smax.close()
+    # SpTRSM, k = 32 right-hand sides, row-major
+    kv = 32
+    B = np.random.default_rng(3).uniform(-1, 1, n * kv)
+    smax, k = b.kernel(KernelType.SPTRSM, vt, lambda k: k.set_vec_row_major(True))
+    Xd, Bd = b.zeros(n * kv, vt), b.dev(B)
+    k.register_A(n, n, nnz, col.copy(), rp, val.copy())
+    k.register_B(n, kv, Xd)
+    k.register_C(n, kv, Bd)
+    k.set_stream(b.stream.cuda_stream)
+    k.initialize()
+    nbytes = _tri_bytes(n, nnz, vb, kv)
+    with b.clocks() as clk:
+        t, reps = b.time(k.apply, budget_s=2.0, max_reps=50)
+    cpu = b.cpu(lambda: b.ref.time_sptrsm(rp, col, val, B, kv, True, warm=0, reps=1), nbytes,
+                "1 solve (reference naive row-major SpTRSM, serial)")
+    b.emit("sptrsm_k32_f64_laplace2d_2048_natural_graph", "SpTRSM GB/s", nbytes / t / 1e9, "GB/s", t, reps,
+           "f64", {"n_rows": n, "nnz": nnz, "k": kv, "levels": n_lv, "layout": "row-major"}, clk.summary(),
+           b.hbm(nbytes, t, "level_kernel/segment_kernel"), cpu, us_per_level=round(t * 1e6 / n_lv, 4))
+    smax.close()
+
+
+def b_types(vt):
+    from smaxkernels_b200 import FloatType, IntType, PlatformType
+    return (PlatformType.CUDA, IntType.INT32, FloatType.FLOAT64 if vt == np.float64 else FloatType.FLOAT32)
+
+
+def wl_sptrsv_batch(b: Bench):
+    """64 lower triangles of 5-point Laplacians, sides 100 + round(600 i / 63):
+    one persistent graph-captured launch vs one launch per level per matrix."""
+    from smaxkernels_b200 import matrices as M
+    from smaxkernels_b200.interface import TriangularBatch
+    sides = [100 + int(round(600 * i / 63)) for i in range(64)]
+    mats = [M.lower_triangle(*M.laplace2d_5pt(s)) for s in sides]
+    tb = TriangularBatch(mats)
+    n, total_levels, max_levels = tb.info()
+    nnz = sum(len(m[1]) for m in mats)
+    rhs = np.random.default_rng(3).uniform(-1, 1, n)
+    bd, xd = b.dev(rhs), b.zeros(n, np.float64)
+    nbytes = _tri_bytes(n, nnz, 8)
+    times = {}
+    names = {3: "persistent_graph", 2: "persistent", 1: "per_level"}
+    for mode in (3, 2, 1):
+        fn = lambda: tb.solve(bd, xd, mode, b.stream.cuda_stream)
+        with b.clocks() as clk:
+            t, reps = b.time(fn, budget_s=2.0, max_reps=200)
+        times[mode] = t
+        cpu = None
+        if mode == 3 and b.ref is not None:
+            def ref_time():
+                return sum(b.ref.time_sptrsv(rp, c, v, np.ones(len(rp) - 1), warm=0, reps=1)[0]
+                           for rp, c, v in mats)
+            cpu = b.cpu(ref_time, nbytes, "1 solve of each of the 64 matrices (reference naive_crs_sptrsv)")
+        b.emit(f"sptrsv_batch64_f64_laplace2d_{names[mode]}", "batched SpTRSV GB/s", nbytes / t / 1e9, "GB/s", t,
+               reps, "f64", {"matrices": 64, "n_rows": n, "nnz": nnz, "total_levels": total_levels,
+                             "max_levels": max_levels, "scheme": names[mode]}, clk.summary(),
+               b.hbm(nbytes, t, "batch_sptrsv_kernel"), cpu,
+               launches=total_levels * reps if mode == 1 else reps,
+               speedup_vs_per_level=(round(times[1] / t, 3) if 1 in times else None))
+    tb.close()
+
+
+def wl_sptrsv_refine(b: Bench):
+    """FP32 solve + FP64-residual refinement vs the FP64 solve, to 1e-12,
+    natural and permuted 2048^2 triangles."""
+    from smaxkernels_b200 import KernelType
+    from smaxkernels_b200 import matrices as M
+    A = M.laplace2d_5pt(2048)
+    rp, col, val = M.lower_triangle(*A)
+    n, nnz = len(rp) - 1, len(col)
+    rhs = M.uniform_vector(n, 3)
+    bd = b.dev(rhs)
+    out = {}
+    for steps in (0, 2):
+        smax, k = b.kernel(KernelType.SPTRSV, np.float64, lambda k: k.set_refine(steps))
+        xd = b.zeros(n, np.float64)
+        k.register_A(n, n, nnz, col.copy(), rp, val.copy())
+        k.register_B(n, xd)
+        k.register_C(n, bd)
+        k.set_stream(b.stream.cuda_stream)
+        k.initialize()
+        with b.clocks() as clk:
+            t, reps = b.time(k.apply, budget_s=2.0, max_reps=100)
+        b.torch.cuda.synchronize()
+        out[steps] = (t, reps, xd.clone(), clk.summary())
+        smax.close()
+    t64, _, x64, _ = out[0]
+    t32, reps, x32, clk = out[2]
+    err = float(b.torch.linalg.norm(x32 - x64) / b.torch.linalg.norm(x64))
+    nbytes = _tri_bytes(n, nnz, 8)
+    b.emit("sptrsv_refine2_vs_f64_laplace2d_2048_natural", "refined FP32 SpTRSV speed-up over FP64",
+           t64 / t32, "x", t32, reps, "f32+f64", {"n_rows": n, "nnz": nnz, "corrections": 2}, clk,
+           b.hbm(nbytes, t32, "level kernels (FP32) + residual_kernel"), None,
+           fp64_ms=round(t64 * 1e3, 4), refined_ms=round(t32 * 1e3, 4), rel_diff_vs_fp64=err)
+
+
+def wl_adjoint(b: Bench):
+    """Adjoint vs forward time: y = A x (7-point 64^3) and x = L^-1 b (lower
+    5-point 512^2, 1023 levels), FP64; the adjoint computes d_in and d_val."""
+    from smaxkernels_b200 import matrices as M
+    from smaxkernels_b200.autograd import SparsePattern
+    torch = b.torch
+    cases = [("spmv_laplace3d_64", "spmv", M.laplace3d_7pt(64)),
+             ("sptrsv_laplace2d_512", "sptrsv", M.lower_triangle(*M.laplace2d_5pt(512)))]
+    for name, kind, (rp, col, val) in cases:
+        n, nnz = len(rp) - 1, len(col)
+        P = SparsePattern(rp, col, kind=kind)
+        v = b.dev(val)
+        xin = b.dev(M.uniform_vector(n, 4))
+        P.forward(v, xin)
+        xs = P._out.clone()  # the solve's x (or any x for SpMV)
+        x_for_adj = xin if kind == "spmv" else xs
+        P.k.set_stream(b.stream.cuda_stream)
+        with b.clocks() as clk:
+            tf, reps = b.time(P.k.apply, budget_s=1.0)
+            ta, _ = b.time(lambda: P.k.adjoint(P._g, P._din, P._dval, x=x_for_adj), budget_s=1.0)
+        b.emit(f"adjoint_{name}_f64", "adjoint time / forward time", ta / tf, "ratio", ta, reps, "f64",
+               {"n_rows": n, "nnz": nnz, "outputs": "d_in and d_val"}, clk.summary(), None, None, higher=False,
+               forward_ms=round(tf * 1e3, 5), adjoint_ms=round(ta * 1e3, 5))
+        del P
+        torch.cuda.empty_cache()
+
+
+def run_extra(args):
+    import torch
+    torch.cuda.set_device(0)
+    b = Bench(args)
+    names = EXTRA_WORKLOADS if args.workload == "all" else (args.workload,)
+    for nm in names:
+        log(f"[bench] workload {nm}")
+        globals()[f"wl_{nm}"](b)
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -210,10 +707,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=N_ROWS, help="rows per rank (default 2^22)")
     ap.add_argument("--variant", type=int, default=0, help="CRS kernel: 0 auto, 1 warp-stream, 2 row-tile")
+    ap.add_argument("--workload", default="crs_spmv", choices=("crs_spmv", "all") + EXTRA_WORKLOADS,
+                    help="crs_spmv (the headline line) or another workload of the hot path (1 GPU)")
     args = ap.parse_args()
     globals()["N_ROWS"] = args.rows
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "crs_spmv":
+        return run_extra(args)
 
     import torch
     import torch.distributed as dist

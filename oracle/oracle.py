@@ -328,6 +328,8 @@ class Reference:
                                       _INT, _INT]
         L.ref_time_sptrsv.restype = C.c_double
         L.ref_sptrsm.argtypes = [_INT, _INT, _INT, _U64, _U64, _U64, _P, _P, _P, _U64, _P, _P]
+        L.ref_time_sptrsm.argtypes = [_INT, _INT, _U64, _U64, _U64, _P, _P, _P, _U64, _P, _P, _INT, _INT]
+        L.ref_time_sptrsm.restype = C.c_double
         L.ref_convert_crs_to_scs.argtypes = [_INT, _U64, _U64, _U64, _P, _P, _P, _U64, _U64, _P] + \
             [C.POINTER(_P)] * 5
         L.ref_convert_crs_to_bcrs.argtypes = [_INT, _U64, _U64, _U64, _P, _P, _P, _U64, _U64, _U64, _U64,
@@ -444,6 +446,54 @@ class Reference:
         if t < 0:
             self._check(-1)
         return t, x
+
+    # -- timers (seconds per apply after `warm` applies) -----------------------
+    def _t(self, t):
+        if t < 0:
+            self._check(-1)
+        return t
+
+    def time_spmv_scs(self, s, x, warm=1, reps=10):
+        vs = max(s["n_rows_padded"], len(x))
+        xx = np.zeros(vs, dtype=s["val"].dtype)
+        xx[: len(x)] = x
+        y = np.zeros(vs, dtype=s["val"].dtype)
+        return self._t(self.lib.ref_time_spmv_scs(
+            _vbits(s["val"].dtype), s["C"], s["sigma"], s["n_rows"], s["n_rows_padded"], len(x), s["n_chunks"],
+            s["n_elements"], s["nnz"], _p(_i32(s["chunk_ptr"])), _p(_i32(s["chunk_lengths"])),
+            _p(_i32(s["col"])), _p(s["val"]), _p(_i32(s["perm"])), _p(xx), _p(y), warm, reps))
+
+    def time_spmv_bcrs(self, b, x, col_major=False, warm=1, reps=10):
+        y = np.zeros(b["n_rows"] * b["height_pad"], dtype=b["val"].dtype)
+        x = np.ascontiguousarray(x, b["val"].dtype)
+        return self._t(self.lib.ref_time_spmv_bcrs(
+            _vbits(b["val"].dtype), b["n_rows"], b["n_cols"], b["n_blocks"], b["b_height"], b["b_width"],
+            b["height_pad"], b["width_pad"], _p(_i32(b["col"])), _p(_i32(b["row_ptr"])), _p(b["val"]),
+            int(bool(col_major)), _p(x), _p(y), warm, reps))
+
+    def time_spmm(self, row_ptr, col, val, X, k, row_major=True, warm=1, reps=10):
+        rp, cl = _i32(row_ptr), _i32(col)
+        n = len(rp) - 1
+        Y = np.zeros(n * k, dtype=val.dtype)
+        X = np.ascontiguousarray(X, val.dtype).ravel()
+        return self._t(self.lib.ref_time_spmm(_vbits(val.dtype), int(bool(row_major)), n, n, len(cl), _p(cl),
+                                              _p(rp), _p(val), k, _p(X), _p(Y), warm, reps))
+
+    def time_spgemm(self, row_ptr, col, val, reps=3):
+        """C = A*A: seconds of apply() (symbolic + numeric phases)."""
+        rp, cl = _i32(row_ptr), _i32(col)
+        n = len(rp) - 1
+        return self._t(self.lib.ref_time_spgemm(_vbits(val.dtype), n, n, len(cl), _p(cl), _p(rp), _p(val), reps))
+
+    def time_sptrsm(self, row_ptr, col, val, B, k, row_major=True, warm=1, reps=5):
+        rp = _i32(row_ptr)
+        cl = _i32(col).copy()
+        vv = val.copy()
+        n = len(rp) - 1
+        X = np.zeros(n * k, dtype=val.dtype)
+        BB = np.ascontiguousarray(B, val.dtype).ravel().copy()
+        return self._t(self.lib.ref_time_sptrsm(_vbits(val.dtype), int(bool(row_major)), n, n, len(cl), _p(cl),
+                                                _p(rp), _p(vv), k, _p(X), _p(BB), warm, reps))
 
     def sptrsm(self, row_ptr, col, val, B, k, row_major=True):
         rp = _i32(row_ptr)

@@ -408,6 +408,26 @@ int ref_sptrsm(int vbits, int row_major, int upper, uint64_t n_rows,
     });
 }
 
+double ref_time_sptrsm(int vbits, int row_major, uint64_t n_rows,
+                       uint64_t n_cols, uint64_t nnz, int *col, int *row_ptr,
+                       void *val, uint64_t k, void *X, void *B, int warm,
+                       int reps) {
+    double t = -1.0;
+    int rc = guarded([&] {
+        SMAX::Interface smax;
+        smax.register_kernel("k", SMAX::KernelType::SPTRSM,
+                             SMAX::PlatformType::CPU, SMAX::IntType::INT32,
+                             ftype(vbits));
+        smax.kernel("k")->register_A(n_rows, n_cols, nnz, col, row_ptr, val);
+        smax.kernel("k")->register_B(n_cols, k, X);
+        smax.kernel("k")->register_C(n_rows, k, B);
+        smax.kernel("k")->set_vec_row_major(row_major != 0);
+        t = time_applies(&smax, "k", warm, reps);
+        return 0;
+    });
+    return rc == 0 ? t : -1.0;
+}
+
 // ------------------------------------------------------------- conversions --
 int ref_convert_crs_to_scs(int vbits, uint64_t n_rows, uint64_t n_cols,
                            uint64_t nnz, const int *col, const int *row_ptr,
