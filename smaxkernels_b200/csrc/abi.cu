@@ -220,9 +220,9 @@ template <typename VT> void tri_apply_t(smax_kernel_s *k, const VT *Bv, VT *Xv) 
         return;
     }
     if (k->solve_mode == SMAX_SOLVE_AUTO || k->solve_mode == SMAX_SOLVE_GRAPH)
-        tri_solve_graph<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, kk, rm, ld, merge, k->stream);
+        tri_solve_graph<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, kk, rm, ld, merge, k->vals_version, k->stream);
     else
-        tri_solve<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, kk, rm, ld, merge, k->stream);
+        tri_solve<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, kk, rm, ld, merge, k->vals_version, k->stream);
 }
 
 // ------------------------------------------------------------------ SpGEMM --

@@ -63,9 +63,9 @@ template <typename VT> void adjoint_t(smax_kernel_s *k, const VT *x, const VT *g
     }
     const int merge = tri_merge_rows(k);
     if (k->solve_mode == SMAX_SOLVE_AUTO || k->solve_mode == SMAX_SOLVE_GRAPH)
-        tri_solve_graph<VT>(k->adj_plan, k->adj.at, k->D.as<VT>(), g, lam, 1, true, n, merge, st);
+        tri_solve_graph<VT>(k->adj_plan, k->adj.at, k->D.as<VT>(), g, lam, 1, true, n, merge, k->vals_version, st);
     else
-        tri_solve<VT>(k->adj_plan, k->adj.at, k->D.as<VT>(), g, lam, 1, true, n, merge, st);
+        tri_solve<VT>(k->adj_plan, k->adj.at, k->D.as<VT>(), g, lam, 1, true, n, merge, k->vals_version, st);
     if (dval) sddmm_outer<VT>(k->dA, k->adj.row_of.as<int>(), VT(-1), lam, x, dval, st);
 }
 

@@ -1,0 +1,448 @@
+// levelpack.cu -- level-ordered packed triangular solves on sm_100a.
+//
+// The per-row recurrence is the reference's (naive_crs_sptrsv / crs_sptrsv_lvl,
+// src/kernels/sptrsv/sptrsv_cpu/sptrsv_cpu_crs_impl.hpp:9-55,
+// sptrsv_lvl_cpu_crs_impl.hpp:11-82): x[r] = (b[r] - sum_j val[j] x[col[j]]) / D[r]
+// with the off-diagonal entries summed in stored order.  What changes is the
+// layout, for latency: a level-scheduled solve of a matrix with thousands of
+// narrow levels is a chain of dependent steps, and in the plain layout every
+// step waits on order -> row_ptr -> col/val -> x, four dependent global loads.
+//
+// * Rows are renumbered in sweep order ("positions") and each level's
+//   off-diagonal entries are stored as a dense column-major block, so a thread
+//   finds its row's entries at a fixed offset: no row_ptr hop, coalesced loads.
+// * The single-CTA sweep over a run of narrow levels keeps the last kRing
+//   solutions in a shared-memory ring indexed by position; an entry whose
+//   solution is guaranteed to still be in the ring is encoded with its slot
+//   at pack time (the ring slot of position q is q % kRing; it survives until
+//   position q + kRing is written, so it is safe while q >= level_end - kRing).
+// * While a level is computed, each thread already loads the next level's
+//   entries, right-hand sides and diagonals into registers, and the block
+//   prefetches the level after that into L2: the critical path per level is
+//   ring reads, a few FMAs, the division and the CTA barrier.
+// * Right-hand sides are gathered into position order before the sweep and
+//   the solution scattered back after it (two coalesced passes over n).
+#include "levelpack.cuh"
+
+#include <algorithm>
+
+#include <cub/device/device_segmented_reduce.cuh>
+
+namespace smax {
+
+namespace {
+
+using Level = LevelPack::Level;
+constexpr int kPad = LevelPack::kPad;
+constexpr int kRing = LevelPack::kRing;
+constexpr int kSweepThreads = 1024;
+constexpr int kRowsPerThread = 2;  // rows of a level held in registers per thread
+constexpr int kEnts = 2;           // prefetched entries per row (the rest are loaded when used)
+
+unsigned grid_for(int64_t work) {
+    const int64_t cap = (int64_t)sm_count() * 8;
+    int64_t g = (work + 255) / 256;
+    return (unsigned)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+// ---------------------------------------------------------------- build ----
+__global__ void positions_kernel(const int *__restrict__ pos_begin, int n_lv, const int *__restrict__ src_begin,
+                                 const int *__restrict__ order, int64_t n, int *__restrict__ prow,
+                                 int *__restrict__ plev, int *__restrict__ pos_of_row) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        int lo = 0, hi = n_lv - 1;  // last s with pos_begin[s] <= p
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (pos_begin[mid] <= p) lo = mid;
+            else hi = mid - 1;
+        }
+        const int k = src_begin[lo] + (int)(p - pos_begin[lo]);
+        const int r = order ? order[k] : k;
+        prow[p] = r;
+        plev[p] = lo;
+        pos_of_row[r] = (int)p;
+    }
+}
+
+__global__ void off_len_kernel(const int *__restrict__ rp, const int *__restrict__ prow, int64_t n,
+                               int *__restrict__ len) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        const int r = prow[p];
+        len[p] = rp[r + 1] - rp[r] - 1;
+    }
+}
+
+template <typename W>
+__global__ void fill_kernel(const int *__restrict__ rp, const int *__restrict__ ci, const W *__restrict__ val,
+                            const W *__restrict__ D, int64_t n, const int *__restrict__ prow,
+                            const int *__restrict__ plev, const int *__restrict__ pos_of_row,
+                            const Level *__restrict__ lv, const int *__restrict__ seg_pos, int *__restrict__ psrc,
+                            W *__restrict__ pval, W *__restrict__ pD, int *needs_init) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        const int s = plev[p];
+        const Level L = lv[s];
+        const int t = (int)(p - L.pos);
+        const int r = prow[p];
+        const int j0 = rp[r], len = rp[r + 1] - j0 - 1;
+        const int segb = seg_pos[s], le = L.pos + L.m;
+        for (int i = 0; i < L.w; ++i) {
+            const long long idx = L.base + (long long)i * L.m + t;
+            if (i < len) {
+                const int q = pos_of_row[ci[j0 + i]];
+                if (q >= L.pos) atomicExch(needs_init, 1);
+                const bool ring = q >= segb && q < L.pos && q >= le - kRing;
+                psrc[idx] = ring ? -(q % kRing) - 1 : q;
+                pval[idx] = val[j0 + i];
+            } else {
+                psrc[idx] = kPad;
+                pval[idx] = W(0);
+            }
+        }
+        pD[p] = D[r];
+    }
+}
+
+// ---------------------------------------------------------------- solve ----
+template <typename VT>
+__global__ void gather_kernel(const int *__restrict__ prow, int64_t n, const VT *__restrict__ B, VT *__restrict__ bp,
+                              const VT *__restrict__ X, VT *__restrict__ xp) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        const int r = prow[p];
+        bp[p] = B[r];
+        if (xp) xp[p] = X[r];
+    }
+}
+
+template <typename VT>
+__global__ void scatter_kernel(const int *__restrict__ prow, int64_t n, const VT *__restrict__ xp, VT *__restrict__ X) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) X[prow[p]] = xp[p];
+}
+
+// one wide level: thread per row
+template <typename VT>
+__global__ void wide_level_kernel(Level L, const int *__restrict__ psrc, const VT *__restrict__ pval,
+                                  const VT *__restrict__ pD, const VT *__restrict__ bp, VT *xp) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= L.m) return;
+    VT sum = VT(0);
+    for (int i = 0; i < L.w; ++i) {
+        const long long idx = L.base + (long long)i * L.m + t;
+        const int src = psrc[idx];
+        if (src == kPad) break;
+        sum += pval[idx] * xp[src];
+    }
+    const int p = L.pos + t;
+    xp[p] = (bp[p] - sum) / pD[p];
+}
+
+template <typename VT> struct RowRegs {
+    int src[kEnts];
+    VT v[kEnts];
+    VT b, d;
+};
+
+__device__ __forceinline__ Level load_level(const Level *lv, int s) {
+    Level L;
+    L.pos = lv[s].pos;
+    L.m = lv[s].m;
+    L.w = lv[s].w;
+    L.base = lv[s].base;
+    return L;
+}
+
+template <typename VT>
+__device__ __forceinline__ void load_rows(const Level &L, const int *__restrict__ psrc, const VT *__restrict__ pval,
+                                          const VT *__restrict__ pD, const VT *__restrict__ bp, RowRegs<VT> (&R)[kRowsPerThread]) {
+#pragma unroll
+    for (int k = 0; k < kRowsPerThread; ++k) {
+        const int t = threadIdx.x + k * kSweepThreads;
+#pragma unroll
+        for (int i = 0; i < kEnts; ++i) R[k].src[i] = kPad;
+        if (t < L.m) {
+            const int p = L.pos + t;
+            R[k].b = bp[p];
+            R[k].d = pD[p];
+#pragma unroll
+            for (int i = 0; i < kEnts; ++i)
+                if (i < L.w) {
+                    const int idx = L.base + i * L.m + t;
+                    R[k].src[i] = psrc[idx];
+                    R[k].v[i] = pval[idx];
+                }
+        }
+    }
+}
+
+// every thread prefetches a few 128-byte lines of level L's data into L2
+template <typename VT>
+__device__ __forceinline__ void prefetch_level_l2(const Level &L, const int *psrc, const VT *pval, const VT *pD,
+                                                  const VT *bp) {
+    const int t = threadIdx.x;
+    const long long ne = (long long)L.m * L.w;
+    const char *r0 = reinterpret_cast<const char *>(psrc + L.base);
+    const char *r1 = reinterpret_cast<const char *>(pval + L.base);
+    const char *r2 = reinterpret_cast<const char *>(pD + L.pos);
+    const char *r3 = reinterpret_cast<const char *>(bp + L.pos);
+    const long long b0 = ne * 4, b1 = ne * (long long)sizeof(VT), b2 = (long long)L.m * sizeof(VT);
+    for (long long o = (long long)t * 128; o < b0; o += 128LL * kSweepThreads)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(r0 + o));
+    for (long long o = (long long)t * 128; o < b1; o += 128LL * kSweepThreads)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(r1 + o));
+    for (long long o = (long long)t * 128; o < b2; o += 128LL * kSweepThreads) {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(r2 + o));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(r3 + o));
+    }
+}
+
+template <typename VT>
+__device__ __forceinline__ VT solution(int src, const VT *ring, const VT *xp) {
+    return src < 0 ? ring[-src - 1] : xp[src];
+}
+
+// Sweeps steps [s0, s1) of the pack in one CTA.
+template <typename VT>
+__device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const int *__restrict__ psrc,
+                          const VT *__restrict__ pval, const VT *__restrict__ pD, const VT *__restrict__ bp, VT *xp,
+                          VT *ring) {
+    if (s0 >= s1) return;
+    RowRegs<VT> cur[kRowsPerThread], nxt[kRowsPerThread];
+    Level Lc = load_level(lv, s0);
+    Level Ln = load_level(lv, s0 + 1 < s1 ? s0 + 1 : s0);
+    load_rows<VT>(Lc, psrc, pval, pD, bp, cur);
+    for (int s = s0; s < s1; ++s) {
+        const Level Lnn = load_level(lv, s + 2 < s1 ? s + 2 : s);
+        if (s + 1 < s1) load_rows<VT>(Ln, psrc, pval, pD, bp, nxt);
+        if (s + 2 < s1) prefetch_level_l2<VT>(Lnn, psrc, pval, pD, bp);
+#pragma unroll
+        for (int k = 0; k < kRowsPerThread; ++k) {
+            const int t = threadIdx.x + k * kSweepThreads;
+            if (t < Lc.m) {
+                VT sum = VT(0);
+                bool more = true;
+#pragma unroll
+                for (int i = 0; i < kEnts; ++i) {
+                    const int src = cur[k].src[i];
+                    if (src == kPad) { more = false; break; }
+                    sum += cur[k].v[i] * solution(src, ring, xp);
+                }
+                if (more)
+                    for (int i = kEnts; i < Lc.w; ++i) {
+                        const int idx = Lc.base + i * Lc.m + t;
+                        const int src = psrc[idx];
+                        if (src == kPad) break;
+                        sum += pval[idx] * solution(src, ring, xp);
+                    }
+                const int p = Lc.pos + t;
+                const VT x = (cur[k].b - sum) / cur[k].d;
+                ring[p % kRing] = x;
+                xp[p] = x;
+            }
+        }
+        // rows beyond the register slots (levels wider than the slots cover)
+        for (int t = threadIdx.x + kRowsPerThread * kSweepThreads; t < Lc.m; t += kSweepThreads) {
+            VT sum = VT(0);
+            for (int i = 0; i < Lc.w; ++i) {
+                const int idx = Lc.base + i * Lc.m + t;
+                const int src = psrc[idx];
+                if (src == kPad) break;
+                sum += pval[idx] * solution(src, ring, xp);
+            }
+            const int p = Lc.pos + t;
+            const VT x = (bp[p] - sum) / pD[p];
+            ring[p % kRing] = x;
+            xp[p] = x;
+        }
+        __syncthreads();
+        Lc = Ln;
+        Ln = Lnn;
+#pragma unroll
+        for (int k = 0; k < kRowsPerThread; ++k) cur[k] = nxt[k];
+    }
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(kSweepThreads, 1)
+    sweep_kernel(const Level *__restrict__ lv, int s0, int s1, const int *__restrict__ psrc,
+                 const VT *__restrict__ pval, const VT *__restrict__ pD, const VT *__restrict__ bp, VT *xp) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    sweep_run<VT>(lv, s0, s1, psrc, pval, pD, bp, xp, reinterpret_cast<VT *>(smem));
+}
+
+// Work queue of matrices; each CTA sweeps its matrix's steps.
+template <typename VT>
+__global__ void __launch_bounds__(kSweepThreads, 1)
+    sweep_batch_kernel(const Level *__restrict__ lv, const int *__restrict__ mat_steps,
+                       const int *__restrict__ queue_order, int n_mats, int *queue, const int *__restrict__ psrc,
+                       const VT *__restrict__ pval, const VT *__restrict__ pD, const VT *__restrict__ bp, VT *xp) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int m_sh;
+    while (true) {
+        if (threadIdx.x == 0) m_sh = atomicAdd(queue, 1);
+        __syncthreads();
+        const int q = m_sh;
+        __syncthreads();  // m_sh is rewritten on the next turn
+        if (q >= n_mats) return;
+        const int m = queue_order[q];
+        sweep_run<VT>(lv, mat_steps[m], mat_steps[m + 1], psrc, pval, pD, bp, xp, reinterpret_cast<VT *>(smem));
+    }
+}
+
+template <typename VT> void set_smem_attr() {
+    static bool done[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || done[dev]) return;
+    SMAX_CUDA(cudaFuncSetAttribute(sweep_kernel<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(kRing * sizeof(VT))));
+    SMAX_CUDA(cudaFuncSetAttribute(sweep_batch_kernel<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(kRing * sizeof(VT))));
+    done[dev] = true;
+}
+
+}  // namespace
+
+bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *val, const void *D, int vbytes,
+                      int64_t n, const int *order, const std::vector<int> &src_begin, const std::vector<int> &count,
+                      const std::vector<int> &seg_begin, cudaStream_t st) {
+    const int L = (int)count.size();
+    if ((int)src_begin.size() != L || (int)seg_begin.size() != L) fail(SMAX_ERR_STATE, "inconsistent sweep steps");
+    pk = LevelPack();
+    pk.n = n;
+    pk.vbytes = vbytes;
+    // the sweep kernels' shared-memory opt-in, set here and not inside a capture
+    if (vbytes == 8) set_smem_attr<double>();
+    else set_smem_attr<float>();
+    std::vector<int> pos_begin(L + 1, 0);
+    for (int s = 0; s < L; ++s) pos_begin[s + 1] = pos_begin[s] + count[s];
+    if (pos_begin[L] != n) fail(SMAX_ERR_STATE, "sweep steps do not cover all rows");
+    const size_t nb = sizeof(int) * (n > 0 ? n : 1);
+    pk.prow.alloc(nb);
+    pk.pD.alloc((size_t)vbytes * (n > 0 ? n : 1));
+    pk.bp.alloc((size_t)vbytes * (n > 0 ? n : 1));
+    pk.xp.alloc((size_t)vbytes * (n > 0 ? n : 1));
+    if (n == 0 || L == 0) {
+        pk.lv.alloc(sizeof(Level));
+        pk.psrc.alloc(sizeof(int));
+        pk.pval.alloc(vbytes);
+        return true;
+    }
+    DevBuf d_pos(sizeof(int) * (L + 1)), d_src(sizeof(int) * L), plev(nb), pos_of_row(nb), len(nb), wmax(sizeof(int) * L);
+    SMAX_CUDA(cudaMemcpyAsync(d_pos.p, pos_begin.data(), sizeof(int) * (L + 1), cudaMemcpyHostToDevice, st));
+    SMAX_CUDA(cudaMemcpyAsync(d_src.p, src_begin.data(), sizeof(int) * L, cudaMemcpyHostToDevice, st));
+    positions_kernel<<<grid_for(n), 256, 0, st>>>(d_pos.as<int>(), L, d_src.as<int>(), order, n, pk.prow.as<int>(),
+                                                  plev.as<int>(), pos_of_row.as<int>());
+    off_len_kernel<<<grid_for(n), 256, 0, st>>>(rp, pk.prow.as<int>(), n, len.as<int>());
+    SMAX_CUDA(cudaGetLastError());
+    size_t tb = 0;
+    SMAX_CUDA(cub::DeviceSegmentedReduce::Max(nullptr, tb, len.as<int>(), wmax.as<int>(), L, d_pos.as<int>(),
+                                              d_pos.as<int>() + 1, st));
+    DevBuf tmp(tb);
+    SMAX_CUDA(cub::DeviceSegmentedReduce::Max(tmp.p, tb, len.as<int>(), wmax.as<int>(), L, d_pos.as<int>(),
+                                              d_pos.as<int>() + 1, st));
+    std::vector<int> w(L);
+    SMAX_CUDA(cudaMemcpyAsync(w.data(), wmax.p, sizeof(int) * L, cudaMemcpyDeviceToHost, st));
+    int h_rp_end = 0;
+    SMAX_CUDA(cudaMemcpyAsync(&h_rp_end, rp + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SMAX_CUDA(cudaStreamSynchronize(st));
+    {
+        long long padded = 0;
+        for (int s = 0; s < L; ++s) padded += (long long)count[s] * (count[s] > 0 ? std::max(w[s], 0) : 0);
+        const long long off = (long long)h_rp_end - n;  // off-diagonal entries
+        if (padded > 3 * off + (1ll << 20) || padded >= (1ll << 31)) {
+            pk = LevelPack();
+            return false;
+        }
+    }
+    pk.h_lv.resize(L);
+    long long base = 0;
+    std::vector<int> seg_pos(L);
+    for (int s = 0; s < L; ++s) {
+        const int ws = count[s] > 0 ? std::max(w[s], 0) : 0;
+        pk.h_lv[s] = Level{pos_begin[s], count[s], ws, (int)base};
+        base += (long long)count[s] * ws;
+        if (seg_begin[s] < 0 || seg_begin[s] > s) fail(SMAX_ERR_STATE, "bad run start");
+        seg_pos[s] = pos_begin[seg_begin[s]];
+    }
+    pk.ents = base;
+    pk.lv.alloc(sizeof(Level) * L);
+    SMAX_CUDA(cudaMemcpyAsync(pk.lv.p, pk.h_lv.data(), sizeof(Level) * L, cudaMemcpyHostToDevice, st));
+    DevBuf d_seg(sizeof(int) * L), flag(sizeof(int));
+    SMAX_CUDA(cudaMemcpyAsync(d_seg.p, seg_pos.data(), sizeof(int) * L, cudaMemcpyHostToDevice, st));
+    SMAX_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+    pk.psrc.alloc(sizeof(int) * (base > 0 ? base : 1));
+    pk.pval.alloc((size_t)vbytes * (base > 0 ? base : 1));
+    if (vbytes == 8)
+        fill_kernel<unsigned long long><<<grid_for(n), 256, 0, st>>>(
+            rp, ci, static_cast<const unsigned long long *>(val), static_cast<const unsigned long long *>(D), n,
+            pk.prow.as<int>(), plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(),
+            pk.psrc.as<int>(), pk.pval.as<unsigned long long>(), pk.pD.as<unsigned long long>(), flag.as<int>());
+    else
+        fill_kernel<unsigned><<<grid_for(n), 256, 0, st>>>(
+            rp, ci, static_cast<const unsigned *>(val), static_cast<const unsigned *>(D), n, pk.prow.as<int>(),
+            plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(), pk.psrc.as<int>(),
+            pk.pval.as<unsigned>(), pk.pD.as<unsigned>(), flag.as<int>());
+    SMAX_CUDA(cudaGetLastError());
+    int h_flag = 0;
+    SMAX_CUDA(cudaMemcpyAsync(&h_flag, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SMAX_CUDA(cudaStreamSynchronize(st));  // the temporaries die here
+    pk.needs_x_init = h_flag != 0;
+    return true;
+}
+
+template <typename VT>
+void pack_solve(const LevelPack &pk, const std::vector<PackStep> &steps, const VT *B, VT *X, cudaStream_t st) {
+    if (pk.n == 0) return;
+    set_smem_attr<VT>();
+    const int *prow = pk.prow.as<int>();
+    VT *bp = pk.bp.as<VT>(), *xp = pk.xp.as<VT>();
+    gather_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, B, bp, X, pk.needs_x_init ? xp : nullptr);
+    const int *psrc = pk.psrc.as<int>();
+    const VT *pval = pk.pval.as<VT>(), *pD = pk.pD.as<VT>();
+    for (const PackStep &s : steps) {
+        if (s.kind == 0) {
+            for (int l = s.first; l < s.first + s.count; ++l) {
+                const Level &L = pk.h_lv[l];
+                if (L.m > 0)
+                    wide_level_kernel<VT><<<ceil_div_u(L.m, 256), 256, 0, st>>>(L, psrc, pval, pD, bp, xp);
+            }
+        } else {
+            sweep_kernel<VT><<<1, kSweepThreads, kRing * sizeof(VT), st>>>(pk.lv.as<Level>(), s.first,
+                                                                           s.first + s.count, psrc, pval, pD, bp, xp);
+        }
+    }
+    scatter_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, xp, X);
+    SMAX_CUDA(cudaGetLastError());
+}
+
+template <typename VT>
+void pack_solve_batch(const LevelPack &pk, const int *mat_steps, const int *queue_order, int n_mats, int *queue,
+                      const VT *B, VT *X, cudaStream_t st) {
+    if (pk.n == 0 || n_mats == 0) return;
+    set_smem_attr<VT>();
+    const int *prow = pk.prow.as<int>();
+    VT *bp = pk.bp.as<VT>(), *xp = pk.xp.as<VT>();
+    gather_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, B, bp, X, pk.needs_x_init ? xp : nullptr);
+    const int grid = std::max(1, std::min(n_mats, sm_count()));  // one 1024-thread CTA per SM
+    SMAX_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), st));
+    sweep_batch_kernel<VT><<<grid, kSweepThreads, kRing * sizeof(VT), st>>>(
+        pk.lv.as<Level>(), mat_steps, queue_order, n_mats, queue, pk.psrc.as<int>(), pk.pval.as<VT>(),
+        pk.pD.as<VT>(), bp, xp);
+    scatter_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, xp, X);
+    SMAX_CUDA(cudaGetLastError());
+}
+
+template void pack_solve<double>(const LevelPack &, const std::vector<PackStep> &, const double *, double *,
+                                 cudaStream_t);
+template void pack_solve<float>(const LevelPack &, const std::vector<PackStep> &, const float *, float *,
+                                cudaStream_t);
+template void pack_solve_batch<double>(const LevelPack &, const int *, const int *, int, int *, const double *,
+                                       double *, cudaStream_t);
+template void pack_solve_batch<float>(const LevelPack &, const int *, const int *, int, int *, const float *, float *,
+                                      cudaStream_t);
+
+}  // namespace smax

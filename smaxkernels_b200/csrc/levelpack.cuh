@@ -1,0 +1,70 @@
+// levelpack.cuh -- level-ordered packed triangular matrices and the sweep
+// kernels over them (levelpack.cu).
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace smax {
+
+// Rows in sweep order ("positions"), each level stored as a dense
+// column-major block of its rows' off-diagonal entries (ELL per level): the
+// i-th entry of the t-th row of level s sits at ent_base[s] + i*m[s] + t, so a
+// warp reads its rows' i-th entries with one coalesced load.  Each entry's
+// source is encoded for the single-CTA sweep:
+//   src <  0, != kPad : the solution is in the shared-memory ring slot -src-1
+//                       (written by the same sweep at most kRing positions ago
+//                       and not overwritten by the current level)
+//   src >= 0          : the solution's position in the position-ordered x
+//   src == kPad       : padding (the row has fewer entries than the level width)
+struct LevelPack {
+    static constexpr int kPad = -0x7fffffff - 1;
+    static constexpr int kRing = 8192;  // shared-memory ring of recent solutions (positions)
+
+    struct Level {
+        int pos, m, w;      // first position, rows, width (max off-diagonals)
+        int base;           // first entry (packs are limited to 2^31 entries)
+    };
+    int64_t n = 0, ents = 0;
+    int vbytes = 8;
+    std::vector<Level> h_lv;
+    DevBuf lv;      // Level[n_levels]
+    DevBuf prow;    // int[n]: row of each position
+    DevBuf psrc;    // int[ents]
+    DevBuf pval;    // VT[ents]
+    DevBuf pD;      // VT[n]
+    DevBuf bp, xp;  // VT[n]: right-hand side and solution in position order
+    bool needs_x_init = false;  // some entry reads a solution not computed before it
+    int n_levels() const { return (int)h_lv.size(); }
+};
+
+// Builds the pack of a triangular CRS matrix (diagonal last in each row, D its
+// diagonal) for a sweep whose step s solves the rows order[src_begin[s] ..
+// src_begin[s] + count[s]) (order == nullptr: the identity).  seg_begin[s] is
+// the first sweep step of the single-CTA run step s belongs to (s itself for
+// a level solved by its own grid launch): only solutions produced inside the
+// same run may come from the ring.
+// Returns false (building nothing) when the per-level padding would make the
+// pack more than about three times the off-diagonal entries.
+bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *val, const void *D, int vbytes,
+                      int64_t n, const int *order, const std::vector<int> &src_begin, const std::vector<int> &count,
+                      const std::vector<int> &seg_begin, cudaStream_t st);
+
+// Solves with the pack: gathers B into position order, runs each step --
+// wide levels as one grid launch each, runs of narrow levels as one
+// single-CTA sweep -- and scatters the solution to X.  steps: (first sweep
+// step, number of steps, kind 0 wide / 1 run).
+struct PackStep {
+    int first, count, kind;
+};
+template <typename VT>
+void pack_solve(const LevelPack &pk, const std::vector<PackStep> &steps, const VT *B, VT *X, cudaStream_t st);
+
+// One single-CTA sweep per matrix of a batch, matrices taken from a device
+// work queue: mat_steps[m] .. mat_steps[m+1] are matrix m's sweep steps.
+template <typename VT>
+void pack_solve_batch(const LevelPack &pk, const int *mat_steps, const int *queue_order, int n_mats, int *queue,
+                      const VT *B, VT *X, cudaStream_t st);
+
+}  // namespace smax

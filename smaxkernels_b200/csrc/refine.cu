@@ -125,13 +125,13 @@ void sequence(smax_kernel_s *k, const double *B, double *X, bool initial, int st
     auto *stats = R.stats.as<unsigned long long>();
     if (initial) {
         cast_to_float<<<grid_of(n), 256, 0, st>>>(B, n, b32);
-        tri_solve_raw<float>(k->tri, rp, ci, v32, D32, b32, x32, 1, true, n, merge, st);
+        tri_solve_raw<float>(k->tri, rp, ci, v32, D32, b32, x32, 1, true, n, merge, k->vals_version, st);
         SMAX_CUDA(cudaMemsetAsync(stats, 0, 2 * sizeof(unsigned long long), st));
         update_x<<<grid_of(n), 256, 0, st>>>(x32, n, true, X, stats);
     }
     for (int s = 0; s < steps; ++s) {
         residual_kernel<<<grid_of(n), 256, 0, st>>>(rp, ci, k->dA.val.as<double>(), B, X, n, r32);
-        tri_solve_raw<float>(k->tri, rp, ci, v32, D32, r32, x32, 1, true, n, merge, st);
+        tri_solve_raw<float>(k->tri, rp, ci, v32, D32, r32, x32, 1, true, n, merge, k->vals_version, st);
         SMAX_CUDA(cudaMemsetAsync(stats, 0, 2 * sizeof(unsigned long long), st));
         update_x<<<grid_of(n), 256, 0, st>>>(x32, n, false, X, stats);
     }
@@ -147,6 +147,7 @@ void refine_solve(smax_kernel_s *k, const double *B, double *X) {
     ensure_copies(k);
     const int merge = tri_merge_rows(k);
     const int steps = k->refine_steps;
+    k->tri.ensure_pack(k->dA.rp(), k->dA.ci(), R.val32.p, R.D32.p, sizeof(float), merge, k->vals_version, k->stream);
     k->tri.prepare(1, merge, k->stream);
     if (k->refine_tol > 0) {
         // host-checked: stop at the first correction below the tolerance
@@ -172,7 +173,8 @@ void refine_solve(smax_kernel_s *k, const double *B, double *X) {
     cudaStream_t st = fenced ? R.aux.enter(k->stream) : k->stream;
     const void *key0 = B, *key1 = X;
     const bool stale = !R.graph || R.gkey[0] != key0 || R.gkey[1] != key1 || R.g_steps != steps ||
-                       R.g_merge != merge || R.g_serial != k->tri_plan_serial || R.g_aver != k->a_version;
+                       R.g_merge != merge || R.g_serial != k->tri_plan_serial || R.g_aver != k->a_version ||
+                       R.g_pack != k->tri.pack.psrc.p;
     if (stale) {
         R.release_graph();
         SMAX_CUDA(cudaStreamSynchronize(st));
@@ -198,6 +200,7 @@ void refine_solve(smax_kernel_s *k, const double *B, double *X) {
         R.g_merge = merge;
         R.g_serial = k->tri_plan_serial;
         R.g_aver = k->a_version;
+        R.g_pack = k->tri.pack.psrc.p;
     }
     SMAX_CUDA(cudaGraphLaunch(R.graph, st));
     if (fenced) R.aux.leave(k->stream);

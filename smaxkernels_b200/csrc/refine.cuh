@@ -16,6 +16,7 @@ struct RefineState {
     const void *gkey[2] = {nullptr, nullptr};
     int g_steps = -1, g_merge = -1;
     uint64_t g_serial = ~0ull, g_aver = ~0ull;  // level plan and A upload the graph was captured for
+    const void *g_pack = nullptr;                // level pack the graph reads
     int steps_done = 0;
     double last_rel = 0.0;          // max|d| / max|x| of the last correction
     void release_graph() {

@@ -200,6 +200,46 @@ void TriPlan::assign_reverse(const TriPlan &src, cudaStream_t st) {
 
 void TriPlan::finish(cudaStream_t) {
     graph_valid = false;
+    pack_ok = false;
+    pack_unfit = false;
+    pack = LevelPack();
+}
+
+bool TriPlan::ensure_pack(const int *rp, const int *ci, const void *val, const void *D, int vbytes, int merge_rows,
+                          uint64_t tag, cudaStream_t st) {
+    if (scheduled_k != 1 || scheduled_merge != merge_rows) schedule(1, merge_rows);
+    if (pack_ok && pack_key[0] == val && pack_key[1] == D && pack_tag == tag && pack_merge == merge_rows &&
+        pack_vbytes == vbytes)
+        return true;
+    if (pack_unfit) return false;  // a property of the pattern and the level sets
+    const int L = n_levels();
+    std::vector<int> src_begin(L), count(L), seg_begin(L);
+    pack_steps.clear();
+    for (const Step &s : steps) {
+        for (int i = 0; i < s.sweep_count; ++i) {
+            const int sw = s.sweep_first + i;
+            const int lv = descending ? L - 1 - sw : sw;
+            src_begin[sw] = lvl_ptr[lv];
+            count[sw] = lvl_ptr[lv + 1] - lvl_ptr[lv];
+            seg_begin[sw] = s.kind == 1 ? s.sweep_first : sw;
+        }
+        pack_steps.push_back(PackStep{s.sweep_first, s.sweep_count, s.kind});
+    }
+    release_graph();
+    pack_ok = false;
+    const bool ok = build_level_pack(pack, rp, ci, val, D, vbytes, n_rows, has_order ? order.as<int>() : nullptr,
+                                     src_begin, count, seg_begin, st);
+    if (!ok) {
+        pack_unfit = true;
+        return false;
+    }
+    pack_ok = true;
+    pack_key[0] = val;
+    pack_key[1] = D;
+    pack_tag = tag;
+    pack_merge = merge_rows;
+    pack_vbytes = vbytes;
+    return true;
 }
 
 void TriPlan::prepare(int64_t k, int merge_rows, cudaStream_t st) {
@@ -226,6 +266,7 @@ void TriPlan::schedule(int64_t k, int merge_rows) {
             Step s;
             s.kind = 1;
             s.seg_first = (int)seg_ranges.size();
+            s.sweep_first = l;
             while (l < L) {
                 const int lv2 = level_at(l);
                 const int64_t m2 = lvl_ptr[lv2 + 1] - lvl_ptr[lv2];
@@ -234,12 +275,15 @@ void TriPlan::schedule(int64_t k, int merge_rows) {
                 ++l;
             }
             s.seg_count = (int)seg_ranges.size() - s.seg_first;
+            s.sweep_count = s.seg_count;
             steps.push_back(s);
         } else {
             Step s;
             s.kind = 0;
             s.row0 = lvl_ptr[lv];
             s.m = (int)m;
+            s.sweep_first = l;
+            s.sweep_count = 1;
             steps.push_back(s);
             ++l;
         }
@@ -253,14 +297,20 @@ void TriPlan::schedule(int64_t k, int merge_rows) {
 
 template <typename VT>
 void tri_solve(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int64_t k, bool row_major, int64_t ld,
-               int merge_rows, cudaStream_t st) {
-    tri_solve_raw<VT>(p, a.rp(), a.ci(), a.val.as<VT>(), D, B, X, k, row_major, ld, merge_rows, st);
+               int merge_rows, uint64_t tag, cudaStream_t st) {
+    if (k == 1 && p.n_rows > 0) p.ensure_pack(a.rp(), a.ci(), a.val.p, D, sizeof(VT), merge_rows, tag, st);
+    tri_solve_raw<VT>(p, a.rp(), a.ci(), a.val.as<VT>(), D, B, X, k, row_major, ld, merge_rows, tag, st);
 }
 
 template <typename VT>
 void tri_solve_raw(TriPlan &p, const int *rp, const int *ci, const VT *val, const VT *D, const VT *B, VT *X,
-                   int64_t k, bool row_major, int64_t ld, int merge_rows, cudaStream_t st) {
+                   int64_t k, bool row_major, int64_t ld, int merge_rows, uint64_t tag, cudaStream_t st) {
     if (p.n_rows == 0) return;
+    if (k == 1 && p.pack_ok && p.pack_key[0] == val && p.pack_key[1] == D && p.pack_tag == tag &&
+        p.pack_merge == merge_rows && p.pack_vbytes == (int)sizeof(VT)) {
+        pack_solve<VT>(p.pack, p.pack_steps, B, X, st);
+        return;
+    }
     if (p.scheduled_k != k || p.scheduled_merge != merge_rows) p.schedule(k, merge_rows);
     if (!p.ranges_uploaded && !p.seg_ranges.empty()) {
         SMAX_CUDA(cudaMemcpyAsync(p.d_ranges.p, p.seg_ranges.data(), sizeof(int2) * p.seg_ranges.size(),
@@ -285,8 +335,10 @@ void tri_solve_raw(TriPlan &p, const int *rp, const int *ci, const VT *val, cons
 
 template <typename VT>
 void tri_solve_graph(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int64_t k, bool row_major,
-                     int64_t ld, int merge_rows, cudaStream_t caller) {
+                     int64_t ld, int merge_rows, uint64_t tag, cudaStream_t caller) {
     if (p.n_rows == 0) return;
+    // the pack is built outside the capture (it synchronises); a rebuild drops the graph
+    if (k == 1) p.ensure_pack(a.rp(), a.ci(), a.val.p, D, sizeof(VT), merge_rows, tag, caller);
     // graphs are captured (and replayed) on a capturable stream
     const bool fenced = !is_capturable(caller);
     cudaStream_t st = fenced ? p.aux.enter(caller) : caller;
@@ -302,9 +354,9 @@ void tri_solve_graph(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *
         }
     } leave{p, fenced, caller};
     if (p.scheduled_k != k || p.scheduled_merge != merge_rows) p.schedule(k, merge_rows);
-    const void *key[3] = {B, X, D};
+    const void *key[4] = {B, X, D, a.val.p};
     if (!p.graph_valid || p.graph_key[0] != key[0] || p.graph_key[1] != key[1] || p.graph_key[2] != key[2] ||
-        p.graph_row_major != row_major || p.graph_ld != ld) {
+        p.graph_key[3] != key[3] || p.graph_row_major != row_major || p.graph_ld != ld) {
         if (!p.ranges_uploaded && !p.seg_ranges.empty()) {
             SMAX_CUDA(cudaMemcpyAsync(p.d_ranges.p, p.seg_ranges.data(), sizeof(int2) * p.seg_ranges.size(),
                                       cudaMemcpyHostToDevice, st));
@@ -315,7 +367,7 @@ void tri_solve_graph(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *
         cudaGraph_t g = nullptr;
         SMAX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         try {
-            tri_solve<VT>(p, a, D, B, X, k, row_major, ld, merge_rows, st);
+            tri_solve_raw<VT>(p, a.rp(), a.ci(), a.val.as<VT>(), D, B, X, k, row_major, ld, merge_rows, tag, st);
         } catch (...) {
             cudaStreamEndCapture(st, &g);
             if (g) cudaGraphDestroy(g);
@@ -331,6 +383,7 @@ void tri_solve_graph(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *
         p.graph_key[0] = key[0];
         p.graph_key[1] = key[1];
         p.graph_key[2] = key[2];
+        p.graph_key[3] = key[3];
         p.graph_row_major = row_major;
         p.graph_ld = ld;
     }
@@ -346,16 +399,16 @@ void TriPlan::release_graph() {
 TriPlan::~TriPlan() { release_graph(); }
 
 template void tri_solve<double>(TriPlan &, const DevCRS &, const double *, const double *, double *, int64_t, bool,
-                                int64_t, int, cudaStream_t);
+                                int64_t, int, uint64_t, cudaStream_t);
 template void tri_solve<float>(TriPlan &, const DevCRS &, const float *, const float *, float *, int64_t, bool,
-                               int64_t, int, cudaStream_t);
+                               int64_t, int, uint64_t, cudaStream_t);
 template void tri_solve_raw<double>(TriPlan &, const int *, const int *, const double *, const double *,
-                                    const double *, double *, int64_t, bool, int64_t, int, cudaStream_t);
+                                    const double *, double *, int64_t, bool, int64_t, int, uint64_t, cudaStream_t);
 template void tri_solve_raw<float>(TriPlan &, const int *, const int *, const float *, const float *, const float *,
-                                   float *, int64_t, bool, int64_t, int, cudaStream_t);
+                                   float *, int64_t, bool, int64_t, int, uint64_t, cudaStream_t);
 template void tri_solve_graph<double>(TriPlan &, const DevCRS &, const double *, const double *, double *, int64_t,
-                                      bool, int64_t, int, cudaStream_t);
+                                      bool, int64_t, int, uint64_t, cudaStream_t);
 template void tri_solve_graph<float>(TriPlan &, const DevCRS &, const float *, const float *, float *, int64_t, bool,
-                                     int64_t, int, cudaStream_t);
+                                     int64_t, int, uint64_t, cudaStream_t);
 
 }  // namespace smax

@@ -3,6 +3,7 @@
 
 #include <vector>
 
+#include "levelpack.cuh"
 #include "levels.cuh"
 #include "spmv_formats.cuh"
 
@@ -29,6 +30,7 @@ struct TriPlan {
         int kind = 0;
         int row0 = 0, m = 0;
         int seg_first = 0, seg_count = 0;
+        int sweep_first = 0, sweep_count = 0;  // levels of the step, in sweep order
     };
     std::vector<Step> steps;
     std::vector<int2> seg_ranges;
@@ -40,10 +42,24 @@ struct TriPlan {
     // CUDA graph of the launch sequence (bound to the operand addresses)
     cudaGraphExec_t graph = nullptr;
     bool graph_valid = false;
-    const void *graph_key[3] = {nullptr, nullptr, nullptr};
+    const void *graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
     bool graph_row_major = false;
     int64_t graph_ld = 0;
     AuxStream aux;  // capture stream when the caller's stream cannot be captured
+
+    // level-ordered pack for one right-hand side (levelpack.cu), built for the
+    // value arrays, their version tag and the merge threshold below
+    LevelPack pack;
+    std::vector<PackStep> pack_steps;
+    bool pack_ok = false, pack_unfit = false;
+    const void *pack_key[2] = {nullptr, nullptr};
+    uint64_t pack_tag = ~0ull;
+    int pack_merge = -1, pack_vbytes = 0;
+    // (re)builds the pack when its key changed; false when the matrix does
+    // not pack compactly and the plain kernels must be used.  Synchronises:
+    // call outside stream capture.
+    bool ensure_pack(const int *rp, const int *ci, const void *val, const void *D, int vbytes, int merge_rows,
+                     uint64_t tag, cudaStream_t st);
 
     // dependency levels of the matrix itself (plain solve)
     void build_own(const DevCRS &a, bool upper, cudaStream_t st);
@@ -64,17 +80,21 @@ struct TriPlan {
 // X = A^{-1} B for k right-hand sides (row-major: element (r, v) at r*k+v;
 // column-major: at r + v*ld).  merge_rows: levels with at most this many
 // (row, vector) pairs are merged into single-CTA runs (0 disables merging).
+// `tag` identifies the current values of (val, D): a caller that changes the
+// values in place passes a new tag so the level-ordered pack is rebuilt.
+// With k == 1 the solve runs on the pack (levelpack.cu); tri_solve_raw does
+// not build it (it may run inside a stream capture): call ensure_pack first.
 template <typename VT>
 void tri_solve(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int64_t k, bool row_major, int64_t ld,
-               int merge_rows, cudaStream_t st);
+               int merge_rows, uint64_t tag, cudaStream_t st);
 // tri_solve on raw arrays (rp/ci of the matrix the plan was built for, with
 // any values of type VT, e.g. a float copy of double values).
 template <typename VT>
 void tri_solve_raw(TriPlan &p, const int *rp, const int *ci, const VT *val, const VT *D, const VT *B, VT *X,
-                   int64_t k, bool row_major, int64_t ld, int merge_rows, cudaStream_t st);
+                   int64_t k, bool row_major, int64_t ld, int merge_rows, uint64_t tag, cudaStream_t st);
 // The same launch sequence, captured once into a CUDA graph and replayed.
 template <typename VT>
 void tri_solve_graph(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int64_t k, bool row_major,
-                     int64_t ld, int merge_rows, cudaStream_t st);
+                     int64_t ld, int merge_rows, uint64_t tag, cudaStream_t st);
 
 }  // namespace smax

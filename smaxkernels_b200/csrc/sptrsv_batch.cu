@@ -6,6 +6,10 @@
 //    next matrix from a device work queue (an atomic counter over the matrices
 //    in longest-first order) and sweeps that matrix's levels, with
 //    __syncthreads() as the level barrier; when done it takes the next one.
+//    The sweep runs on the level-ordered pack of the batch (levelpack.cu:
+//    per-level ELL blocks, a shared-memory ring of recent solutions, the next
+//    level prefetched into registers); matrices that would pack too sparsely
+//    use the plain kernel below.
 //    There is no spin-wait anywhere: the queue is a fetch-add and the level
 //    barrier is the CTA barrier.  The launch (queue reset + kernel) is
 //    captured once into a CUDA graph and replayed.
@@ -229,11 +233,26 @@ void TriBatch::build(int vbytes_, const std::vector<RegCRS> &mats, cudaStream_t 
     h_mat_lvl_off = moff;
     row_off = roff;
     SMAX_CUDA(cudaStreamSynchronize(st));
+    // sweep steps = every matrix's levels in order; each matrix is one run
+    const int L = total_levels;
+    std::vector<int> src_begin(L), count(L), seg_begin(L);
+    for (int m = 0; m < n_mats; ++m)
+        for (int l = moff[m]; l < moff[m + 1]; ++l) {
+            src_begin[l] = lrows[l];
+            count[l] = lrows[l + 1] - lrows[l];
+            seg_begin[l] = moff[m];
+        }
+    pack_ok = build_level_pack(pack, A.rp(), A.ci(), A.val.p, D.p, vbytes, n_rows, order.as<int>(), src_begin, count,
+                               seg_begin, st);
 }
 
 template <typename VT>
 void TriBatch::solve_persistent(const VT *B, VT *X, cudaStream_t st) {
     if (n_mats == 0) return;
+    if (pack_ok) {
+        pack_solve_batch<VT>(pack, mat_lvl_off.as<int>(), queue_order.as<int>(), n_mats, queue.as<int>(), B, X, st);
+        return;
+    }
     int per_sm = 0;
     SMAX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_persistent<VT>, kBatchThreads, 0));
     const int grid = std::max(1, std::min(n_mats, per_sm * sm_count()));

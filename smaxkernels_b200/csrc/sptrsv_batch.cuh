@@ -21,6 +21,8 @@ struct TriBatch {
     std::vector<int> h_lvl_rows, h_mat_lvl_off;
     DevCRS A;
     DevBuf D, order, mat_lvl_off, lvl_rows, queue_order, queue;
+    LevelPack pack;          // level-ordered pack, one single-CTA run per matrix
+    bool pack_ok = false;    // false: the plain batch kernel (the pack would be too sparse)
     cudaGraphExec_t graph = nullptr;
     const void *graph_b = nullptr, *graph_x = nullptr;
     AuxStream aux;  // capture stream when the caller's stream cannot be captured
