@@ -495,14 +495,16 @@ def wl_sptrsv(b: Bench):
     from smaxkernels_b200 import KernelType
     from smaxkernels_b200 import matrices as M
     vt, vb = np.float64, 8
-    A = M.laplace2d_5pt(2048)
+    side = b.args.tri_side
+    A = M.laplace2d_5pt(side)
     rp, col, val = M.lower_triangle(*A)
     n, nnz = len(rp) - 1, len(col)
-    n_lv = 2 * 2048 - 1
+    n_lv = 2 * side - 1
     rhs = M.uniform_vector(n, 3)
     names = {1: "per_level", 2: "merged", 3: "graph", 4: "persistent"}
     results = {}
-    for mode in (1, 2, 3, 4):
+    modes = [int(m) for m in b.args.tri_modes.split(",")]
+    for mode in [m for m in (1, 2, 3, 4) if m in modes]:
         smax, k = b.kernel(KernelType.SPTRSV, vt, lambda k: k.set_solve_mode(mode))
         xd, bd = b.zeros(n, vt), b.dev(rhs)
         k.register_A(n, n, nnz, col.copy(), rp, val.copy())
@@ -518,12 +520,14 @@ def wl_sptrsv(b: Bench):
         if mode == 3:
             cpu = b.cpu(lambda: b.ref.time_sptrsv(rp, col, val, rhs, warm=1, reps=3)[0], nbytes,
                         "3 solves after 1 warm-up (reference naive_crs_sptrsv, serial)")
-        b.emit(f"sptrsv_f64_laplace2d_2048_natural_{names[mode]}", "SpTRSV GB/s", nbytes / t / 1e9, "GB/s", t,
+        b.emit(f"sptrsv_f64_laplace2d_{side}_natural_{names[mode]}", "SpTRSV GB/s", nbytes / t / 1e9, "GB/s", t,
                reps, "f64", {"n_rows": n, "nnz": nnz, "levels": n_lv, "scheme": names[mode]}, clk.summary(),
                b.hbm(nbytes, t, "level_kernel/segment_kernel"), cpu,
                launches=n_lv * reps if mode == 1 else (reps if mode == 4 else None),
                us_per_level=round(t * 1e6 / n_lv, 4))
         smax.close()
+    if b.args.tri_natural_only:
+        return
     # permuted flow: random symmetric permutation (seed 3), RS levels, level order
     Ar, Ac, Av, _ = M.random_symmetric_permutation(*A, seed=3)
     smax, k = b.kernel(KernelType.SPTRSV, vt)
@@ -555,7 +559,7 @@ def wl_sptrsv(b: Bench):
         if mode == 3:
             cpu = b.cpu(lambda: b.ref.time_sptrsv(lrp, lcol, lval, rhs, levels=lvl, warm=1, reps=5)[0], nbytes,
                         "5 solves after 1 warm-up (reference crs_sptrsv_lvl, OpenMP within levels)")
-        b.emit(f"sptrsv_f64_laplace2d_2048_permuted_{names[mode]}", "SpTRSV GB/s", nbytes / t / 1e9, "GB/s", t,
+        b.emit(f"sptrsv_f64_laplace2d_{side}_permuted_{names[mode]}", "SpTRSV GB/s", nbytes / t / 1e9, "GB/s", t,
                reps, "f64", {"n_rows": n, "nnz": len(lcol), "levels": nl, "scheme": names[mode],
                              "ordering": "random symmetric permutation (seed 3), RS level order"},
                clk.summary(), b.hbm(nbytes, t, "level_kernel/segment_kernel"), cpu,
@@ -576,7 +580,7 @@ def wl_sptrsv(b: Bench):
         t, reps = b.time(k.apply, budget_s=2.0, max_reps=50)
     cpu = b.cpu(lambda: b.ref.time_sptrsm(rp, col, val, B, kv, True, warm=0, reps=1), nbytes,
                 "1 solve (reference naive row-major SpTRSM, serial)")
-    b.emit("sptrsm_k32_f64_laplace2d_2048_natural_graph", "SpTRSM GB/s", nbytes / t / 1e9, "GB/s", t, reps,
+    b.emit(f"sptrsm_k32_f64_laplace2d_{side}_natural_graph", "SpTRSM GB/s", nbytes / t / 1e9, "GB/s", t, reps,
            "f64", {"n_rows": n, "nnz": nnz, "k": kv, "levels": n_lv, "layout": "row-major"}, clk.summary(),
            b.hbm(nbytes, t, "level_kernel/segment_kernel"), cpu, us_per_level=round(t * 1e6 / n_lv, 4))
     smax.close()
@@ -602,7 +606,8 @@ def wl_sptrsv_batch(b: Bench):
     nbytes = _tri_bytes(n, nnz, 8)
     times = {}
     names = {3: "persistent_graph", 2: "persistent", 1: "per_level"}
-    for mode in (3, 2, 1):
+    # the per-level baseline first, so every line carries the speed-up over it
+    for mode in (1, 3, 2):
         fn = lambda: tb.solve(bd, xd, mode, b.stream.cuda_stream)
         with b.clocks() as clk:
             t, reps = b.time(fn, budget_s=2.0, max_reps=200)
@@ -709,6 +714,9 @@ def main():
     ap.add_argument("--variant", type=int, default=0, help="CRS kernel: 0 auto, 1 warp-stream, 2 row-tile")
     ap.add_argument("--workload", default="crs_spmv", choices=("crs_spmv", "all") + EXTRA_WORKLOADS,
                     help="crs_spmv (the headline line) or another workload of the hot path (1 GPU)")
+    ap.add_argument("--tri-side", type=int, default=2048, help="sptrsv workload: grid side of the Laplacian")
+    ap.add_argument("--tri-modes", default="1,2,3,4", help="sptrsv workload: solve modes of the natural case")
+    ap.add_argument("--tri-natural-only", action="store_true", help="sptrsv workload: natural order only")
     args = ap.parse_args()
     globals()["N_ROWS"] = args.rows
     if args.impl == "reference":

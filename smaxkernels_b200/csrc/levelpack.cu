@@ -17,9 +17,9 @@
 //   at pack time (the ring slot of position q is q % kRing; it survives until
 //   position q + kRing is written, so it is safe while q >= level_end - kRing).
 // * While a level is computed, each thread already loads the next level's
-//   entries, right-hand sides and diagonals into registers, and the block
-//   prefetches the level after that into L2: the critical path per level is
-//   ring reads, a few FMAs, the division and the CTA barrier.
+//   entries, right-hand sides and diagonals into registers, and after the
+//   compute the block prefetches the level after that into L2: the critical
+//   path per level is ring reads, a few FMAs, the division and the CTA barrier.
 // * Right-hand sides are gathered into position order before the sweep and
 //   the solution scattered back after it (two coalesced passes over n).
 #include "levelpack.cuh"
@@ -74,12 +74,12 @@ __global__ void off_len_kernel(const int *__restrict__ rp, const int *__restrict
     }
 }
 
-template <typename W>
-__global__ void fill_kernel(const int *__restrict__ rp, const int *__restrict__ ci, const W *__restrict__ val,
-                            const W *__restrict__ D, int64_t n, const int *__restrict__ prow,
+template <typename VT>
+__global__ void fill_kernel(const int *__restrict__ rp, const int *__restrict__ ci, const VT *__restrict__ val,
+                            const VT *__restrict__ D, int64_t n, const int *__restrict__ prow,
                             const int *__restrict__ plev, const int *__restrict__ pos_of_row,
                             const Level *__restrict__ lv, const int *__restrict__ seg_pos, int *__restrict__ psrc,
-                            W *__restrict__ pval, W *__restrict__ pD, int *needs_init) {
+                            VT *__restrict__ pval, VT *__restrict__ pinv, int *needs_init) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
         const int s = plev[p];
@@ -94,14 +94,14 @@ __global__ void fill_kernel(const int *__restrict__ rp, const int *__restrict__ 
                 const int q = pos_of_row[ci[j0 + i]];
                 if (q >= L.pos) atomicExch(needs_init, 1);
                 const bool ring = q >= segb && q < L.pos && q >= le - kRing;
-                psrc[idx] = ring ? -(q % kRing) - 1 : q;
+                psrc[idx] = ring ? -(q & (kRing - 1)) - 1 : q;
                 pval[idx] = val[j0 + i];
             } else {
                 psrc[idx] = kPad;
-                pval[idx] = W(0);
+                pval[idx] = VT(0);
             }
         }
-        pD[p] = D[r];
+        pinv[p] = VT(1) / D[r];
     }
 }
 
@@ -126,7 +126,7 @@ __global__ void scatter_kernel(const int *__restrict__ prow, int64_t n, const VT
 // one wide level: thread per row
 template <typename VT>
 __global__ void wide_level_kernel(Level L, const int *__restrict__ psrc, const VT *__restrict__ pval,
-                                  const VT *__restrict__ pD, const VT *__restrict__ bp, VT *xp) {
+                                  const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= L.m) return;
     VT sum = VT(0);
@@ -137,36 +137,34 @@ __global__ void wide_level_kernel(Level L, const int *__restrict__ psrc, const V
         sum += pval[idx] * xp[src];
     }
     const int p = L.pos + t;
-    xp[p] = (bp[p] - sum) / pD[p];
+    xp[p] = (bp[p] - sum) * pinv[p];
 }
 
 template <typename VT> struct RowRegs {
     int src[kEnts];
     VT v[kEnts];
-    VT b, d;
+    VT b, inv;
 };
 
 __device__ __forceinline__ Level load_level(const Level *lv, int s) {
-    Level L;
-    L.pos = lv[s].pos;
-    L.m = lv[s].m;
-    L.w = lv[s].w;
-    L.base = lv[s].base;
-    return L;
+    static_assert(sizeof(Level) == sizeof(int4), "a level is one 16-byte load");
+    const int4 v = *reinterpret_cast<const int4 *>(lv + s);
+    return Level{v.x, v.y, v.z, v.w};
 }
 
-template <typename VT>
+template <typename VT, int T>
 __device__ __forceinline__ void load_rows(const Level &L, const int *__restrict__ psrc, const VT *__restrict__ pval,
-                                          const VT *__restrict__ pD, const VT *__restrict__ bp, RowRegs<VT> (&R)[kRowsPerThread]) {
+                                          const VT *__restrict__ pinv, const VT *__restrict__ bp,
+                                          RowRegs<VT> (&R)[kRowsPerThread]) {
 #pragma unroll
     for (int k = 0; k < kRowsPerThread; ++k) {
-        const int t = threadIdx.x + k * kSweepThreads;
+        const int t = threadIdx.x + k * T;
 #pragma unroll
         for (int i = 0; i < kEnts; ++i) R[k].src[i] = kPad;
         if (t < L.m) {
             const int p = L.pos + t;
             R[k].b = bp[p];
-            R[k].d = pD[p];
+            R[k].inv = pinv[p];
 #pragma unroll
             for (int i = 0; i < kEnts; ++i)
                 if (i < L.w) {
@@ -178,24 +176,20 @@ __device__ __forceinline__ void load_rows(const Level &L, const int *__restrict_
     }
 }
 
-// every thread prefetches a few 128-byte lines of level L's data into L2
-template <typename VT>
-__device__ __forceinline__ void prefetch_level_l2(const Level &L, const int *psrc, const VT *pval, const VT *pD,
+// thread t prefetches the t-th 128-byte line of each of level L's ranges into
+// L2 (a level's ranges are at most kRowsPerThread*T rows; wider levels are
+// prefetched in part)
+template <typename VT, int T>
+__device__ __forceinline__ void prefetch_level_l2(const Level &L, const int *psrc, const VT *pval, const VT *pinv,
                                                   const VT *bp) {
-    const int t = threadIdx.x;
+    const long long o = (long long)threadIdx.x * 128;
     const long long ne = (long long)L.m * L.w;
-    const char *r0 = reinterpret_cast<const char *>(psrc + L.base);
-    const char *r1 = reinterpret_cast<const char *>(pval + L.base);
-    const char *r2 = reinterpret_cast<const char *>(pD + L.pos);
-    const char *r3 = reinterpret_cast<const char *>(bp + L.pos);
-    const long long b0 = ne * 4, b1 = ne * (long long)sizeof(VT), b2 = (long long)L.m * sizeof(VT);
-    for (long long o = (long long)t * 128; o < b0; o += 128LL * kSweepThreads)
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(r0 + o));
-    for (long long o = (long long)t * 128; o < b1; o += 128LL * kSweepThreads)
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(r1 + o));
-    for (long long o = (long long)t * 128; o < b2; o += 128LL * kSweepThreads) {
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(r2 + o));
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(r3 + o));
+    if (o < ne * 4) asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(psrc + L.base) + o));
+    if (o < ne * (long long)sizeof(VT))
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(pval + L.base) + o));
+    if (o < (long long)L.m * (long long)sizeof(VT)) {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(pinv + L.pos) + o));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(bp + L.pos) + o));
     }
 }
 
@@ -204,58 +198,61 @@ __device__ __forceinline__ VT solution(int src, const VT *ring, const VT *xp) {
     return src < 0 ? ring[-src - 1] : xp[src];
 }
 
-// Sweeps steps [s0, s1) of the pack in one CTA.
-template <typename VT>
+// Sweeps steps [s0, s1) of the pack in one CTA of T threads.
+template <typename VT, int T>
 __device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const int *__restrict__ psrc,
-                          const VT *__restrict__ pval, const VT *__restrict__ pD, const VT *__restrict__ bp, VT *xp,
+                          const VT *__restrict__ pval, const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp,
                           VT *ring) {
     if (s0 >= s1) return;
     RowRegs<VT> cur[kRowsPerThread], nxt[kRowsPerThread];
     Level Lc = load_level(lv, s0);
     Level Ln = load_level(lv, s0 + 1 < s1 ? s0 + 1 : s0);
-    load_rows<VT>(Lc, psrc, pval, pD, bp, cur);
+    load_rows<VT, T>(Lc, psrc, pval, pinv, bp, cur);
+    const int warp0 = threadIdx.x & ~31;
     for (int s = s0; s < s1; ++s) {
         const Level Lnn = load_level(lv, s + 2 < s1 ? s + 2 : s);
-        if (s + 1 < s1) load_rows<VT>(Ln, psrc, pval, pD, bp, nxt);
-        if (s + 2 < s1) prefetch_level_l2<VT>(Lnn, psrc, pval, pD, bp);
+        if (s + 1 < s1 && warp0 < Ln.m) load_rows<VT, T>(Ln, psrc, pval, pinv, bp, nxt);
+        if (s + 2 < s1) prefetch_level_l2<VT, T>(Lnn, psrc, pval, pinv, bp);
+        if (warp0 < Lc.m) {
 #pragma unroll
-        for (int k = 0; k < kRowsPerThread; ++k) {
-            const int t = threadIdx.x + k * kSweepThreads;
-            if (t < Lc.m) {
-                VT sum = VT(0);
-                bool more = true;
+            for (int k = 0; k < kRowsPerThread; ++k) {
+                const int t = threadIdx.x + k * T;
+                if (t < Lc.m) {
+                    VT sum = VT(0);
+                    bool more = true;
 #pragma unroll
-                for (int i = 0; i < kEnts; ++i) {
-                    const int src = cur[k].src[i];
-                    if (src == kPad) { more = false; break; }
-                    sum += cur[k].v[i] * solution(src, ring, xp);
-                }
-                if (more)
-                    for (int i = kEnts; i < Lc.w; ++i) {
-                        const int idx = Lc.base + i * Lc.m + t;
-                        const int src = psrc[idx];
-                        if (src == kPad) break;
-                        sum += pval[idx] * solution(src, ring, xp);
+                    for (int i = 0; i < kEnts; ++i) {
+                        const int src = cur[k].src[i];
+                        if (src == kPad) { more = false; break; }
+                        sum += cur[k].v[i] * solution(src, ring, xp);
                     }
+                    if (more)
+                        for (int i = kEnts; i < Lc.w; ++i) {
+                            const int idx = Lc.base + i * Lc.m + t;
+                            const int src = psrc[idx];
+                            if (src == kPad) break;
+                            sum += pval[idx] * solution(src, ring, xp);
+                        }
+                    const int p = Lc.pos + t;
+                    const VT x = (cur[k].b - sum) * cur[k].inv;
+                    ring[p & (kRing - 1)] = x;
+                    xp[p] = x;
+                }
+            }
+            // rows beyond the register slots (levels wider than the slots cover)
+            for (int t = threadIdx.x + kRowsPerThread * T; t < Lc.m; t += T) {
+                VT sum = VT(0);
+                for (int i = 0; i < Lc.w; ++i) {
+                    const int idx = Lc.base + i * Lc.m + t;
+                    const int src = psrc[idx];
+                    if (src == kPad) break;
+                    sum += pval[idx] * solution(src, ring, xp);
+                }
                 const int p = Lc.pos + t;
-                const VT x = (cur[k].b - sum) / cur[k].d;
-                ring[p % kRing] = x;
+                const VT x = (bp[p] - sum) * pinv[p];
+                ring[p & (kRing - 1)] = x;
                 xp[p] = x;
             }
-        }
-        // rows beyond the register slots (levels wider than the slots cover)
-        for (int t = threadIdx.x + kRowsPerThread * kSweepThreads; t < Lc.m; t += kSweepThreads) {
-            VT sum = VT(0);
-            for (int i = 0; i < Lc.w; ++i) {
-                const int idx = Lc.base + i * Lc.m + t;
-                const int src = psrc[idx];
-                if (src == kPad) break;
-                sum += pval[idx] * solution(src, ring, xp);
-            }
-            const int p = Lc.pos + t;
-            const VT x = (bp[p] - sum) / pD[p];
-            ring[p % kRing] = x;
-            xp[p] = x;
         }
         __syncthreads();
         Lc = Ln;
@@ -265,20 +262,20 @@ __device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const in
     }
 }
 
-template <typename VT>
-__global__ void __launch_bounds__(kSweepThreads, 1)
+template <typename VT, int T>
+__global__ void __launch_bounds__(T, 1)
     sweep_kernel(const Level *__restrict__ lv, int s0, int s1, const int *__restrict__ psrc,
-                 const VT *__restrict__ pval, const VT *__restrict__ pD, const VT *__restrict__ bp, VT *xp) {
+                 const VT *__restrict__ pval, const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp) {
     extern __shared__ __align__(16) unsigned char smem[];
-    sweep_run<VT>(lv, s0, s1, psrc, pval, pD, bp, xp, reinterpret_cast<VT *>(smem));
+    sweep_run<VT, T>(lv, s0, s1, psrc, pval, pinv, bp, xp, reinterpret_cast<VT *>(smem));
 }
 
 // Work queue of matrices; each CTA sweeps its matrix's steps.
-template <typename VT>
-__global__ void __launch_bounds__(kSweepThreads, 1)
+template <typename VT, int T>
+__global__ void __launch_bounds__(T, 1)
     sweep_batch_kernel(const Level *__restrict__ lv, const int *__restrict__ mat_steps,
                        const int *__restrict__ queue_order, int n_mats, int *queue, const int *__restrict__ psrc,
-                       const VT *__restrict__ pval, const VT *__restrict__ pD, const VT *__restrict__ bp, VT *xp) {
+                       const VT *__restrict__ pval, const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int m_sh;
     while (true) {
@@ -288,8 +285,15 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
         __syncthreads();  // m_sh is rewritten on the next turn
         if (q >= n_mats) return;
         const int m = queue_order[q];
-        sweep_run<VT>(lv, mat_steps[m], mat_steps[m + 1], psrc, pval, pD, bp, xp, reinterpret_cast<VT *>(smem));
+        sweep_run<VT, T>(lv, mat_steps[m], mat_steps[m + 1], psrc, pval, pinv, bp, xp, reinterpret_cast<VT *>(smem));
     }
+}
+
+template <typename VT, int T> void set_smem_attr_t() {
+    SMAX_CUDA(cudaFuncSetAttribute(sweep_kernel<VT, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(kRing * sizeof(VT))));
+    SMAX_CUDA(cudaFuncSetAttribute(sweep_batch_kernel<VT, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(kRing * sizeof(VT))));
 }
 
 template <typename VT> void set_smem_attr() {
@@ -297,11 +301,29 @@ template <typename VT> void set_smem_attr() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64 || done[dev]) return;
-    SMAX_CUDA(cudaFuncSetAttribute(sweep_kernel<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(kRing * sizeof(VT))));
-    SMAX_CUDA(cudaFuncSetAttribute(sweep_batch_kernel<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(kRing * sizeof(VT))));
+    set_smem_attr_t<VT, 256>();
+    set_smem_attr_t<VT, 512>();
+    set_smem_attr_t<VT, 1024>();
     done[dev] = true;
+}
+
+// CTA size of a single-CTA run: enough threads for its widest level at
+// kRowsPerThread rows each, from 256 to 1024
+int run_threads(const LevelPack &pk, int s0, int s1) {
+    int w = 0;
+    for (int s = s0; s < s1; ++s) w = std::max(w, pk.h_lv[s].m);
+    const int need = (w + kRowsPerThread - 1) / kRowsPerThread;
+    return need <= 256 ? 256 : (need <= 512 ? 512 : 1024);
+}
+
+template <typename VT>
+void launch_sweep(int threads, const LevelPack &pk, int s0, int s1, const int *psrc, const VT *pval,
+                  const VT *pinv, const VT *bp, VT *xp, cudaStream_t st) {
+    const size_t sm = kRing * sizeof(VT);
+    const Level *lv = pk.lv.as<Level>();
+    if (threads == 256) sweep_kernel<VT, 256><<<1, 256, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
+    else if (threads == 512) sweep_kernel<VT, 512><<<1, 512, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
+    else sweep_kernel<VT, 1024><<<1, 1024, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
 }
 
 }  // namespace
@@ -322,7 +344,7 @@ bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *v
     if (pos_begin[L] != n) fail(SMAX_ERR_STATE, "sweep steps do not cover all rows");
     const size_t nb = sizeof(int) * (n > 0 ? n : 1);
     pk.prow.alloc(nb);
-    pk.pD.alloc((size_t)vbytes * (n > 0 ? n : 1));
+    pk.pinv.alloc((size_t)vbytes * (n > 0 ? n : 1));
     pk.bp.alloc((size_t)vbytes * (n > 0 ? n : 1));
     pk.xp.alloc((size_t)vbytes * (n > 0 ? n : 1));
     if (n == 0 || L == 0) {
@@ -377,15 +399,15 @@ bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *v
     pk.psrc.alloc(sizeof(int) * (base > 0 ? base : 1));
     pk.pval.alloc((size_t)vbytes * (base > 0 ? base : 1));
     if (vbytes == 8)
-        fill_kernel<unsigned long long><<<grid_for(n), 256, 0, st>>>(
-            rp, ci, static_cast<const unsigned long long *>(val), static_cast<const unsigned long long *>(D), n,
-            pk.prow.as<int>(), plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(),
-            pk.psrc.as<int>(), pk.pval.as<unsigned long long>(), pk.pD.as<unsigned long long>(), flag.as<int>());
-    else
-        fill_kernel<unsigned><<<grid_for(n), 256, 0, st>>>(
-            rp, ci, static_cast<const unsigned *>(val), static_cast<const unsigned *>(D), n, pk.prow.as<int>(),
+        fill_kernel<double><<<grid_for(n), 256, 0, st>>>(
+            rp, ci, static_cast<const double *>(val), static_cast<const double *>(D), n, pk.prow.as<int>(),
             plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(), pk.psrc.as<int>(),
-            pk.pval.as<unsigned>(), pk.pD.as<unsigned>(), flag.as<int>());
+            pk.pval.as<double>(), pk.pinv.as<double>(), flag.as<int>());
+    else
+        fill_kernel<float><<<grid_for(n), 256, 0, st>>>(
+            rp, ci, static_cast<const float *>(val), static_cast<const float *>(D), n, pk.prow.as<int>(),
+            plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(), pk.psrc.as<int>(),
+            pk.pval.as<float>(), pk.pinv.as<float>(), flag.as<int>());
     SMAX_CUDA(cudaGetLastError());
     int h_flag = 0;
     SMAX_CUDA(cudaMemcpyAsync(&h_flag, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -402,17 +424,17 @@ void pack_solve(const LevelPack &pk, const std::vector<PackStep> &steps, const V
     VT *bp = pk.bp.as<VT>(), *xp = pk.xp.as<VT>();
     gather_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, B, bp, X, pk.needs_x_init ? xp : nullptr);
     const int *psrc = pk.psrc.as<int>();
-    const VT *pval = pk.pval.as<VT>(), *pD = pk.pD.as<VT>();
+    const VT *pval = pk.pval.as<VT>(), *pinv = pk.pinv.as<VT>();
     for (const PackStep &s : steps) {
         if (s.kind == 0) {
             for (int l = s.first; l < s.first + s.count; ++l) {
                 const Level &L = pk.h_lv[l];
                 if (L.m > 0)
-                    wide_level_kernel<VT><<<ceil_div_u(L.m, 256), 256, 0, st>>>(L, psrc, pval, pD, bp, xp);
+                    wide_level_kernel<VT><<<ceil_div_u(L.m, 256), 256, 0, st>>>(L, psrc, pval, pinv, bp, xp);
             }
         } else {
-            sweep_kernel<VT><<<1, kSweepThreads, kRing * sizeof(VT), st>>>(pk.lv.as<Level>(), s.first,
-                                                                           s.first + s.count, psrc, pval, pD, bp, xp);
+            launch_sweep<VT>(run_threads(pk, s.first, s.first + s.count), pk, s.first, s.first + s.count, psrc, pval,
+                             pinv, bp, xp, st);
         }
     }
     scatter_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, xp, X);
@@ -427,11 +449,24 @@ void pack_solve_batch(const LevelPack &pk, const int *mat_steps, const int *queu
     const int *prow = pk.prow.as<int>();
     VT *bp = pk.bp.as<VT>(), *xp = pk.xp.as<VT>();
     gather_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, B, bp, X, pk.needs_x_init ? xp : nullptr);
-    const int grid = std::max(1, std::min(n_mats, sm_count()));  // one 1024-thread CTA per SM
+    const int threads = run_threads(pk, 0, pk.n_levels());
+    // one CTA per matrix at a time: as many CTAs as fit (the ring limits residency)
+    const int per_sm = threads <= 512 ? 2 : 1;
+    const int grid = std::max(1, std::min(n_mats, per_sm * sm_count()));
     SMAX_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), st));
-    sweep_batch_kernel<VT><<<grid, kSweepThreads, kRing * sizeof(VT), st>>>(
-        pk.lv.as<Level>(), mat_steps, queue_order, n_mats, queue, pk.psrc.as<int>(), pk.pval.as<VT>(),
-        pk.pD.as<VT>(), bp, xp);
+    const size_t sm = kRing * sizeof(VT);
+    const Level *lv = pk.lv.as<Level>();
+    const int *psrc = pk.psrc.as<int>();
+    const VT *pval = pk.pval.as<VT>(), *pinv = pk.pinv.as<VT>();
+    if (threads == 256)
+        sweep_batch_kernel<VT, 256><<<grid, 256, sm, st>>>(lv, mat_steps, queue_order, n_mats, queue, psrc, pval,
+                                                            pinv, bp, xp);
+    else if (threads == 512)
+        sweep_batch_kernel<VT, 512><<<grid, 512, sm, st>>>(lv, mat_steps, queue_order, n_mats, queue, psrc, pval,
+                                                            pinv, bp, xp);
+    else
+        sweep_batch_kernel<VT, 1024><<<grid, 1024, sm, st>>>(lv, mat_steps, queue_order, n_mats, queue, psrc, pval,
+                                                              pinv, bp, xp);
     scatter_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, xp, X);
     SMAX_CUDA(cudaGetLastError());
 }

@@ -20,7 +20,7 @@ namespace smax {
 //   src == kPad       : padding (the row has fewer entries than the level width)
 struct LevelPack {
     static constexpr int kPad = -0x7fffffff - 1;
-    static constexpr int kRing = 8192;  // shared-memory ring of recent solutions (positions)
+    static constexpr int kRing = 8192;  // shared-memory ring of recent solutions (positions; a power of 2)
 
     struct Level {
         int pos, m, w;      // first position, rows, width (max off-diagonals)
@@ -33,7 +33,7 @@ struct LevelPack {
     DevBuf prow;    // int[n]: row of each position
     DevBuf psrc;    // int[ents]
     DevBuf pval;    // VT[ents]
-    DevBuf pD;      // VT[n]
+    DevBuf pinv;    // VT[n]: 1 / diagonal
     DevBuf bp, xp;  // VT[n]: right-hand side and solution in position order
     bool needs_x_init = false;  // some entry reads a solution not computed before it
     int n_levels() const { return (int)h_lv.size(); }
