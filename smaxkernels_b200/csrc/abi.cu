@@ -342,8 +342,8 @@ void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
         k->timers["apply"] += k->apply_events.trim(512);
         auto ev = k->apply_events.acquire();
         SMAX_CUDA(cudaEventRecord(ev.first, k->stream));
-        if (k->vbytes == 8) spgemm<double>(k->dA, k->dBm, k->dCm, &k->spgemm_times, k->stream);
-        else spgemm<float>(k->dA, k->dBm, k->dCm, &k->spgemm_times, k->stream);
+        if (k->vbytes == 8) spgemm<double>(k->dA, k->dBm, k->dCm, k->spgemm_work, &k->spgemm_times, k->stream);
+        else spgemm<float>(k->dA, k->dBm, k->dCm, k->spgemm_work, &k->spgemm_times, k->stream);
         SMAX_CUDA(cudaEventRecord(ev.second, k->stream));
         const SpgemmTimes &t = k->spgemm_times;
         k->timers["Symbolic_Setup"] += t.setup;

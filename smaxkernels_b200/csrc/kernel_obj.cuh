@@ -117,6 +117,7 @@ struct smax_kernel_s {
     // SpGEMM
     smax::DevCRS dBm, dCm;
     smax::SpgemmTimes spgemm_times;
+    smax::SpgemmWork spgemm_work;
     bool spgemm_done = false;
 
     // triangular solves (SpTRSV / SpTRSM)

@@ -24,8 +24,6 @@
 #include "spgemm.cuh"
 
 #include <cub/device/device_scan.cuh>
-#include <cub/device/device_select.cuh>
-#include <thrust/iterator/counting_iterator.h>
 
 namespace smax {
 
@@ -54,14 +52,25 @@ __global__ void row_products(const int *__restrict__ arp, const int *__restrict_
     if (lane == 0) P[i] = s;
 }
 
-__global__ void bin_flags(const long long *__restrict__ P, int64_t n, unsigned char *__restrict__ fw,
-                          unsigned char *__restrict__ fc, unsigned char *__restrict__ fg) {
+// rows into three lists by product count (warp, CTA, global paths); the
+// order inside a list is irrelevant (rows are independent)
+__global__ void bin_rows(const long long *__restrict__ P, int64_t n, int *__restrict__ lists, int *counts) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const long long p = P[i];
-    fw[i] = p <= kWarpP;
-    fc[i] = p > kWarpP && p <= kCtaP;
-    fg[i] = p > kCtaP;
+    const bool valid = i < n;
+    const long long p = valid ? P[i] : 0;
+    const int bin = p <= kWarpP ? 0 : (p <= kCtaP ? 1 : 2);
+    const unsigned active = __ballot_sync(0xffffffffu, valid);
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        const unsigned mask = __ballot_sync(0xffffffffu, valid && bin == b) & active;
+        if (!mask) continue;
+        const int leader = __ffs(mask) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(counts + b, __popc(mask));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (valid && bin == b) lists[(int64_t)b * n + base + __popc(mask & ((1u << lane) - 1u))] = (int)i;
+    }
 }
 
 // The body shared by all three paths: a team of `tsize` threads (`t` its
@@ -219,111 +228,105 @@ __global__ void compact_kernel(const int *__restrict__ crp, const long long *__r
     }
 }
 
-template <typename T> void excl_scan(const T *in, T *out, int64_t n, cudaStream_t st) {
+template <typename T> void excl_scan(const T *in, T *out, int64_t n, DevBuf &tmp, cudaStream_t st) {
     SMAX_CUDA(cudaMemsetAsync(out, 0, sizeof(T), st));
     if (n == 0) return;
     size_t tb = 0;
     SMAX_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb, in, out + 1, (int)n, st));
-    DevBuf tmp(tb);
+    tmp.ensure(tb);
     SMAX_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tb, in, out + 1, (int)n, st));
-}
-
-int select_rows(const unsigned char *flags, int64_t n, DevBuf &out, DevBuf &cnt, cudaStream_t st) {
-    out.alloc(sizeof(int) * (n ? n : 1));
-    thrust::counting_iterator<int> it(0);
-    size_t tb = 0;
-    SMAX_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, it, flags, out.as<int>(), cnt.as<int>(), (int)n, st));
-    DevBuf tmp(tb);
-    SMAX_CUDA(cub::DeviceSelect::Flagged(tmp.p, tb, it, flags, out.as<int>(), cnt.as<int>(), (int)n, st));
-    int h = 0;
-    SMAX_CUDA(cudaMemcpyAsync(&h, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    SMAX_CUDA(cudaStreamSynchronize(st));
-    return h;
 }
 
 }  // namespace
 
 template <typename VT>
-void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmTimes *times, cudaStream_t st) {
+void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTimes *times, cudaStream_t st) {
     if (A.n_cols != B.n_rows) fail(SMAX_ERR_BAD_ARG, "A.n_cols must equal B.n_rows");
     const int64_t n = A.n_rows;
     C.n_rows = n;
     C.n_cols = B.n_cols;
-    C.row_ptr.alloc(sizeof(int) * (n + 1));
+    C.row_ptr.ensure(sizeof(int) * (n + 1));
     cudaEvent_t ev[5];
     for (auto &e : ev) SMAX_CUDA(cudaEventCreate(&e));
+    struct Destroy {
+        cudaEvent_t *ev;
+        ~Destroy() {
+            for (int i = 0; i < 5; ++i) cudaEventDestroy(ev[i]);
+        }
+    } destroy{ev};
     SMAX_CUDA(cudaEventRecord(ev[0], st));
     // --- setup: product counts, their offsets, row bins
-    DevBuf P(sizeof(long long) * (n ? n : 1)), Poff(sizeof(long long) * (n + 1));
+    w.P.ensure(sizeof(long long) * (n ? n : 1));
+    w.Poff.ensure(sizeof(long long) * (n + 1));
+    w.lists.ensure(sizeof(int) * 3 * (n ? n : 1));
+    w.counts.ensure(sizeof(int) * 4);
+    w.count.ensure(sizeof(int) * (n ? n : 1));
+    long long *P = w.P.as<long long>(), *Poff = w.Poff.as<long long>();
+    SMAX_CUDA(cudaMemsetAsync(w.counts.p, 0, sizeof(int) * 4, st));
     if (n > 0) {
-        row_products<<<ceil_div_u((uint64_t)n * 32, 256), 256, 0, st>>>(A.rp(), A.ci(), B.rp(), n, P.as<long long>());
+        row_products<<<ceil_div_u((uint64_t)n * 32, 256), 256, 0, st>>>(A.rp(), A.ci(), B.rp(), n, P);
+        bin_rows<<<ceil_div_u(n, 256), 256, 0, st>>>(P, n, w.lists.as<int>(), w.counts.as<int>());
         SMAX_CUDA(cudaGetLastError());
     }
-    excl_scan<long long>(P.as<long long>(), Poff.as<long long>(), n, st);
-    long long total_p = 0;
-    SMAX_CUDA(cudaMemcpyAsync(&total_p, Poff.as<long long>() + n, sizeof(long long), cudaMemcpyDeviceToHost, st));
-    DevBuf fw(n ? n : 1), fc(n ? n : 1), fg(n ? n : 1), cnt(sizeof(int)), rw, rc, rg;
-    if (n > 0) {
-        bin_flags<<<ceil_div_u(n, 256), 256, 0, st>>>(P.as<long long>(), n, fw.as<unsigned char>(),
-                                                       fc.as<unsigned char>(), fg.as<unsigned char>());
-        SMAX_CUDA(cudaGetLastError());
-    }
-    const int nw = n ? select_rows(fw.as<unsigned char>(), n, rw, cnt, st) : 0;
-    const int nc = n ? select_rows(fc.as<unsigned char>(), n, rc, cnt, st) : 0;
-    const int ng = n ? select_rows(fg.as<unsigned char>(), n, rg, cnt, st) : 0;
+    excl_scan<long long>(P, Poff, n, w.scan_tmp, st);
+    struct {
+        long long total_p;
+        int counts[4];
+    } h{};
+    SMAX_CUDA(cudaMemcpyAsync(&h.total_p, Poff + n, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    SMAX_CUDA(cudaMemcpyAsync(h.counts, w.counts.p, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
     SMAX_CUDA(cudaStreamSynchronize(st));
+    const long long total_p = h.total_p;
+    const int nw = h.counts[0], nc = h.counts[1], ng = h.counts[2];
+    const int *rw = w.lists.as<int>(), *rc = rw + n, *rg = rw + 2 * n;
     SMAX_CUDA(cudaEventRecord(ev[1], st));
     // --- fused Gustavson pass into product-offset (padded) buffers
-    DevBuf pcol(sizeof(int) * (total_p ? total_p : 1)), pval(sizeof(VT) * (total_p ? total_p : 1));
-    DevBuf count(sizeof(int) * (n ? n : 1));
+    w.pcol.ensure(sizeof(int) * (total_p ? total_p : 1));
+    w.pval.ensure(sizeof(VT) * (total_p ? total_p : 1));
+    int *pcol = w.pcol.as<int>(), *count = w.count.as<int>();
+    VT *pval = w.pval.as<VT>();
     if (nw > 0)
         gustavson_warp<VT><<<ceil_div_u(nw, kWarpsPerCta), kWarpsPerCta * 32, 0, st>>>(
-            rw.as<int>(), nw, P.as<long long>(), Poff.as<long long>(), A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(),
-            B.val.as<VT>(), pcol.as<int>(), pval.as<VT>(), count.as<int>());
+            rw, nw, P, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), pcol, pval, count);
     if (nc > 0) {
         const size_t sm = (size_t)kCtaTS * (sizeof(VT) + 2 * sizeof(int)) + sizeof(int) * kCtaP;
         SMAX_CUDA(cudaFuncSetAttribute(gustavson_cta<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        gustavson_cta<VT><<<nc, kCtaThreads, sm, st>>>(rc.as<int>(), nc, P.as<long long>(), Poff.as<long long>(),
-                                                       A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(),
-                                                       pcol.as<int>(), pval.as<VT>(), count.as<int>());
+        gustavson_cta<VT><<<nc, kCtaThreads, sm, st>>>(rc, nc, P, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(),
+                                                       B.ci(), B.val.as<VT>(), pcol, pval, count);
     }
-    DevBuf wts, wsz, woff, wkeys, wfirst, wvals, wpos;
     if (ng > 0) {
-        wts.alloc(sizeof(unsigned) * ng);
-        wsz.alloc(sizeof(long long) * ng);
-        woff.alloc(sizeof(long long) * (ng + 1));
-        ws_sizes<<<ceil_div_u(ng, 256), 256, 0, st>>>(rg.as<int>(), ng, P.as<long long>(), wts.as<unsigned>(),
-                                                      wsz.as<long long>());
+        w.wts.ensure(sizeof(unsigned) * ng);
+        w.wsz.ensure(sizeof(long long) * ng);
+        w.woff.ensure(sizeof(long long) * (ng + 1));
+        ws_sizes<<<ceil_div_u(ng, 256), 256, 0, st>>>(rg, ng, P, w.wts.as<unsigned>(), w.wsz.as<long long>());
         SMAX_CUDA(cudaGetLastError());
-        excl_scan<long long>(wsz.as<long long>(), woff.as<long long>(), ng, st);
+        excl_scan<long long>(w.wsz.as<long long>(), w.woff.as<long long>(), ng, w.scan_tmp, st);
         long long wtot = 0;
-        SMAX_CUDA(cudaMemcpyAsync(&wtot, woff.as<long long>() + ng, sizeof(long long), cudaMemcpyDeviceToHost, st));
+        SMAX_CUDA(cudaMemcpyAsync(&wtot, w.woff.as<long long>() + ng, sizeof(long long), cudaMemcpyDeviceToHost, st));
         SMAX_CUDA(cudaStreamSynchronize(st));
-        wkeys.alloc(sizeof(int) * wtot);
-        wfirst.alloc(sizeof(int) * wtot);
-        wvals.alloc(sizeof(VT) * wtot);
-        wpos.alloc(sizeof(int) * total_p);
-        gustavson_global<VT><<<ng, kCtaThreads, 0, st>>>(rg.as<int>(), woff.as<long long>(), wts.as<unsigned>(),
-                                                         P.as<long long>(), Poff.as<long long>(), A.rp(), A.ci(),
-                                                         A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(),
-                                                         pcol.as<int>(), pval.as<VT>(), count.as<int>(),
-                                                         wkeys.as<int>(), wfirst.as<int>(), wvals.as<VT>(),
-                                                         wpos.as<int>());
+        w.wkeys.ensure(sizeof(int) * wtot);
+        w.wfirst.ensure(sizeof(int) * wtot);
+        w.wvals.ensure(sizeof(VT) * wtot);
+        w.wpos.ensure(sizeof(int) * total_p);
+        gustavson_global<VT><<<ng, kCtaThreads, 0, st>>>(rg, w.woff.as<long long>(), w.wts.as<unsigned>(), P, Poff,
+                                                         A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(),
+                                                         B.val.as<VT>(), pcol, pval, count, w.wkeys.as<int>(),
+                                                         w.wfirst.as<int>(), w.wvals.as<VT>(), w.wpos.as<int>());
     }
     SMAX_CUDA(cudaGetLastError());
     SMAX_CUDA(cudaEventRecord(ev[2], st));
     // --- C's row pointer and arrays
-    excl_scan<int>(count.as<int>(), C.row_ptr.as<int>(), n, st);
+    excl_scan<int>(count, C.row_ptr.as<int>(), n, w.scan_tmp, st);
     int nnz = 0;
     SMAX_CUDA(cudaMemcpyAsync(&nnz, C.row_ptr.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost, st));
     SMAX_CUDA(cudaStreamSynchronize(st));
     C.nnz = nnz;
-    C.col.alloc(sizeof(int) * (nnz ? nnz : 1));
-    C.val.alloc(sizeof(VT) * (nnz ? nnz : 1));
+    C.col.ensure(sizeof(int) * (nnz ? nnz : 1));
+    C.val.ensure(sizeof(VT) * (nnz ? nnz : 1));
     SMAX_CUDA(cudaEventRecord(ev[3], st));
     if (n > 0) {
-        compact_kernel<VT><<<ceil_div_u((uint64_t)n * 32, 256), 256, 0, st>>>(
-            C.rp(), Poff.as<long long>(), n, pcol.as<int>(), pval.as<VT>(), C.col.as<int>(), C.val.as<VT>());
+        compact_kernel<VT><<<ceil_div_u((uint64_t)n * 32, 256), 256, 0, st>>>(C.rp(), Poff, n, pcol, pval,
+                                                                              C.col.as<int>(), C.val.as<VT>());
         SMAX_CUDA(cudaGetLastError());
     }
     SMAX_CUDA(cudaEventRecord(ev[4], st));
@@ -340,10 +343,9 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmTimes *times, cud
         times->compress = d * 1e-3;
         times->products = total_p;
     }
-    for (auto &e : ev) cudaEventDestroy(e);
 }
 
-template void spgemm<double>(const DevCRS &, const DevCRS &, DevCRS &, SpgemmTimes *, cudaStream_t);
-template void spgemm<float>(const DevCRS &, const DevCRS &, DevCRS &, SpgemmTimes *, cudaStream_t);
+template void spgemm<double>(const DevCRS &, const DevCRS &, DevCRS &, SpgemmWork &, SpgemmTimes *, cudaStream_t);
+template void spgemm<float>(const DevCRS &, const DevCRS &, DevCRS &, SpgemmWork &, SpgemmTimes *, cudaStream_t);
 
 }  // namespace smax

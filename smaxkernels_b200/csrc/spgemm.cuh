@@ -10,8 +10,17 @@ struct SpgemmTimes {
     long long products = 0;                                // sum over rows of the product counts
 };
 
+// Device workspace of the multiply, kept by the caller across applies: every
+// buffer only grows, so repeated products of same-shaped matrices allocate
+// nothing after the first.
+struct SpgemmWork {
+    DevBuf P, Poff, lists, counts, count, pcol, pval, scan_tmp;
+    DevBuf wts, wsz, woff, wkeys, wfirst, wvals, wpos;
+};
+
 // C's columns per row are in first-touch order and its values are summed in
-// the reference's product order.
-template <typename VT> void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmTimes *times, cudaStream_t st);
+// the reference's product order.  C's buffers grow as needed and are reused.
+template <typename VT>
+void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTimes *times, cudaStream_t st);
 
 }  // namespace smax
