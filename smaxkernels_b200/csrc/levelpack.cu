@@ -74,27 +74,12 @@ __global__ void off_len_kernel(const int *__restrict__ rp, const int *__restrict
     }
 }
 
-// An entry is one 16-byte (double) or 8-byte (float) record: the value and
-// the source bits; a row's right-hand side and 1/D likewise share a record.
-template <typename VT> struct Vec2;
-template <> struct Vec2<double> { using T = double2; };
-template <> struct Vec2<float> { using T = float2; };
-template <typename VT> using V2 = typename Vec2<VT>::T;
-
-__device__ __forceinline__ double src_bits(int s) { return __longlong_as_double((long long)(unsigned)s); }
-__device__ __forceinline__ int src_of(double y) { return (int)(unsigned)__double_as_longlong(y); }
-__device__ __forceinline__ float src_bits_f(int s) { return __int_as_float(s); }
-__device__ __forceinline__ int src_of(float y) { return __float_as_int(y); }
-template <typename VT> __device__ __forceinline__ VT make_src(int s);
-template <> __device__ __forceinline__ double make_src<double>(int s) { return src_bits(s); }
-template <> __device__ __forceinline__ float make_src<float>(int s) { return src_bits_f(s); }
-
 template <typename VT>
 __global__ void fill_kernel(const int *__restrict__ rp, const int *__restrict__ ci, const VT *__restrict__ val,
                             const VT *__restrict__ D, int64_t n, const int *__restrict__ prow,
                             const int *__restrict__ plev, const int *__restrict__ pos_of_row,
-                            const Level *__restrict__ lv, const int *__restrict__ seg_pos, V2<VT> *__restrict__ pent,
-                            V2<VT> *__restrict__ pbi, int *needs_init) {
+                            const Level *__restrict__ lv, const int *__restrict__ seg_pos, int *__restrict__ psrc,
+                            VT *__restrict__ pval, VT *__restrict__ pinv, int *needs_init) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
         const int s = plev[p];
@@ -105,34 +90,29 @@ __global__ void fill_kernel(const int *__restrict__ rp, const int *__restrict__ 
         const int segb = seg_pos[s], le = L.pos + L.m;
         for (int i = 0; i < L.w; ++i) {
             const long long idx = L.base + (long long)i * L.m + t;
-            V2<VT> e;
             if (i < len) {
                 const int q = pos_of_row[ci[j0 + i]];
                 if (q >= L.pos) atomicExch(needs_init, 1);
                 const bool ring = q >= segb && q < L.pos && q >= le - kRing;
-                e.x = val[j0 + i];
-                e.y = make_src<VT>(ring ? -(q & (kRing - 1)) - 1 : q);
+                psrc[idx] = ring ? -(q & (kRing - 1)) - 1 : q;
+                pval[idx] = val[j0 + i];
             } else {
-                e.x = VT(0);
-                e.y = make_src<VT>(kPad);
+                psrc[idx] = kPad;
+                pval[idx] = VT(0);
             }
-            pent[idx] = e;
         }
-        V2<VT> bi;
-        bi.x = VT(0);  // the right-hand side, gathered by every solve
-        bi.y = VT(1) / D[r];
-        pbi[p] = bi;
+        pinv[p] = VT(1) / D[r];
     }
 }
 
 // ---------------------------------------------------------------- solve ----
 template <typename VT>
-__global__ void gather_kernel(const int *__restrict__ prow, int64_t n, const VT *__restrict__ B,
-                              V2<VT> *__restrict__ pbi, const VT *__restrict__ X, VT *__restrict__ xp) {
+__global__ void gather_kernel(const int *__restrict__ prow, int64_t n, const VT *__restrict__ B, VT *__restrict__ bp,
+                              const VT *__restrict__ X, VT *__restrict__ xp) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
         const int r = prow[p];
-        pbi[p].x = B[r];
+        bp[p] = B[r];
         if (xp) xp[p] = X[r];
     }
 }
@@ -145,24 +125,25 @@ __global__ void scatter_kernel(const int *__restrict__ prow, int64_t n, const VT
 
 // one wide level: thread per row
 template <typename VT>
-__global__ void wide_level_kernel(Level L, const V2<VT> *__restrict__ pent, const V2<VT> *__restrict__ pbi, VT *xp) {
+__global__ void wide_level_kernel(Level L, const int *__restrict__ psrc, const VT *__restrict__ pval,
+                                  const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= L.m) return;
     VT sum = VT(0);
     for (int i = 0; i < L.w; ++i) {
-        const V2<VT> e = pent[L.base + (long long)i * L.m + t];
-        const int src = src_of(e.y);
+        const long long idx = L.base + (long long)i * L.m + t;
+        const int src = psrc[idx];
         if (src == kPad) break;
-        sum += e.x * xp[src];
+        sum += pval[idx] * xp[src];
     }
     const int p = L.pos + t;
-    const V2<VT> bi = pbi[p];
-    xp[p] = (bi.x - sum) * bi.y;
+    xp[p] = (bp[p] - sum) * pinv[p];
 }
 
 template <typename VT> struct RowRegs {
-    V2<VT> e[kEnts];
-    V2<VT> bi;
+    int src[kEnts];
+    VT v[kEnts];
+    VT b, inv;
 };
 
 __device__ __forceinline__ Level load_level(const Level *lv, int s) {
@@ -172,29 +153,44 @@ __device__ __forceinline__ Level load_level(const Level *lv, int s) {
 }
 
 template <typename VT, int T>
-__device__ __forceinline__ void load_rows(const Level &L, const V2<VT> *__restrict__ pent,
-                                          const V2<VT> *__restrict__ pbi, RowRegs<VT> (&R)[kRowsPerThread]) {
+__device__ __forceinline__ void load_rows(const Level &L, const int *__restrict__ psrc, const VT *__restrict__ pval,
+                                          const VT *__restrict__ pinv, const VT *__restrict__ bp,
+                                          RowRegs<VT> (&R)[kRowsPerThread]) {
 #pragma unroll
     for (int k = 0; k < kRowsPerThread; ++k) {
         const int t = threadIdx.x + k * T;
+#pragma unroll
+        for (int i = 0; i < kEnts; ++i) R[k].src[i] = kPad;
         if (t < L.m) {
-            R[k].bi = pbi[L.pos + t];
+            const int p = L.pos + t;
+            R[k].b = bp[p];
+            R[k].inv = pinv[p];
 #pragma unroll
             for (int i = 0; i < kEnts; ++i)
-                if (i < L.w) R[k].e[i] = pent[L.base + i * L.m + t];
+                if (i < L.w) {
+                    const int idx = L.base + i * L.m + t;
+                    R[k].src[i] = psrc[idx];
+                    R[k].v[i] = pval[idx];
+                }
         }
     }
 }
 
-// thread t prefetches the t-th 128-byte line of level L's entries and of its
-// row records into L2 (the rest of a very wide level is left to demand loads)
+// thread t prefetches the t-th 128-byte line of each of level L's ranges into
+// L2 (a level's ranges are at most kRowsPerThread*T rows; wider levels are
+// prefetched in part)
 template <typename VT, int T>
-__device__ __forceinline__ void prefetch_level_l2(const Level &L, const V2<VT> *pent, const V2<VT> *pbi) {
+__device__ __forceinline__ void prefetch_level_l2(const Level &L, const int *psrc, const VT *pval, const VT *pinv,
+                                                  const VT *bp) {
     const long long o = (long long)threadIdx.x * 128;
-    if (o < (long long)L.m * L.w * (long long)sizeof(V2<VT>))
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(pent + L.base) + o));
-    if (o < (long long)L.m * (long long)sizeof(V2<VT>))
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(pbi + L.pos) + o));
+    const long long ne = (long long)L.m * L.w;
+    if (o < ne * 4) asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(psrc + L.base) + o));
+    if (o < ne * (long long)sizeof(VT))
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(pval + L.base) + o));
+    if (o < (long long)L.m * (long long)sizeof(VT)) {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(pinv + L.pos) + o));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(bp + L.pos) + o));
+    }
 }
 
 template <typename VT>
@@ -202,99 +198,84 @@ __device__ __forceinline__ VT solution(int src, const VT *ring, const VT *xp) {
     return src < 0 ? ring[-src - 1] : xp[src];
 }
 
-// Solves level Lc from the registers `cur` while loading level Ln into `nxt`
-// and prefetching level Lpf into L2; ends with the CTA barrier.
+// Sweeps steps [s0, s1) of the pack in one CTA of T threads.
 template <typename VT, int T>
-__device__ __forceinline__ void level_step(const Level &Lc, const Level &Ln, bool has_next, const Level &Lpf,
-                                           bool has_pf, const RowRegs<VT> (&cur)[kRowsPerThread],
-                                           RowRegs<VT> (&nxt)[kRowsPerThread], const V2<VT> *__restrict__ pent,
-                                           const V2<VT> *__restrict__ pbi, VT *xp, VT *ring) {
+__device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const int *__restrict__ psrc,
+                          const VT *__restrict__ pval, const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp,
+                          VT *ring) {
+    if (s0 >= s1) return;
+    RowRegs<VT> cur[kRowsPerThread], nxt[kRowsPerThread];
+    Level Lc = load_level(lv, s0);
+    Level Ln = load_level(lv, s0 + 1 < s1 ? s0 + 1 : s0);
+    load_rows<VT, T>(Lc, psrc, pval, pinv, bp, cur);
     const int warp0 = threadIdx.x & ~31;
-    if (has_next && warp0 < Ln.m) load_rows<VT, T>(Ln, pent, pbi, nxt);
-    if (has_pf) prefetch_level_l2<VT, T>(Lpf, pent, pbi);
-    if (warp0 < Lc.m) {
+    for (int s = s0; s < s1; ++s) {
+        const Level Lnn = load_level(lv, s + 2 < s1 ? s + 2 : s);
+        if (s + 1 < s1 && warp0 < Ln.m) load_rows<VT, T>(Ln, psrc, pval, pinv, bp, nxt);
+        if (s + 2 < s1) prefetch_level_l2<VT, T>(Lnn, psrc, pval, pinv, bp);
+        if (warp0 < Lc.m) {
 #pragma unroll
-        for (int k = 0; k < kRowsPerThread; ++k) {
-            const int t = threadIdx.x + k * T;
-            if (t < Lc.m) {
-                VT sum = VT(0);
-                bool more = Lc.w > 0;
+            for (int k = 0; k < kRowsPerThread; ++k) {
+                const int t = threadIdx.x + k * T;
+                if (t < Lc.m) {
+                    VT sum = VT(0);
+                    bool more = true;
 #pragma unroll
-                for (int i = 0; i < kEnts; ++i) {
-                    if (!more || i >= Lc.w) { more = false; break; }
-                    const int src = src_of(cur[k].e[i].y);
-                    if (src == kPad) { more = false; break; }
-                    sum += cur[k].e[i].x * solution(src, ring, xp);
-                }
-                if (more)
-                    for (int i = kEnts; i < Lc.w; ++i) {
-                        const V2<VT> e = pent[Lc.base + i * Lc.m + t];
-                        const int src = src_of(e.y);
-                        if (src == kPad) break;
-                        sum += e.x * solution(src, ring, xp);
+                    for (int i = 0; i < kEnts; ++i) {
+                        const int src = cur[k].src[i];
+                        if (src == kPad) { more = false; break; }
+                        sum += cur[k].v[i] * solution(src, ring, xp);
                     }
+                    if (more)
+                        for (int i = kEnts; i < Lc.w; ++i) {
+                            const int idx = Lc.base + i * Lc.m + t;
+                            const int src = psrc[idx];
+                            if (src == kPad) break;
+                            sum += pval[idx] * solution(src, ring, xp);
+                        }
+                    const int p = Lc.pos + t;
+                    const VT x = (cur[k].b - sum) * cur[k].inv;
+                    ring[p & (kRing - 1)] = x;
+                    xp[p] = x;
+                }
+            }
+            // rows beyond the register slots (levels wider than the slots cover)
+            for (int t = threadIdx.x + kRowsPerThread * T; t < Lc.m; t += T) {
+                VT sum = VT(0);
+                for (int i = 0; i < Lc.w; ++i) {
+                    const int idx = Lc.base + i * Lc.m + t;
+                    const int src = psrc[idx];
+                    if (src == kPad) break;
+                    sum += pval[idx] * solution(src, ring, xp);
+                }
                 const int p = Lc.pos + t;
-                const VT x = (cur[k].bi.x - sum) * cur[k].bi.y;
+                const VT x = (bp[p] - sum) * pinv[p];
                 ring[p & (kRing - 1)] = x;
                 xp[p] = x;
             }
         }
-        // rows beyond the register slots (levels wider than the slots cover)
-        for (int t = threadIdx.x + kRowsPerThread * T; t < Lc.m; t += T) {
-            VT sum = VT(0);
-            for (int i = 0; i < Lc.w; ++i) {
-                const V2<VT> e = pent[Lc.base + i * Lc.m + t];
-                const int src = src_of(e.y);
-                if (src == kPad) break;
-                sum += e.x * solution(src, ring, xp);
-            }
-            const int p = Lc.pos + t;
-            const V2<VT> bi = pbi[p];
-            const VT x = (bi.x - sum) * bi.y;
-            ring[p & (kRing - 1)] = x;
-            xp[p] = x;
-        }
-    }
-    __syncthreads();
-}
-
-// Sweeps steps [s0, s1) of the pack in one CTA of T threads; the loop is
-// unrolled by two so the register buffers alternate instead of being copied.
-template <typename VT, int T>
-__device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const V2<VT> *__restrict__ pent,
-                          const V2<VT> *__restrict__ pbi, VT *xp, VT *ring) {
-    if (s0 >= s1) return;
-    RowRegs<VT> A[kRowsPerThread], B[kRowsPerThread];
-    Level L0 = load_level(lv, s0);
-    Level L1 = load_level(lv, s0 + 1 < s1 ? s0 + 1 : s0);
-    load_rows<VT, T>(L0, pent, pbi, A);
-    int s = s0;
-    while (true) {
-        Level L2 = load_level(lv, s + 2 < s1 ? s + 2 : s);
-        level_step<VT, T>(L0, L1, s + 1 < s1, L2, s + 2 < s1, A, B, pent, pbi, xp, ring);
-        if (++s >= s1) break;
-        Level L3 = load_level(lv, s + 2 < s1 ? s + 2 : s);
-        level_step<VT, T>(L1, L2, s + 1 < s1, L3, s + 2 < s1, B, A, pent, pbi, xp, ring);
-        if (++s >= s1) break;
-        L0 = L2;
-        L1 = L3;
+        __syncthreads();
+        Lc = Ln;
+        Ln = Lnn;
+#pragma unroll
+        for (int k = 0; k < kRowsPerThread; ++k) cur[k] = nxt[k];
     }
 }
 
 template <typename VT, int T>
 __global__ void __launch_bounds__(T, 1)
-    sweep_kernel(const Level *__restrict__ lv, int s0, int s1, const V2<VT> *__restrict__ pent,
-                 const V2<VT> *__restrict__ pbi, VT *xp) {
+    sweep_kernel(const Level *__restrict__ lv, int s0, int s1, const int *__restrict__ psrc,
+                 const VT *__restrict__ pval, const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp) {
     extern __shared__ __align__(16) unsigned char smem[];
-    sweep_run<VT, T>(lv, s0, s1, pent, pbi, xp, reinterpret_cast<VT *>(smem));
+    sweep_run<VT, T>(lv, s0, s1, psrc, pval, pinv, bp, xp, reinterpret_cast<VT *>(smem));
 }
 
 // Work queue of matrices; each CTA sweeps its matrix's steps.
 template <typename VT, int T>
 __global__ void __launch_bounds__(T, 1)
     sweep_batch_kernel(const Level *__restrict__ lv, const int *__restrict__ mat_steps,
-                       const int *__restrict__ queue_order, int n_mats, int *queue, const V2<VT> *__restrict__ pent,
-                       const V2<VT> *__restrict__ pbi, VT *xp) {
+                       const int *__restrict__ queue_order, int n_mats, int *queue, const int *__restrict__ psrc,
+                       const VT *__restrict__ pval, const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int m_sh;
     while (true) {
@@ -304,7 +285,7 @@ __global__ void __launch_bounds__(T, 1)
         __syncthreads();  // m_sh is rewritten on the next turn
         if (q >= n_mats) return;
         const int m = queue_order[q];
-        sweep_run<VT, T>(lv, mat_steps[m], mat_steps[m + 1], pent, pbi, xp, reinterpret_cast<VT *>(smem));
+        sweep_run<VT, T>(lv, mat_steps[m], mat_steps[m + 1], psrc, pval, pinv, bp, xp, reinterpret_cast<VT *>(smem));
     }
 }
 
@@ -336,14 +317,13 @@ int run_threads(const LevelPack &pk, int s0, int s1) {
 }
 
 template <typename VT>
-void launch_sweep(int threads, const LevelPack &pk, int s0, int s1, cudaStream_t st) {
+void launch_sweep(int threads, const LevelPack &pk, int s0, int s1, const int *psrc, const VT *pval,
+                  const VT *pinv, const VT *bp, VT *xp, cudaStream_t st) {
     const size_t sm = kRing * sizeof(VT);
     const Level *lv = pk.lv.as<Level>();
-    const V2<VT> *pent = pk.pent.as<V2<VT>>(), *pbi = pk.pbi.as<V2<VT>>();
-    VT *xp = pk.xp.as<VT>();
-    if (threads == 256) sweep_kernel<VT, 256><<<1, 256, sm, st>>>(lv, s0, s1, pent, pbi, xp);
-    else if (threads == 512) sweep_kernel<VT, 512><<<1, 512, sm, st>>>(lv, s0, s1, pent, pbi, xp);
-    else sweep_kernel<VT, 1024><<<1, 1024, sm, st>>>(lv, s0, s1, pent, pbi, xp);
+    if (threads == 256) sweep_kernel<VT, 256><<<1, 256, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
+    else if (threads == 512) sweep_kernel<VT, 512><<<1, 512, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
+    else sweep_kernel<VT, 1024><<<1, 1024, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
 }
 
 }  // namespace
@@ -364,11 +344,13 @@ bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *v
     if (pos_begin[L] != n) fail(SMAX_ERR_STATE, "sweep steps do not cover all rows");
     const size_t nb = sizeof(int) * (n > 0 ? n : 1);
     pk.prow.alloc(nb);
-    pk.pbi.alloc((size_t)2 * vbytes * (n > 0 ? n : 1));
+    pk.pinv.alloc((size_t)vbytes * (n > 0 ? n : 1));
+    pk.bp.alloc((size_t)vbytes * (n > 0 ? n : 1));
     pk.xp.alloc((size_t)vbytes * (n > 0 ? n : 1));
     if (n == 0 || L == 0) {
         pk.lv.alloc(sizeof(Level));
-        pk.pent.alloc(2 * vbytes);
+        pk.psrc.alloc(sizeof(int));
+        pk.pval.alloc(vbytes);
         return true;
     }
     DevBuf d_pos(sizeof(int) * (L + 1)), d_src(sizeof(int) * L), plev(nb), pos_of_row(nb), len(nb), wmax(sizeof(int) * L);
@@ -414,17 +396,18 @@ bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *v
     DevBuf d_seg(sizeof(int) * L), flag(sizeof(int));
     SMAX_CUDA(cudaMemcpyAsync(d_seg.p, seg_pos.data(), sizeof(int) * L, cudaMemcpyHostToDevice, st));
     SMAX_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
-    pk.pent.alloc((size_t)2 * vbytes * (base > 0 ? base : 1));
+    pk.psrc.alloc(sizeof(int) * (base > 0 ? base : 1));
+    pk.pval.alloc((size_t)vbytes * (base > 0 ? base : 1));
     if (vbytes == 8)
         fill_kernel<double><<<grid_for(n), 256, 0, st>>>(
             rp, ci, static_cast<const double *>(val), static_cast<const double *>(D), n, pk.prow.as<int>(),
-            plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(), pk.pent.as<double2>(),
-            pk.pbi.as<double2>(), flag.as<int>());
+            plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(), pk.psrc.as<int>(),
+            pk.pval.as<double>(), pk.pinv.as<double>(), flag.as<int>());
     else
         fill_kernel<float><<<grid_for(n), 256, 0, st>>>(
             rp, ci, static_cast<const float *>(val), static_cast<const float *>(D), n, pk.prow.as<int>(),
-            plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(), pk.pent.as<float2>(),
-            pk.pbi.as<float2>(), flag.as<int>());
+            plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(), pk.psrc.as<int>(),
+            pk.pval.as<float>(), pk.pinv.as<float>(), flag.as<int>());
     SMAX_CUDA(cudaGetLastError());
     int h_flag = 0;
     SMAX_CUDA(cudaMemcpyAsync(&h_flag, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -438,18 +421,20 @@ void pack_solve(const LevelPack &pk, const std::vector<PackStep> &steps, const V
     if (pk.n == 0) return;
     set_smem_attr<VT>();
     const int *prow = pk.prow.as<int>();
-    V2<VT> *pbi = pk.pbi.as<V2<VT>>();
-    const V2<VT> *pent = pk.pent.as<V2<VT>>();
-    VT *xp = pk.xp.as<VT>();
-    gather_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, B, pbi, X, pk.needs_x_init ? xp : nullptr);
+    VT *bp = pk.bp.as<VT>(), *xp = pk.xp.as<VT>();
+    gather_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, B, bp, X, pk.needs_x_init ? xp : nullptr);
+    const int *psrc = pk.psrc.as<int>();
+    const VT *pval = pk.pval.as<VT>(), *pinv = pk.pinv.as<VT>();
     for (const PackStep &s : steps) {
         if (s.kind == 0) {
             for (int l = s.first; l < s.first + s.count; ++l) {
                 const Level &L = pk.h_lv[l];
-                if (L.m > 0) wide_level_kernel<VT><<<ceil_div_u(L.m, 256), 256, 0, st>>>(L, pent, pbi, xp);
+                if (L.m > 0)
+                    wide_level_kernel<VT><<<ceil_div_u(L.m, 256), 256, 0, st>>>(L, psrc, pval, pinv, bp, xp);
             }
         } else {
-            launch_sweep<VT>(run_threads(pk, s.first, s.first + s.count), pk, s.first, s.first + s.count, st);
+            launch_sweep<VT>(run_threads(pk, s.first, s.first + s.count), pk, s.first, s.first + s.count, psrc, pval,
+                             pinv, bp, xp, st);
         }
     }
     scatter_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, xp, X);
@@ -462,10 +447,8 @@ void pack_solve_batch(const LevelPack &pk, const int *mat_steps, const int *queu
     if (pk.n == 0 || n_mats == 0) return;
     set_smem_attr<VT>();
     const int *prow = pk.prow.as<int>();
-    V2<VT> *pbi = pk.pbi.as<V2<VT>>();
-    const V2<VT> *pent = pk.pent.as<V2<VT>>();
-    VT *xp = pk.xp.as<VT>();
-    gather_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, B, pbi, X, pk.needs_x_init ? xp : nullptr);
+    VT *bp = pk.bp.as<VT>(), *xp = pk.xp.as<VT>();
+    gather_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, B, bp, X, pk.needs_x_init ? xp : nullptr);
     const int threads = run_threads(pk, 0, pk.n_levels());
     // one CTA per matrix at a time: as many CTAs as fit (the ring limits residency)
     const int per_sm = threads <= 512 ? 2 : 1;
@@ -473,13 +456,17 @@ void pack_solve_batch(const LevelPack &pk, const int *mat_steps, const int *queu
     SMAX_CUDA(cudaMemsetAsync(queue, 0, sizeof(int), st));
     const size_t sm = kRing * sizeof(VT);
     const Level *lv = pk.lv.as<Level>();
+    const int *psrc = pk.psrc.as<int>();
+    const VT *pval = pk.pval.as<VT>(), *pinv = pk.pinv.as<VT>();
     if (threads == 256)
-        sweep_batch_kernel<VT, 256><<<grid, 256, sm, st>>>(lv, mat_steps, queue_order, n_mats, queue, pent, pbi, xp);
+        sweep_batch_kernel<VT, 256><<<grid, 256, sm, st>>>(lv, mat_steps, queue_order, n_mats, queue, psrc, pval,
+                                                            pinv, bp, xp);
     else if (threads == 512)
-        sweep_batch_kernel<VT, 512><<<grid, 512, sm, st>>>(lv, mat_steps, queue_order, n_mats, queue, pent, pbi, xp);
+        sweep_batch_kernel<VT, 512><<<grid, 512, sm, st>>>(lv, mat_steps, queue_order, n_mats, queue, psrc, pval,
+                                                            pinv, bp, xp);
     else
-        sweep_batch_kernel<VT, 1024><<<grid, 1024, sm, st>>>(lv, mat_steps, queue_order, n_mats, queue, pent, pbi,
-                                                              xp);
+        sweep_batch_kernel<VT, 1024><<<grid, 1024, sm, st>>>(lv, mat_steps, queue_order, n_mats, queue, psrc, pval,
+                                                              pinv, bp, xp);
     scatter_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, xp, X);
     SMAX_CUDA(cudaGetLastError());
 }

@@ -31,9 +31,10 @@ struct LevelPack {
     std::vector<Level> h_lv;
     DevBuf lv;      // Level[n_levels]
     DevBuf prow;    // int[n]: row of each position
-    DevBuf pent;    // (value, source bits) records, 2*VT each, ents of them
-    DevBuf pbi;     // (right-hand side, 1/diagonal) records, 2*VT each, n of them
-    DevBuf xp;      // VT[n]: the solution in position order
+    DevBuf psrc;    // int[ents]
+    DevBuf pval;    // VT[ents]
+    DevBuf pinv;    // VT[n]: 1 / diagonal
+    DevBuf bp, xp;  // VT[n]: right-hand side and solution in position order
     bool needs_x_init = false;  // some entry reads a solution not computed before it
     int n_levels() const { return (int)h_lv.size(); }
 };

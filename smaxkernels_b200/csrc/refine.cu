@@ -174,7 +174,7 @@ void refine_solve(smax_kernel_s *k, const double *B, double *X) {
     const void *key0 = B, *key1 = X;
     const bool stale = !R.graph || R.gkey[0] != key0 || R.gkey[1] != key1 || R.g_steps != steps ||
                        R.g_merge != merge || R.g_serial != k->tri_plan_serial || R.g_aver != k->a_version ||
-                       R.g_pack != k->tri.pack.pent.p;
+                       R.g_pack != k->tri.pack.psrc.p;
     if (stale) {
         R.release_graph();
         SMAX_CUDA(cudaStreamSynchronize(st));
@@ -200,7 +200,7 @@ void refine_solve(smax_kernel_s *k, const double *B, double *X) {
         R.g_merge = merge;
         R.g_serial = k->tri_plan_serial;
         R.g_aver = k->a_version;
-        R.g_pack = k->tri.pack.pent.p;
+        R.g_pack = k->tri.pack.psrc.p;
     }
     SMAX_CUDA(cudaGraphLaunch(R.graph, st));
     if (fenced) R.aux.leave(k->stream);
