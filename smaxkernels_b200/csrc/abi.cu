@@ -103,6 +103,7 @@ void spmv_upload(smax_kernel_s *k) {
             SMAX_CUDA(cudaMemcpyAsync(d.val.p, r.val, (size_t)k->vbytes * r.n_elements, cudaMemcpyHostToDevice, st));
         validate_scs(d, dstatus(k), st);
         read_status(k);
+        scs_plan(d, k->vbytes, st);
     } else if (k->f_bcrs) {
         const RegBCRS &r = k->A_bcrs;
         require(r.set, SMAX_ERR_STATE, "register_A (BCRS) before initialize");

@@ -213,6 +213,7 @@ void tune_format(const RegCRS &r, smax_format_choice &out) {
             DevSCS s;
             DevBuf perm;
             crs_to_scs(a, vbytes, C, sg, s, perm, st);
+            scs_plan(s, vbytes, st);
             if (s.n_rows_padded > n + 64) {
                 // one more padded chunk than y holds: grow y
                 y.alloc(sizeof(VT) * s.n_rows_padded);

@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32)
 
         VT p[U];
 #pragma unroll
-        for (int i = 0; i < U; ++i) p[i] = cur.v[i] * ld_keep(x + cur.c[i]);
+        for (int i = 0; i < U; ++i) p[i] = cur.v[i] * __ldcg(x + cur.c[i]);  // L2 only: x lines are not reused in L1
 
         const int nend = __popc(nib);
         int incl = nend;

@@ -18,7 +18,17 @@ struct DevCRS {
 struct DevSCS {
     int64_t C = 0, sigma = 0, n_rows = 0, n_rows_padded = 0, n_cols = 0, n_chunks = 0, n_elements = 0, nnz = 0;
     DevBuf chunk_ptr, chunk_len, col, val;
+    // warp tasks of at most kScsTaskCols chunk columns (scs_plan): a chunk
+    // longer than that is split, its tasks write partial sums to slots that a
+    // fix-up pass adds in task order
+    int64_t n_tasks = 0, n_multi = 0, n_slots = 0;
+    DevBuf task_chunk, task_j0, task_slot, multi_chunk, multi_first, multi_count, partial;
+    int plan_vbytes = 0;
 };
+
+constexpr int kScsTaskCols = 32;
+// Builds the task plan of a SELL-C-sigma matrix (after upload or conversion).
+void scs_plan(DevSCS &m, int vbytes, cudaStream_t st);
 
 // BCRS (src/common.hpp:90-111): n_rows/n_cols count blocks
 struct DevBCRS {

@@ -6,7 +6,10 @@
 // y is produced in the permuted order (y[perm[r]] is row r of the CRS product).
 //
 // SpMV (SPMV::CPU::naive_scs_spmv, src/kernels/spmv/spmv_cpu/spmv_cpu_scs_impl.hpp:9-49):
-//   * C a multiple of VEC = 16 / sizeof(VT) and C/VEC <= 32: one warp per chunk;
+//   * C a multiple of VEC = 16 / sizeof(VT) and C/VEC <= 32: warp tasks of at
+//     most kScsTaskCols chunk columns (a long chunk -- sigma sorting puts the
+//     longest rows together -- is split over several warps, whose partial
+//     sums a fix-up pass adds in task order, so no warp holds a long tail);
 //     each lane owns VEC adjacent rows and reads them with one 128-bit load per
 //     chunk column, so C/VEC lanes cover a chunk column and the warp covers
 //     32*VEC/C columns per instruction (chunk-column-major, fully coalesced);
@@ -20,6 +23,8 @@
 // by scan, perm[old] = new, and a scatter of col/val into the zero-filled
 // chunk-column-major arrays -- all on the GPU.
 #include "spmv_formats.cuh"
+
+#include <vector>
 
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_segmented_radix_sort.cuh>
@@ -84,6 +89,106 @@ __global__ void __launch_bounds__(256) scs_warp_kernel(const int *__restrict__ c
         else { out.x = acc[0]; out.y = acc[1]; out.z = acc[2]; out.w = acc[3]; }
         __stcs(reinterpret_cast<VV *>(y + c * C + sub * VEC), out);
     }
+}
+
+// One warp per task: chunk columns [j0, min(len, j0 + kScsTaskCols)) of one
+// chunk, unrolled four instructions deep so the gathers of several columns
+// are in flight together.
+template <typename VT, int LPC>
+__global__ void __launch_bounds__(256) scs_task_kernel(const int *__restrict__ chunk_ptr,
+                                                       const int *__restrict__ chunk_len,
+                                                       const int *__restrict__ task_chunk,
+                                                       const int *__restrict__ task_j0,
+                                                       const int *__restrict__ task_slot, int64_t n_tasks,
+                                                       const int *__restrict__ col, const VT *__restrict__ val,
+                                                       const VT *__restrict__ x, VT *__restrict__ y,
+                                                       VT *__restrict__ partial) {
+    constexpr int VEC = Vec<VT>::N;
+    constexpr int C = LPC * VEC;
+    constexpr int CPI = 32 / LPC;  // chunk columns per warp instruction
+    using VV = typename Vec<VT>::T;
+    const int lane = threadIdx.x & 31;
+    const int64_t t = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (t >= n_tasks) return;
+    const int c = task_chunk[t];
+    const int jt = task_j0[t];
+    const int slot = task_slot[t];
+    const int64_t cs = chunk_ptr[c];
+    const int jl = min(chunk_len[c], jt + kScsTaskCols);
+    const int sub = lane % LPC;
+    VT acc[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) acc[i] = VT(0);
+    int j = jt + lane / LPC;
+    auto step = [&](int jj) {
+        const int64_t idx = cs + (int64_t)jj * C + sub * VEC;
+        VT v[VEC];
+        vec_get<VT>(__ldcs(reinterpret_cast<const VV *>(val + idx)), v);
+        int cc[VEC];
+        if constexpr (VEC == 2) {
+            int2 q = __ldcs(reinterpret_cast<const int2 *>(col + idx));
+            cc[0] = q.x; cc[1] = q.y;
+        } else {
+            int4 q = __ldcs(reinterpret_cast<const int4 *>(col + idx));
+            cc[0] = q.x; cc[1] = q.y; cc[2] = q.z; cc[3] = q.w;
+        }
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) acc[i] += v[i] * __ldcg(x + cc[i]);
+    };
+    for (; j + 3 * CPI < jl; j += 4 * CPI) {
+        // four columns' loads first, then their products in column order
+        const int64_t i0 = cs + (int64_t)j * C + sub * VEC;
+        VT v[4][VEC];
+        int cc[4][VEC];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t idx = i0 + (int64_t)u * CPI * C;
+            vec_get<VT>(__ldcs(reinterpret_cast<const VV *>(val + idx)), v[u]);
+            if constexpr (VEC == 2) {
+                int2 q = __ldcs(reinterpret_cast<const int2 *>(col + idx));
+                cc[u][0] = q.x; cc[u][1] = q.y;
+            } else {
+                int4 q = __ldcs(reinterpret_cast<const int4 *>(col + idx));
+                cc[u][0] = q.x; cc[u][1] = q.y; cc[u][2] = q.z; cc[u][3] = q.w;
+            }
+        }
+        VT xv[4][VEC];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int i = 0; i < VEC; ++i) xv[u][i] = __ldcg(x + cc[u][i]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int i = 0; i < VEC; ++i) acc[i] += v[u][i] * xv[u][i];
+    }
+    for (; j < jl; j += CPI) step(j);
+#pragma unroll
+    for (int o = LPC; o < 32; o <<= 1)
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
+    if (lane < LPC) {
+        VV out;
+        if constexpr (VEC == 2) { out.x = acc[0]; out.y = acc[1]; }
+        else { out.x = acc[0]; out.y = acc[1]; out.z = acc[2]; out.w = acc[3]; }
+        VT *dst = slot < 0 ? y + (int64_t)c * C : partial + (int64_t)slot * C;
+        __stcs(reinterpret_cast<VV *>(dst + sub * VEC), out);
+    }
+}
+
+// y rows of a split chunk = its tasks' partial sums, added in task order
+template <typename VT>
+__global__ void scs_fixup_kernel(const int *__restrict__ multi_chunk, const int *__restrict__ multi_first,
+                                 const int *__restrict__ multi_count, int64_t n_multi, int C,
+                                 const VT *__restrict__ partial, VT *__restrict__ y) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_multi * C) return;
+    const int64_t m = g / C;
+    const int i = (int)(g % C);
+    const int f = multi_first[m], k = multi_count[m];
+    VT s = VT(0);
+    for (int p = 0; p < k; ++p) s += partial[(int64_t)(f + p) * C + i];
+    y[(int64_t)multi_chunk[m] * C + i] = s;
 }
 
 // generic: one thread per (padded) row
@@ -174,13 +279,71 @@ bool scs_vector_path(int64_t C, int vbytes) {
     return C % vec == 0 && C / vec >= 1 && C / vec <= 32 && ((C / vec) & (C / vec - 1)) == 0;
 }
 
+void scs_plan(DevSCS &m, int vbytes, cudaStream_t st) {
+    const int64_t nc = m.n_chunks;
+    std::vector<int> len(nc > 0 ? nc : 1);
+    if (nc) SMAX_CUDA(cudaMemcpyAsync(len.data(), m.chunk_len.p, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
+    SMAX_CUDA(cudaStreamSynchronize(st));
+    std::vector<int> tc, tj, ts, mc, mf, mk;
+    int slots = 0;
+    for (int64_t c = 0; c < nc; ++c) {
+        const int parts = len[c] > kScsTaskCols ? (len[c] + kScsTaskCols - 1) / kScsTaskCols : 1;
+        if (parts > 1) {
+            mc.push_back((int)c);
+            mf.push_back(slots);
+            mk.push_back(parts);
+        }
+        for (int p = 0; p < parts; ++p) {
+            tc.push_back((int)c);
+            tj.push_back(p * kScsTaskCols);
+            ts.push_back(parts > 1 ? slots + p : -1);
+        }
+        if (parts > 1) slots += parts;
+    }
+    auto up = [&](DevBuf &d, const std::vector<int> &h) {
+        d.alloc(sizeof(int) * (h.empty() ? 1 : h.size()));
+        if (!h.empty()) SMAX_CUDA(cudaMemcpyAsync(d.p, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, st));
+    };
+    up(m.task_chunk, tc);
+    up(m.task_j0, tj);
+    up(m.task_slot, ts);
+    up(m.multi_chunk, mc);
+    up(m.multi_first, mf);
+    up(m.multi_count, mk);
+    m.partial.alloc((size_t)vbytes * m.C * (slots > 0 ? slots : 1));
+    m.n_tasks = (int64_t)tc.size();
+    m.n_multi = (int64_t)mc.size();
+    m.n_slots = slots;
+    m.plan_vbytes = vbytes;
+    SMAX_CUDA(cudaStreamSynchronize(st));
+}
+
 template <typename VT>
 void scs_spmv(const DevSCS &m, const VT *x, VT *y, cudaStream_t st) {
     if (m.n_chunks == 0) return;
     const int vec = Vec<VT>::N;
     // y is written with 16-byte stores: an offset given to apply() may unalign it
     const bool y_aligned = (reinterpret_cast<uintptr_t>(y) & 15) == 0;
-    if (y_aligned && scs_vector_path(m.C, sizeof(VT))) {
+    if (y_aligned && scs_vector_path(m.C, sizeof(VT)) && m.plan_vbytes == (int)sizeof(VT) && m.n_tasks > 0) {
+        const unsigned grid = ceil_div_u(m.n_tasks, 8);
+        const int *cp = m.chunk_ptr.as<int>(), *cl = m.chunk_len.as<int>(), *ci = m.col.as<int>();
+        const int *tc = m.task_chunk.as<int>(), *tj = m.task_j0.as<int>(), *ts = m.task_slot.as<int>();
+        const VT *v = m.val.as<VT>();
+        VT *part = m.partial.as<VT>();
+        switch (m.C / vec) {
+        case 1: scs_task_kernel<VT, 1><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part); break;
+        case 2: scs_task_kernel<VT, 2><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part); break;
+        case 4: scs_task_kernel<VT, 4><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part); break;
+        case 8: scs_task_kernel<VT, 8><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part); break;
+        case 16: scs_task_kernel<VT, 16><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part); break;
+        case 32: scs_task_kernel<VT, 32><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part); break;
+        default: fail(SMAX_ERR_STATE, "unexpected SELL chunk width");
+        }
+        if (m.n_multi > 0)
+            scs_fixup_kernel<VT><<<ceil_div_u(m.n_multi * m.C, 256), 256, 0, st>>>(
+                m.multi_chunk.as<int>(), m.multi_first.as<int>(), m.multi_count.as<int>(), m.n_multi, (int)m.C, part,
+                y);
+    } else if (y_aligned && scs_vector_path(m.C, sizeof(VT))) {
         const unsigned grid = ceil_div_u(m.n_chunks, 8);
         const int *cp = m.chunk_ptr.as<int>(), *cl = m.chunk_len.as<int>(), *ci = m.col.as<int>();
         const VT *v = m.val.as<VT>();
