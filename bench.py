@@ -352,7 +352,9 @@ def wl_scs_spmv(b: Bench):
     from smaxkernels_b200 import KernelType
     from smaxkernels_b200 import matrices as M
     from smaxkernels_b200.matrices import crs_bytes
-    for vt in (np.float64, np.float32):
+    dts = (np.float64, np.float32) if b.args.extra_dtype == "both" else \
+        ((np.float64,) if b.args.extra_dtype == "f64" else (np.float32,))
+    for vt in dts:
         vb = np.dtype(vt).itemsize
         rp, col, val = M.lognormal_random(1 << 22, seed=1, dtype=vt)
         n, nnz = len(rp) - 1, len(col)
@@ -423,11 +425,14 @@ def wl_spmm(b: Bench):
     nnz = 55,742,968), k = 16 and 64 vectors, FP64 and FP32."""
     from smaxkernels_b200 import KernelType
     from smaxkernels_b200 import matrices as M
-    for vt in (np.float64, np.float32):
+    dts = (np.float64, np.float32) if b.args.extra_dtype == "both" else \
+        ((np.float64,) if b.args.extra_dtype == "f64" else (np.float32,))
+    ks = [int(v) for v in b.args.spmm_k.split(",")]
+    for vt in dts:
         vb = np.dtype(vt).itemsize
         rp, col, val = M.stencil27(128, dtype=vt)
         n, nnz = len(rp) - 1, len(col)
-        for kv in (16, 64):
+        for kv in ks:
             X = np.random.default_rng(2).uniform(-1, 1, n * kv).astype(vt)
             smax, k = b.kernel(KernelType.SPMM, vt, lambda k: k.set_vec_row_major(True))
             Xd, Yd = b.dev(X), b.zeros(n * kv, vt)
@@ -717,6 +722,9 @@ def main():
     ap.add_argument("--tri-side", type=int, default=2048, help="sptrsv workload: grid side of the Laplacian")
     ap.add_argument("--tri-modes", default="1,2,3,4", help="sptrsv workload: solve modes of the natural case")
     ap.add_argument("--tri-natural-only", action="store_true", help="sptrsv workload: natural order only")
+    ap.add_argument("--extra-dtype", default="both", choices=("both", "f64", "f32"),
+                    help="scs_spmv / spmm workloads: value types to run")
+    ap.add_argument("--spmm-k", default="16,64", help="spmm workload: vector counts")
     args = ap.parse_args()
     globals()["N_ROWS"] = args.rows
     if args.impl == "reference":
