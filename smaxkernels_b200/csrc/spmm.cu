@@ -39,53 +39,35 @@ __global__ void __launch_bounds__(256) spmm_row_major_kernel(const int *__restri
 #pragma unroll
         for (int i = 0; i < VEC; ++i) acc[m][i] = VT(0);
     const int s = row_ptr[row], e = row_ptr[row + 1];
-    // entries in batches of B: the B X-row loads of a batch are issued before
-    // any of them is used (memory-level parallelism), then accumulated in
-    // entry order
-    constexpr int B = G < 8 ? G : 8;
     for (int j0 = s; j0 < e; j0 += G) {
         const int jj = j0 + g;
         const int myc = jj < e ? ld_stream(col + jj) : 0;
         const VT myv = jj < e ? ld_stream(val + jj) : VT(0);
         const int cnt = min(G, e - j0);
+        // unrolled so the X-row loads of consecutive entries overlap; holding
+        // more rows in registers lowered occupancy and was measured slower
+#pragma unroll 4
+        for (int t = 0; t < cnt; ++t) {
+            const int c = __shfl_sync(gmask, myc, t, G);
+            const VT v = __shfl_sync(gmask, myv, t, G);
+            const VT *xr = X + (int64_t)c * k;
 #pragma unroll
-        for (int t0 = 0; t0 < G; t0 += B) {
-            if (t0 >= cnt) break;
-            VT vv[B];
-            VT xv[B][NV][VEC];
-#pragma unroll
-            for (int u = 0; u < B; ++u) {
-                const int t = t0 + u;
-                const int c = __shfl_sync(gmask, myc, t, G);
-                vv[u] = __shfl_sync(gmask, myv, t, G);
-                const VT *xr = X + (int64_t)c * k;
-#pragma unroll
-                for (int m = 0; m < NV; ++m) {
-                    const int off = (m * G + g) * VEC;
-                    if (t < cnt) {
-                        if constexpr (VEC == 2) {
-                            const double2 q = __ldg(reinterpret_cast<const double2 *>(xr + off));
-                            xv[u][m][0] = q.x;
-                            xv[u][m][1] = q.y;
-                        } else if constexpr (VEC == 4) {
-                            const float4 q = __ldg(reinterpret_cast<const float4 *>(xr + off));
-                            xv[u][m][0] = q.x;
-                            xv[u][m][1] = q.y;
-                            xv[u][m][2] = q.z;
-                            xv[u][m][3] = q.w;
-                        } else {
-                            xv[u][m][0] = __ldg(xr + off);
-                        }
-                    }
+            for (int m = 0; m < NV; ++m) {
+                const int off = (m * G + g) * VEC;
+                if constexpr (VEC == 2) {
+                    const double2 xv = __ldg(reinterpret_cast<const double2 *>(xr + off));
+                    acc[m][0] += v * xv.x;
+                    acc[m][1] += v * xv.y;
+                } else if constexpr (VEC == 4) {
+                    const float4 xv = __ldg(reinterpret_cast<const float4 *>(xr + off));
+                    acc[m][0] += v * xv.x;
+                    acc[m][1] += v * xv.y;
+                    acc[m][2] += v * xv.z;
+                    acc[m][3] += v * xv.w;
+                } else {
+                    acc[m][0] += v * __ldg(xr + off);
                 }
             }
-#pragma unroll
-            for (int u = 0; u < B; ++u)
-                if (t0 + u < cnt)
-#pragma unroll
-                    for (int m = 0; m < NV; ++m)
-#pragma unroll
-                        for (int i = 0; i < VEC; ++i) acc[m][i] += vv[u] * xv[u][m][i];
         }
     }
     VT *yr = Y + row * k;
