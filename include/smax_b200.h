@@ -184,6 +184,12 @@ smax_status smax_kernel_get_timer(smax_kernel k, const char *name, double *secon
 /* The kernel's CUDA stream (a cudaStream_t). */
 void *smax_kernel_stream(smax_kernel k);
 
+/* Kernel::swap_operands (src/kernels/spmv.hpp:197-200, spmm.hpp:102-105):
+ * B and C exchange roles (x <-> y), for iterations that feed an SpMV's output
+ * back as its input.  The device copies are exchanged too, so an
+ * apply-swap-apply loop reads the previous result without any copy. */
+smax_status smax_kernel_swap_operands(smax_kernel k);
+
 /* Runs the kernel's work on the caller's stream (a cudaStream_t, e.g. the
  * current stream of a framework) instead of its own; NULL restores its own.
  * The caller keeps ownership of the stream. */

@@ -47,6 +47,7 @@ SIGNATURES = {
     "smax_kernel_sync": (I32, [P]),
     "smax_kernel_get_timer": (I32, [P, C.c_char_p, C.POINTER(C.c_double)]),
     "smax_kernel_stream": (P, [P]),
+    "smax_kernel_swap_operands": (I32, [P]),
     "smax_kernel_set_stream": (I32, [P, P]),
     "smax_kernel_adjoint": (I32, [P, P, P, P, P]),
     "smax_kernel_update_A_values": (I32, [P, P]),

@@ -658,6 +658,16 @@ smax_status smax_kernel_get_timer(smax_kernel k, const char *name, double *secon
 
 void *smax_kernel_stream(smax_kernel k) { return k ? (void *)k->stream : nullptr; }
 
+smax_status smax_kernel_swap_operands(smax_kernel k) {
+    return guarded([&] {
+        smax_kernel_s *kk = K(k);
+        require(kk->ktype == SMAX_KERNEL_SPMV || kk->ktype == SMAX_KERNEL_SPMM, SMAX_ERR_UNSUPPORTED,
+                "swap_operands not supported for this kernel");
+        std::swap(kk->B, kk->C);
+        std::swap(kk->dB, kk->dC);
+    });
+}
+
 smax_status smax_kernel_set_stream(smax_kernel k, void *stream) {
     return guarded([&] {
         smax_kernel_s *kk = K(k);

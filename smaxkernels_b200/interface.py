@@ -243,6 +243,14 @@ class Kernel:
     def mark_A_dirty(self):
         return self._flag("a_dirty", 1)
 
+    def swap_operands(self):
+        """x <-> y (src/kernels/spmv.hpp:197-200): the registered B and C, and
+        their device copies, exchange roles."""
+        check(lib.smax_kernel_swap_operands(self._h))
+        kb, kc = self._keep.get("B"), self._keep.get("C")
+        self._keep["B"], self._keep["C"] = kc, kb
+        return 0
+
     def set_refine(self, steps: int, tol_exp: int = 0):
         """float64 SpTRSV: solve in FP32 and apply `steps` FP64-residual
         corrections; with tol_exp > 0 stop once max|dx| <= 10^-tol_exp max|x|."""
