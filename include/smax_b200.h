@@ -116,6 +116,11 @@ smax_status smax_ctx_create(smax_ctx *out);
 smax_status smax_ctx_destroy(smax_ctx ctx);
 int smax_ctx_get_n_levels(smax_ctx ctx);             /* Interface::get_n_levels */
 int smax_ctx_get_level_ptr_at(smax_ctx ctx, int idx); /* Interface::get_level_ptr_at */
+/* Stores a level pointer computed elsewhere (e.g. by the reference's own CPU
+ * Utils::generate_perm, which fills UtilitiesContainer::lvl_ptr,
+ * src/utils/permutations.hpp:485-584): n_levels + 1 non-decreasing entries
+ * starting at 0.  Level-scheduled solves read it as they read generate_perm's. */
+smax_status smax_ctx_set_levels(smax_ctx ctx, int n_levels, const int *lvl_ptr);
 
 /* ---------------------------------------------------------------- kernels */
 /* Interface::register_kernel(name, KernelType, PlatformType::CUDA, IntType,

@@ -377,6 +377,10 @@ class Interface {
 
     int get_n_levels() const { return smax_ctx_get_n_levels(ctx_); }
     int get_level_ptr_at(int idx) const { return smax_ctx_get_level_ptr_at(ctx_, idx); }
+    // a level pointer computed elsewhere (n_levels + 1 entries)
+    int set_levels(int n_levels, const int *lvl_ptr) {
+        return detail::check(smax_ctx_set_levels(ctx_, n_levels, lvl_ptr), "set_levels");
+    }
 
     // Utils::print_timers (src/utils.hpp:24): stopwatches of every kernel
     void print_timers() const {

@@ -31,6 +31,7 @@ SIGNATURES = {
     "smax_ctx_destroy": (I32, [P]),
     "smax_ctx_get_n_levels": (I32, [P]),
     "smax_ctx_get_level_ptr_at": (I32, [P, I32]),
+    "smax_ctx_set_levels": (I32, [P, I32, P]),
     "smax_kernel_create": (I32, [PP, P, I32, I32, I32]),
     "smax_kernel_destroy": (I32, [P]),
     "smax_kernel_set_flag": (I32, [P, I32, I32]),

@@ -447,6 +447,20 @@ smax_status smax_ctx_destroy(smax_ctx ctx) {
 
 int smax_ctx_get_n_levels(smax_ctx ctx) { return ctx ? ctx->n_levels : 0; }
 
+smax_status smax_ctx_set_levels(smax_ctx ctx, int n_levels, const int *lvl_ptr) {
+    return guarded([&] {
+        require(ctx != nullptr, SMAX_ERR_BAD_ARG, "null context");
+        require(n_levels >= 0 && (lvl_ptr != nullptr || n_levels == 0), SMAX_ERR_BAD_ARG, "bad level pointer");
+        std::vector<int> lp(lvl_ptr, lvl_ptr + n_levels + 1);
+        require(lp.empty() || lp[0] == 0, SMAX_ERR_BAD_ARG, "the level pointer must start at 0");
+        for (int i = 1; i <= n_levels; ++i)
+            require(lp[i] >= lp[i - 1], SMAX_ERR_BAD_ARG, "the level pointer must not decrease");
+        ctx->lvl_ptr = std::move(lp);
+        ctx->n_levels = n_levels;
+        ctx->levels_version++;
+    });
+}
+
 int smax_ctx_get_level_ptr_at(smax_ctx ctx, int idx) {
     if (!ctx || idx < 0 || idx >= (int)ctx->lvl_ptr.size()) return -1;
     return ctx->lvl_ptr[idx];

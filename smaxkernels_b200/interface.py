@@ -530,6 +530,11 @@ class Interface:
     def get_level_ptr_at(self, idx: int) -> int:
         return lib.smax_ctx_get_level_ptr_at(self._ctx, idx)
 
+    def set_levels(self, lvl_ptr):
+        """Stores a level pointer computed elsewhere (n_levels + 1 entries)."""
+        lp = np.ascontiguousarray(lvl_ptr, dtype=np.int32)
+        check(lib.smax_ctx_set_levels(self._ctx, len(lp) - 1, _ptr(lp)))
+
     def close(self):
         for k in self._kernels.values():
             k._destroy()

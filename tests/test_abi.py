@@ -78,3 +78,21 @@ def test_product_does_not_import_oracle():
     for f in glob.glob(os.path.join(REPO, "smaxkernels_b200", "**", "*.py"), recursive=True):
         src = open(f).read()
         assert "oracle" not in re.sub(r"#.*|\"\"\"[\s\S]*?\"\"\"", "", src), f
+
+
+def test_ctx_set_levels_validates_and_stores():
+    """A level pointer computed elsewhere (the reference's CPU generate_perm)
+    is stored in the context; malformed ones are rejected."""
+    from smaxkernels_b200 import _lib
+    ctx = ctypes.c_void_p()
+    assert _lib.lib.smax_ctx_create(ctypes.byref(ctx)) == 0
+    lp = (ctypes.c_int * 4)(0, 3, 3, 10)
+    assert _lib.lib.smax_ctx_set_levels(ctx, 3, lp) == 0
+    assert _lib.lib.smax_ctx_get_n_levels(ctx) == 3
+    assert [_lib.lib.smax_ctx_get_level_ptr_at(ctx, i) for i in range(4)] == [0, 3, 3, 10]
+    bad = (ctypes.c_int * 3)(0, 5, 4)
+    assert _lib.lib.smax_ctx_set_levels(ctx, 2, bad) == _lib.ERR_BAD_ARG
+    bad0 = (ctypes.c_int * 2)(1, 4)
+    assert _lib.lib.smax_ctx_set_levels(ctx, 1, bad0) == _lib.ERR_BAD_ARG
+    assert _lib.lib.smax_ctx_get_n_levels(ctx) == 3  # unchanged by the rejected calls
+    assert _lib.lib.smax_ctx_destroy(ctx) == 0

@@ -310,3 +310,29 @@ def test_sptrsm_random_vs_oracle(vt, k_, row_major, mode):
     X, _, _ = gpu_sptrsv(rp, col, val, B, sptrsm_k=k_, row_major=row_major, mode=mode)
     X_ref = O.sptrsm(rp, col, val, B, k_, row_major=row_major)
     assert normwise(X, X_ref) <= tol(vt)
+
+
+def test_sptrsv_level_scheduled_with_levels_from_the_oracle():
+    """Levels computed on the CPU (the reference's generate_perm restated by the
+    oracle) handed over with set_levels drive the level-scheduled solve."""
+    from smaxkernels_b200 import FloatType, IntType, KernelType, PlatformType
+    from smaxkernels_b200 import matrices as M
+    rp, col, val = M.laplace2d_5pt(90)
+    n = len(rp) - 1
+    perm, inv, lvl = O.generate_perm(rp, col, "RS")
+    prp, pcol, pval = O.apply_mat_perm(rp, col, val, perm, inv)
+    lrp, lcol, lval = M.lower_triangle(prp, pcol, pval)
+    smax = _iface()
+    smax.set_levels(lvl)
+    assert smax.get_n_levels() == len(lvl) - 1
+    smax.register_kernel("tri", KernelType.SPTRSV, PlatformType.CUDA, IntType.INT32, FloatType.FLOAT64)
+    k = smax.kernel("tri")
+    k.set_mat_perm(True)
+    b = np.random.default_rng(21).uniform(-1, 1, n)
+    x = np.zeros(n)
+    k.register_A(n, n, len(lcol), lcol.copy(), lrp, lval.copy())
+    k.register_B(n, x)
+    k.register_C(n, b)
+    k.run()
+    assert normwise(x, O.sptrsv(lrp, lcol, lval, b, levels=lvl)) <= 1e-12
+    smax.close()
