@@ -26,6 +26,7 @@
 
 #include <algorithm>
 
+#include <cooperative_groups.h>
 #include <cub/device/device_segmented_reduce.cuh>
 
 namespace smax {
@@ -35,9 +36,12 @@ namespace {
 using Level = LevelPack::Level;
 constexpr int kPad = LevelPack::kPad;
 constexpr int kRing = LevelPack::kRing;
-constexpr int kSweepThreads = 1024;
+constexpr int kRingShift = 13;     // kRing == 1 << kRingShift
 constexpr int kRowsPerThread = 2;  // rows of a level held in registers per thread
 constexpr int kEnts = 2;           // prefetched entries per row (the rest are loaded when used)
+constexpr int kClusterCTAs = 8;    // CTAs of a cluster run (portable cluster size)
+constexpr int kClusterThreads = 256;
+static_assert(kRing == (1 << kRingShift), "ring size");
 
 unsigned grid_for(int64_t work) {
     const int64_t cap = (int64_t)sm_count() * 8;
@@ -78,8 +82,9 @@ template <typename VT>
 __global__ void fill_kernel(const int *__restrict__ rp, const int *__restrict__ ci, const VT *__restrict__ val,
                             const VT *__restrict__ D, int64_t n, const int *__restrict__ prow,
                             const int *__restrict__ plev, const int *__restrict__ pos_of_row,
-                            const Level *__restrict__ lv, const int *__restrict__ seg_pos, int *__restrict__ psrc,
-                            VT *__restrict__ pval, VT *__restrict__ pinv, int *needs_init) {
+                            const Level *__restrict__ lv, const int *__restrict__ seg_pos,
+                            const int2 *__restrict__ geo, int *__restrict__ psrc, VT *__restrict__ pval,
+                            VT *__restrict__ pinv, int *needs_init) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
         const int s = plev[p];
@@ -88,13 +93,23 @@ __global__ void fill_kernel(const int *__restrict__ rp, const int *__restrict__ 
         const int r = prow[p];
         const int j0 = rp[r], len = rp[r + 1] - j0 - 1;
         const int segb = seg_pos[s], le = L.pos + L.m;
+        const int2 g2 = geo[s];  // the run's (CTAs, threads per CTA)
+        const int G = g2.x * g2.y;
         for (int i = 0; i < L.w; ++i) {
             const long long idx = L.base + (long long)i * L.m + t;
             if (i < len) {
                 const int q = pos_of_row[ci[j0 + i]];
                 if (q >= L.pos) atomicExch(needs_init, 1);
                 const bool ring = q >= segb && q < L.pos && q >= le - kRing;
-                psrc[idx] = ring ? -(q & (kRing - 1)) - 1 : q;
+                int code = q;
+                if (ring) {
+                    // the thread of the run that solves position q: its row
+                    // index in its level modulo the run's thread count
+                    const int tq = q - lv[plev[q]].pos;
+                    const int owner = (tq % G) / g2.y;
+                    code = -((owner << kRingShift) | (q & (kRing - 1))) - 1;
+                }
+                psrc[idx] = code;
                 pval[idx] = val[j0 + i];
             } else {
                 psrc[idx] = kPad;
@@ -152,13 +167,13 @@ __device__ __forceinline__ Level load_level(const Level *lv, int s) {
     return Level{v.x, v.y, v.z, v.w};
 }
 
-template <typename VT, int T>
-__device__ __forceinline__ void load_rows(const Level &L, const int *__restrict__ psrc, const VT *__restrict__ pval,
-                                          const VT *__restrict__ pinv, const VT *__restrict__ bp,
-                                          RowRegs<VT> (&R)[kRowsPerThread]) {
+template <typename VT, int T, int CS>
+__device__ __forceinline__ void load_rows(const Level &L, int g, const int *__restrict__ psrc,
+                                          const VT *__restrict__ pval, const VT *__restrict__ pinv,
+                                          const VT *__restrict__ bp, RowRegs<VT> (&R)[kRowsPerThread]) {
 #pragma unroll
     for (int k = 0; k < kRowsPerThread; ++k) {
-        const int t = threadIdx.x + k * T;
+        const int t = g + k * T * CS;
 #pragma unroll
         for (int i = 0; i < kEnts; ++i) R[k].src[i] = kPad;
         if (t < L.m) {
@@ -176,13 +191,12 @@ __device__ __forceinline__ void load_rows(const Level &L, const int *__restrict_
     }
 }
 
-// thread t prefetches the t-th 128-byte line of each of level L's ranges into
-// L2 (a level's ranges are at most kRowsPerThread*T rows; wider levels are
-// prefetched in part)
-template <typename VT, int T>
-__device__ __forceinline__ void prefetch_level_l2(const Level &L, const int *psrc, const VT *pval, const VT *pinv,
-                                                  const VT *bp) {
-    const long long o = (long long)threadIdx.x * 128;
+// the g-th thread of a run prefetches the g-th 128-byte line of each of level
+// L's ranges into L2 (wider levels are prefetched in part)
+template <typename VT>
+__device__ __forceinline__ void prefetch_level_l2(const Level &L, int g, const int *psrc, const VT *pval,
+                                                  const VT *pinv, const VT *bp) {
+    const long long o = (long long)g * 128;
     const long long ne = (long long)L.m * L.w;
     if (o < ne * 4) asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(psrc + L.base) + o));
     if (o < ne * (long long)sizeof(VT))
@@ -193,30 +207,53 @@ __device__ __forceinline__ void prefetch_level_l2(const Level &L, const int *psr
     }
 }
 
-template <typename VT>
-__device__ __forceinline__ VT solution(int src, const VT *ring, const VT *xp) {
-    return src < 0 ? ring[-src - 1] : xp[src];
+// A solution named by an entry: global position, own ring, or (in a cluster
+// run) the ring of another CTA through distributed shared memory.
+template <typename VT, int CS>
+__device__ __forceinline__ VT solution(int src, VT *ring, const VT *xp, unsigned rank) {
+    // in a cluster run another SM may have written xp[src]: read it from L2
+    // (L1 is not coherent across SMs); one CTA reads its own writes
+    if (src >= 0) return CS == 1 ? xp[src] : __ldcg(xp + src);
+    const int code = -src - 1;
+    if constexpr (CS == 1) {
+        return ring[code];
+    } else {
+        const unsigned owner = (unsigned)code >> kRingShift;
+        VT *slot = ring + (code & (kRing - 1));
+        if (owner == rank) return *slot;
+        return *cooperative_groups::this_cluster().map_shared_rank(slot, owner);
+    }
 }
 
-// Sweeps steps [s0, s1) of the pack in one CTA of T threads.
-template <typename VT, int T>
+template <int CS> __device__ __forceinline__ void run_barrier() {
+    if constexpr (CS == 1) __syncthreads();
+    else cooperative_groups::this_cluster().sync();  // barrier.cluster arrive.release / wait.acquire
+}
+
+// Sweeps steps [s0, s1) of the pack with CS CTAs of T threads (one CTA or one
+// cluster); thread g of the run solves rows g, g + T*CS, ... of every level.
+template <typename VT, int T, int CS>
 __device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const int *__restrict__ psrc,
                           const VT *__restrict__ pval, const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp,
                           VT *ring) {
     if (s0 >= s1) return;
+    constexpr int G = T * CS;
+    unsigned rank = 0;
+    if constexpr (CS > 1) rank = cooperative_groups::this_cluster().block_rank();
+    const int g = (int)rank * T + (int)threadIdx.x;
+    const int warp0 = g & ~31;
     RowRegs<VT> cur[kRowsPerThread], nxt[kRowsPerThread];
     Level Lc = load_level(lv, s0);
     Level Ln = load_level(lv, s0 + 1 < s1 ? s0 + 1 : s0);
-    load_rows<VT, T>(Lc, psrc, pval, pinv, bp, cur);
-    const int warp0 = threadIdx.x & ~31;
+    load_rows<VT, T, CS>(Lc, g, psrc, pval, pinv, bp, cur);
     for (int s = s0; s < s1; ++s) {
         const Level Lnn = load_level(lv, s + 2 < s1 ? s + 2 : s);
-        if (s + 1 < s1 && warp0 < Ln.m) load_rows<VT, T>(Ln, psrc, pval, pinv, bp, nxt);
-        if (s + 2 < s1) prefetch_level_l2<VT, T>(Lnn, psrc, pval, pinv, bp);
+        if (s + 1 < s1 && warp0 < Ln.m) load_rows<VT, T, CS>(Ln, g, psrc, pval, pinv, bp, nxt);
+        if (s + 2 < s1) prefetch_level_l2<VT>(Lnn, g, psrc, pval, pinv, bp);
         if (warp0 < Lc.m) {
 #pragma unroll
             for (int k = 0; k < kRowsPerThread; ++k) {
-                const int t = threadIdx.x + k * T;
+                const int t = g + k * G;
                 if (t < Lc.m) {
                     VT sum = VT(0);
                     bool more = true;
@@ -224,14 +261,14 @@ __device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const in
                     for (int i = 0; i < kEnts; ++i) {
                         const int src = cur[k].src[i];
                         if (src == kPad) { more = false; break; }
-                        sum += cur[k].v[i] * solution(src, ring, xp);
+                        sum += cur[k].v[i] * solution<VT, CS>(src, ring, xp, rank);
                     }
                     if (more)
                         for (int i = kEnts; i < Lc.w; ++i) {
                             const int idx = Lc.base + i * Lc.m + t;
                             const int src = psrc[idx];
                             if (src == kPad) break;
-                            sum += pval[idx] * solution(src, ring, xp);
+                            sum += pval[idx] * solution<VT, CS>(src, ring, xp, rank);
                         }
                     const int p = Lc.pos + t;
                     const VT x = (cur[k].b - sum) * cur[k].inv;
@@ -240,13 +277,13 @@ __device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const in
                 }
             }
             // rows beyond the register slots (levels wider than the slots cover)
-            for (int t = threadIdx.x + kRowsPerThread * T; t < Lc.m; t += T) {
+            for (int t = g + kRowsPerThread * G; t < Lc.m; t += G) {
                 VT sum = VT(0);
                 for (int i = 0; i < Lc.w; ++i) {
                     const int idx = Lc.base + i * Lc.m + t;
                     const int src = psrc[idx];
                     if (src == kPad) break;
-                    sum += pval[idx] * solution(src, ring, xp);
+                    sum += pval[idx] * solution<VT, CS>(src, ring, xp, rank);
                 }
                 const int p = Lc.pos + t;
                 const VT x = (bp[p] - sum) * pinv[p];
@@ -254,7 +291,9 @@ __device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const in
                 xp[p] = x;
             }
         }
-        __syncthreads();
+        // every CTA of a cluster passes this barrier after its last level too,
+        // so no CTA leaves while another may still read its ring
+        run_barrier<CS>();
         Lc = Ln;
         Ln = Lnn;
 #pragma unroll
@@ -267,7 +306,17 @@ __global__ void __launch_bounds__(T, 1)
     sweep_kernel(const Level *__restrict__ lv, int s0, int s1, const int *__restrict__ psrc,
                  const VT *__restrict__ pval, const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp) {
     extern __shared__ __align__(16) unsigned char smem[];
-    sweep_run<VT, T>(lv, s0, s1, psrc, pval, pinv, bp, xp, reinterpret_cast<VT *>(smem));
+    sweep_run<VT, T, 1>(lv, s0, s1, psrc, pval, pinv, bp, xp, reinterpret_cast<VT *>(smem));
+}
+
+// one run on a cluster of kClusterCTAs CTAs (launched with cluster dimensions)
+template <typename VT>
+__global__ void __launch_bounds__(kClusterThreads, 1)
+    sweep_cluster_kernel(const Level *__restrict__ lv, int s0, int s1, const int *__restrict__ psrc,
+                         const VT *__restrict__ pval, const VT *__restrict__ pinv, const VT *__restrict__ bp,
+                         VT *xp) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    sweep_run<VT, kClusterThreads, kClusterCTAs>(lv, s0, s1, psrc, pval, pinv, bp, xp, reinterpret_cast<VT *>(smem));
 }
 
 // Work queue of matrices; each CTA sweeps its matrix's steps.
@@ -285,7 +334,8 @@ __global__ void __launch_bounds__(T, 1)
         __syncthreads();  // m_sh is rewritten on the next turn
         if (q >= n_mats) return;
         const int m = queue_order[q];
-        sweep_run<VT, T>(lv, mat_steps[m], mat_steps[m + 1], psrc, pval, pinv, bp, xp, reinterpret_cast<VT *>(smem));
+        sweep_run<VT, T, 1>(lv, mat_steps[m], mat_steps[m + 1], psrc, pval, pinv, bp, xp,
+                            reinterpret_cast<VT *>(smem));
     }
 }
 
@@ -304,33 +354,80 @@ template <typename VT> void set_smem_attr() {
     set_smem_attr_t<VT, 256>();
     set_smem_attr_t<VT, 512>();
     set_smem_attr_t<VT, 1024>();
+    SMAX_CUDA(cudaFuncSetAttribute(sweep_cluster_kernel<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(kRing * sizeof(VT))));
     done[dev] = true;
 }
 
-// CTA size of a single-CTA run: enough threads for its widest level at
-// kRowsPerThread rows each, from 256 to 1024
-int run_threads(const LevelPack &pk, int s0, int s1) {
-    int w = 0;
-    for (int s = s0; s < s1; ++s) w = std::max(w, pk.h_lv[s].m);
-    const int need = (w + kRowsPerThread - 1) / kRowsPerThread;
-    return need <= 256 ? 256 : (need <= 512 ? 512 : 1024);
+cudaLaunchConfig_t cluster_config(cudaLaunchAttribute &attr, size_t smem, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kClusterCTAs, 1, 1);
+    cfg.blockDim = dim3(kClusterThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = kClusterCTAs;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+// whether a cluster of the sweep can be resident on this device
+template <typename VT> bool cluster_ok() {
+    static int state[64] = {};  // 0 unknown, 1 yes, 2 no
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return false;
+    if (state[dev] == 0) {
+        set_smem_attr<VT>();
+        cudaLaunchAttribute attr;
+        cudaLaunchConfig_t cfg = cluster_config(attr, kRing * sizeof(VT), nullptr);
+        int clusters = 0;
+        const cudaError_t e = cudaOccupancyMaxActiveClusters(&clusters, (void *)sweep_cluster_kernel<VT>, &cfg);
+        if (e != cudaSuccess) (void)cudaGetLastError();
+        state[dev] = (e == cudaSuccess && clusters > 0) ? 1 : 2;
+    }
+    return state[dev] == 1;
+}
+
+// Launch geometry of a run: (CTAs, threads per CTA) enough for its widest
+// level at kRowsPerThread rows each; a cluster for levels wider than 1024 rows
+// where allowed and resident, else up to one 1024-thread CTA.
+int2 run_geometry(int max_w, bool allow_cluster, int vbytes) {
+    const int need = (max_w + kRowsPerThread - 1) / kRowsPerThread;
+    if (need <= 256) return make_int2(1, 256);
+    if (need <= 512) return make_int2(1, 512);
+    if (allow_cluster && (vbytes == 8 ? cluster_ok<double>() : cluster_ok<float>()))
+        return make_int2(kClusterCTAs, kClusterThreads);
+    return make_int2(1, 1024);
 }
 
 template <typename VT>
-void launch_sweep(int threads, const LevelPack &pk, int s0, int s1, const int *psrc, const VT *pval,
-                  const VT *pinv, const VT *bp, VT *xp, cudaStream_t st) {
+void launch_run(const LevelPack &pk, int s0, int s1, const int *psrc, const VT *pval, const VT *pinv, const VT *bp,
+                VT *xp, cudaStream_t st) {
     const size_t sm = kRing * sizeof(VT);
     const Level *lv = pk.lv.as<Level>();
-    if (threads == 256) sweep_kernel<VT, 256><<<1, 256, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
-    else if (threads == 512) sweep_kernel<VT, 512><<<1, 512, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
-    else sweep_kernel<VT, 1024><<<1, 1024, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
+    const int2 geo = pk.h_geo[s0];
+    if (geo.x > 1) {
+        cudaLaunchAttribute attr;
+        cudaLaunchConfig_t cfg = cluster_config(attr, sm, st);
+        SMAX_CUDA(cudaLaunchKernelEx(&cfg, sweep_cluster_kernel<VT>, lv, s0, s1, psrc, pval, pinv, bp, xp));
+    } else if (geo.y == 256) {
+        sweep_kernel<VT, 256><<<1, 256, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
+    } else if (geo.y == 512) {
+        sweep_kernel<VT, 512><<<1, 512, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
+    } else {
+        sweep_kernel<VT, 1024><<<1, 1024, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
+    }
 }
 
 }  // namespace
 
 bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *val, const void *D, int vbytes,
                       int64_t n, const int *order, const std::vector<int> &src_begin, const std::vector<int> &count,
-                      const std::vector<int> &seg_begin, cudaStream_t st) {
+                      const std::vector<int> &seg_begin, bool allow_cluster, cudaStream_t st) {
     const int L = (int)count.size();
     if ((int)src_begin.size() != L || (int)seg_begin.size() != L) fail(SMAX_ERR_STATE, "inconsistent sweep steps");
     pk = LevelPack();
@@ -391,6 +488,17 @@ bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *v
         seg_pos[s] = pos_begin[seg_begin[s]];
     }
     pk.ents = base;
+    // launch geometry per run (steps sharing a run start), from its widest level
+    pk.h_geo.assign(L, make_int2(1, 256));
+    for (int s = 0; s < L;) {
+        int e = s + 1, mw = count[s];
+        while (e < L && seg_begin[e] == seg_begin[s]) mw = std::max(mw, count[e++]);
+        const int2 g2 = run_geometry(mw, allow_cluster, vbytes);
+        for (int k = s; k < e; ++k) pk.h_geo[k] = g2;
+        s = e;
+    }
+    DevBuf d_geo(sizeof(int2) * L);
+    SMAX_CUDA(cudaMemcpyAsync(d_geo.p, pk.h_geo.data(), sizeof(int2) * L, cudaMemcpyHostToDevice, st));
     pk.lv.alloc(sizeof(Level) * L);
     SMAX_CUDA(cudaMemcpyAsync(pk.lv.p, pk.h_lv.data(), sizeof(Level) * L, cudaMemcpyHostToDevice, st));
     DevBuf d_seg(sizeof(int) * L), flag(sizeof(int));
@@ -401,13 +509,13 @@ bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *v
     if (vbytes == 8)
         fill_kernel<double><<<grid_for(n), 256, 0, st>>>(
             rp, ci, static_cast<const double *>(val), static_cast<const double *>(D), n, pk.prow.as<int>(),
-            plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(), pk.psrc.as<int>(),
-            pk.pval.as<double>(), pk.pinv.as<double>(), flag.as<int>());
+            plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(), d_geo.as<int2>(),
+            pk.psrc.as<int>(), pk.pval.as<double>(), pk.pinv.as<double>(), flag.as<int>());
     else
         fill_kernel<float><<<grid_for(n), 256, 0, st>>>(
             rp, ci, static_cast<const float *>(val), static_cast<const float *>(D), n, pk.prow.as<int>(),
-            plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(), pk.psrc.as<int>(),
-            pk.pval.as<float>(), pk.pinv.as<float>(), flag.as<int>());
+            plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(), d_geo.as<int2>(),
+            pk.psrc.as<int>(), pk.pval.as<float>(), pk.pinv.as<float>(), flag.as<int>());
     SMAX_CUDA(cudaGetLastError());
     int h_flag = 0;
     SMAX_CUDA(cudaMemcpyAsync(&h_flag, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -433,8 +541,7 @@ void pack_solve(const LevelPack &pk, const std::vector<PackStep> &steps, const V
                     wide_level_kernel<VT><<<ceil_div_u(L.m, 256), 256, 0, st>>>(L, psrc, pval, pinv, bp, xp);
             }
         } else {
-            launch_sweep<VT>(run_threads(pk, s.first, s.first + s.count), pk, s.first, s.first + s.count, psrc, pval,
-                             pinv, bp, xp, st);
+            launch_run<VT>(pk, s.first, s.first + s.count, psrc, pval, pinv, bp, xp, st);
         }
     }
     scatter_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, xp, X);
@@ -449,7 +556,8 @@ void pack_solve_batch(const LevelPack &pk, const int *mat_steps, const int *queu
     const int *prow = pk.prow.as<int>();
     VT *bp = pk.bp.as<VT>(), *xp = pk.xp.as<VT>();
     gather_kernel<VT><<<grid_for(pk.n), 256, 0, st>>>(prow, pk.n, B, bp, X, pk.needs_x_init ? xp : nullptr);
-    const int threads = run_threads(pk, 0, pk.n_levels());
+    int threads = 256;
+    for (const int2 &g2 : pk.h_geo) threads = std::max(threads, g2.y);
     // one CTA per matrix at a time: as many CTAs as fit (the ring limits residency)
     const int per_sm = threads <= 512 ? 2 : 1;
     const int grid = std::max(1, std::min(n_mats, per_sm * sm_count()));

@@ -13,9 +13,11 @@ namespace smax {
 // i-th entry of the t-th row of level s sits at ent_base[s] + i*m[s] + t, so a
 // warp reads its rows' i-th entries with one coalesced load.  Each entry's
 // source is encoded for the single-CTA sweep:
-//   src <  0, != kPad : the solution is in the shared-memory ring slot -src-1
-//                       (written by the same sweep at most kRing positions ago
-//                       and not overwritten by the current level)
+//   src <  0, != kPad : the solution is in slot (-src-1) % kRing of the
+//                       shared-memory ring of CTA (-src-1) / kRing of the run's
+//                       cluster (0 for single-CTA runs); it was written by the
+//                       same run at most kRing positions ago and is not
+//                       overwritten by the current level
 //   src >= 0          : the solution's position in the position-ordered x
 //   src == kPad       : padding (the row has fewer entries than the level width)
 struct LevelPack {
@@ -29,6 +31,10 @@ struct LevelPack {
     int64_t n = 0, ents = 0;
     int vbytes = 8;
     std::vector<Level> h_lv;
+    // launch geometry of the run each step belongs to: x = CTAs in the cluster
+    // (1: a single CTA), y = threads per CTA; ring entries name the CTA that
+    // owns the solution when x > 1
+    std::vector<int2> h_geo;
     DevBuf lv;      // Level[n_levels]
     DevBuf prow;    // int[n]: row of each position
     DevBuf psrc;    // int[ents]
@@ -46,10 +52,12 @@ struct LevelPack {
 // a level solved by its own grid launch): only solutions produced inside the
 // same run may come from the ring.
 // Returns false (building nothing) when the per-level padding would make the
-// pack more than about three times the off-diagonal entries.
+// pack more than about three times the off-diagonal entries.  allow_cluster:
+// runs with levels wider than one CTA covers may be solved by a thread-block
+// cluster (single matrices; the batch kernel is one CTA per matrix).
 bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *val, const void *D, int vbytes,
                       int64_t n, const int *order, const std::vector<int> &src_begin, const std::vector<int> &count,
-                      const std::vector<int> &seg_begin, cudaStream_t st);
+                      const std::vector<int> &seg_begin, bool allow_cluster, cudaStream_t st);
 
 // Solves with the pack: gathers B into position order, runs each step --
 // wide levels as one grid launch each, runs of narrow levels as one

@@ -243,7 +243,7 @@ void TriBatch::build(int vbytes_, const std::vector<RegCRS> &mats, cudaStream_t 
             seg_begin[l] = moff[m];
         }
     pack_ok = build_level_pack(pack, A.rp(), A.ci(), A.val.p, D.p, vbytes, n_rows, order.as<int>(), src_begin, count,
-                               seg_begin, st);
+                               seg_begin, false, st);
 }
 
 template <typename VT>
