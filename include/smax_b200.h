@@ -94,6 +94,7 @@ typedef int smax_status;
 #define SMAX_FLAG_TEST_FORCE_TIMEOUT 14 /* test only: the persistent solve's barrier waits for a missing arrival */
 #define SMAX_FLAG_REFINE 15            /* float64 SpTRSV: solve in FP32, then this many FP64-residual corrections (0: off) */
 #define SMAX_FLAG_REFINE_TOL 16        /* stop refining once max|dx| <= 10^-value * max|x| (host check per step; 0: run all) */
+#define SMAX_FLAG_SWEEP_CLUSTER 17     /* SpTRSV: runs with levels wider than 1024 rows on a thread-block cluster (0: one CTA) */
 
 /* SpTRSV / SpTRSM launch schemes (SMAX_FLAG_SOLVE_MODE) */
 #define SMAX_SOLVE_AUTO 0        /* graph-captured, narrow levels merged (the default) */
@@ -230,7 +231,8 @@ smax_status smax_kernel_get_refine_stats(smax_kernel k, int *steps, double *last
 /* --------------------------------------------------------------- autotuning */
 /* Times the launch variants of an initialized kernel on its registered
  * operands and keeps the fastest: the CRS SpMV kernel for SpMV; the solve
- * mode and the level-merge threshold for SpTRSV / SpTRSM.  Choices are cached
+ * mode, the level-merge threshold and (SpTRSV) cluster runs for SpTRSV /
+ * SpTRSM.  Choices are cached
  * for the life of the process per matrix (kernel type, value type, sizes and
  * a hash of the pattern); a later kernel with the same matrix takes them from
  * the cache.  Overwrites the output operand (C for SpMV, B for solves). */
@@ -238,6 +240,7 @@ typedef struct smax_tuning {
     int spmv_variant; /* SMAX_FLAG_SPMV_VARIANT chosen (SpMV) */
     int solve_mode;   /* SMAX_SOLVE_* chosen (SpTRSV / SpTRSM) */
     int level_merge;  /* SMAX_FLAG_LEVEL_MERGE chosen (SpTRSV / SpTRSM) */
+    int sweep_cluster; /* SMAX_FLAG_SWEEP_CLUSTER chosen (SpTRSV) */
     int from_cache;   /* 1: taken from the process-wide cache */
     int n_candidates; /* configurations timed (0 from the cache) */
     double seconds;   /* one apply with the choice */

@@ -76,7 +76,8 @@ SIGNATURES = {
 class Tuning(C.Structure):
     """struct smax_tuning"""
     _fields_ = [("spmv_variant", C.c_int), ("solve_mode", C.c_int), ("level_merge", C.c_int),
-                ("from_cache", C.c_int), ("n_candidates", C.c_int), ("seconds", C.c_double)]
+                ("sweep_cluster", C.c_int), ("from_cache", C.c_int), ("n_candidates", C.c_int),
+                ("seconds", C.c_double)]
 
 
 class FormatChoice(C.Structure):

@@ -202,6 +202,7 @@ void tri_upload(smax_kernel_s *k) {
 
 template <typename VT> void tri_apply_t(smax_kernel_s *k, const VT *Bv, VT *Xv) {
     tri_plan(k);
+    k->tri.set_allow_cluster(k->sweep_cluster);
     if constexpr (sizeof(VT) == 8) {
         if (k->refine_steps > 0) {
             require(k->ktype == SMAX_KERNEL_SPTRSV, SMAX_ERR_UNSUPPORTED,
@@ -552,6 +553,7 @@ smax_status smax_kernel_set_flag(smax_kernel k, int flag, int value) {
             require(value >= 0 && value <= 16, SMAX_ERR_BAD_ARG, "refinement tolerance exponent must be in [0, 16]");
             kk->refine_tol = value;
             break;
+        case SMAX_FLAG_SWEEP_CLUSTER: kk->sweep_cluster = v; break;
         case SMAX_FLAG_LEVEL_MERGE:
             require(value >= 0, SMAX_ERR_BAD_ARG, "level merge threshold must be >= 0");
             kk->level_merge = value;

@@ -45,6 +45,7 @@ void ensure_adjoint(smax_kernel_s *k) {
         k->adj_plan.assign_reverse(k->tri, k->stream);
         k->adj_plan_serial = k->tri_plan_serial;
     }
+    k->adj_plan.set_allow_cluster(k->sweep_cluster);
 }
 
 template <typename VT> void adjoint_t(smax_kernel_s *k, const VT *x, const VT *g, VT *din, VT *dval) {

@@ -87,6 +87,7 @@ void tune_kernel(smax_kernel_s *k, smax_tuning &r) {
     r.spmv_variant = k->spmv_variant;
     r.solve_mode = k->solve_mode;
     r.level_merge = k->level_merge;
+    r.sweep_cluster = k->sweep_cluster;
     double best = 1e300;
     if (k->ktype == SMAX_KERNEL_SPMV && !k->f_scs && !k->f_bcrs) {
         build_crs_plans(k);
@@ -98,15 +99,20 @@ void tune_kernel(smax_kernel_s *k, smax_tuning &r) {
         }
         k->spmv_variant = r.spmv_variant;
     } else if (is_tri(k)) {
-        struct Cand { int mode, merge; };
+        struct Cand { int mode, merge; bool cluster; };
         std::vector<Cand> cands;
-        for (int m : {0, 1024, 4096, 16384, 65536}) cands.push_back({SMAX_SOLVE_GRAPH, m});
+        for (int m : {0, 1024, 4096, 16384, 65536}) cands.push_back({SMAX_SOLVE_GRAPH, m, false});
         const bool one_rhs = k->ktype == SMAX_KERNEL_SPTRSV || (k->B.n_cols <= 1);
+        if (k->ktype == SMAX_KERNEL_SPTRSV) {
+            cands.push_back({SMAX_SOLVE_GRAPH, 4096, true});
+            cands.push_back({SMAX_SOLVE_GRAPH, 16384, true});
+        }
         if (k->ktype == SMAX_KERNEL_SPTRSV && one_rhs && k->refine_steps == 0)
-            cands.push_back({SMAX_SOLVE_PERSISTENT, 0});
+            cands.push_back({SMAX_SOLVE_PERSISTENT, 0, false});
         for (const Cand &c : cands) {
             k->solve_mode = c.mode;
             k->level_merge = c.merge;
+            k->sweep_cluster = c.cluster;
             double t;
             try {
                 t = time_apply(k);
@@ -116,10 +122,11 @@ void tune_kernel(smax_kernel_s *k, smax_tuning &r) {
                 continue;
             }
             ++r.n_candidates;
-            if (t < best) { best = t; r.solve_mode = c.mode; r.level_merge = c.merge; }
+            if (t < best) { best = t; r.solve_mode = c.mode; r.level_merge = c.merge; r.sweep_cluster = c.cluster; }
         }
         k->solve_mode = r.solve_mode;
         k->level_merge = r.level_merge;
+        k->sweep_cluster = r.sweep_cluster != 0;
     } else {
         best = time_apply(k);
         r.n_candidates = 1;
@@ -134,6 +141,7 @@ void apply_choice(smax_kernel_s *k, const smax_tuning &t) {
     } else if (is_tri(k)) {
         k->solve_mode = t.solve_mode;
         k->level_merge = t.level_merge;
+        k->sweep_cluster = t.sweep_cluster != 0;
     }
 }
 

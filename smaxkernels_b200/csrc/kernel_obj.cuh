@@ -144,6 +144,7 @@ struct smax_kernel_s {
 
     // FP32 solve + FP64 residual refinement (refine.cu); 0 steps = off
     int refine_steps = 0, refine_tol = 0;
+    bool sweep_cluster = false;     // allow cluster runs in the level-pack solves
     smax::RefineState refine;
 
     // stopwatches

@@ -228,7 +228,7 @@ bool TriPlan::ensure_pack(const int *rp, const int *ci, const void *val, const v
     release_graph();
     pack_ok = false;
     const bool ok = build_level_pack(pack, rp, ci, val, D, vbytes, n_rows, has_order ? order.as<int>() : nullptr,
-                                     src_begin, count, seg_begin, true, st);
+                                     src_begin, count, seg_begin, allow_cluster, st);
     if (!ok) {
         pack_unfit = true;
         return false;

@@ -52,6 +52,15 @@ struct TriPlan {
     LevelPack pack;
     std::vector<PackStep> pack_steps;
     bool pack_ok = false, pack_unfit = false;
+    bool allow_cluster = false;  // runs wider than one CTA covers may use a cluster
+    // sets allow_cluster; a change drops the pack and the graph
+    void set_allow_cluster(bool v) {
+        if (v != allow_cluster) {
+            allow_cluster = v;
+            pack_ok = false;
+            release_graph();
+        }
+    }
     const void *pack_key[2] = {nullptr, nullptr};
     uint64_t pack_tag = ~0ull;
     int pack_merge = -1, pack_vbytes = 0;

@@ -64,7 +64,7 @@ class SpMVType(enum.IntEnum):
 FLAG = dict(mat_perm=0, mat_upper_triang=1, mat_lower_triang=2, vec_row_major=3, mat_scs=4, mat_bcrs=5,
             block_column_major=6, kernel_impl=7, device_pointers=8, a_dirty=9,
             spmv_variant=10, solve_mode=11, level_merge=12, spin_limit=13, test_force_timeout=14,
-            refine=15, refine_tol=16)
+            refine=15, refine_tol=16, sweep_cluster=17)
 
 SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED, SOLVE_GRAPH, SOLVE_PERSISTENT = 0, 1, 2, 3, 4
 
@@ -235,6 +235,10 @@ class Kernel:
     def set_spin_limit(self, kilo_polls: int):
         """Polls (x 1000) before a persistent solve's grid barrier gives up with TIMEOUT."""
         return self._flag("spin_limit", kilo_polls)
+
+    def set_sweep_cluster(self, v: bool):
+        """SpTRSV: let runs with levels wider than 1024 rows use a thread-block cluster."""
+        return self._flag("sweep_cluster", int(bool(v)))
 
     def set_level_merge(self, rows: int):
         """Levels with at most `rows` (row, right-hand side) pairs run merged in one CTA."""

@@ -1,6 +1,6 @@
-"""Level-pack solves whose runs have levels wider than 1024 rows: these run on
-a thread-block cluster (8 CTAs, solutions shared through distributed shared
-memory).  Checked against the oracle, lower and upper, FP64 and FP32, with
+"""Level-pack solves whose runs have levels wider than 1024 rows, with
+cluster runs enabled: these run on a thread-block cluster (8 CTAs, solutions
+shared through distributed shared memory).  Checked against the oracle, lower and upper, FP64 and FP32, with
 long-distance couplings that must be read from global memory, and through
 the adjoint (the reversed plan)."""
 import numpy as np
@@ -23,6 +23,7 @@ def _kernel(vt, upper=False, mode=0):
     if upper:
         k.set_mat_upper_triang(True)
     k.set_solve_mode(mode)
+    k.set_sweep_cluster(True)
     return smax, k
 
 
