@@ -3,6 +3,7 @@
 //
 // Dispatch mirrors the reference's L2 kernel fronts (src/kernels/spmv.hpp:138-195,
 // spmm.hpp:68-100): the kernel type and the flags pick the format and kernel.
+#include <algorithm>
 #include <cstring>
 
 #include "abi_internal.cuh"
@@ -10,6 +11,12 @@
 
 smax_kernel_s::~smax_kernel_s() {
     if (stream) cudaStreamSynchronize(stream);
+    if (copy_stream) {
+        cudaStreamSynchronize(copy_stream);
+        cudaStreamDestroy(copy_stream);
+    }
+    for (auto &r : out_ranges) cudaEventDestroy(r.ev);
+    for (auto e : ev_pool) cudaEventDestroy(e);
     if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -296,6 +303,99 @@ void check_extents(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
     require(c_off + need_c <= k->C.elems(), SMAX_ERR_BAD_ARG, "C (with offset) is smaller than the operator needs");
 }
 
+// ------------------------------------------- host-mode output download --
+void record_out(smax_kernel_s *k, uint64_t off, uint64_t count) {
+    // the same range written again: only its latest write is downloaded
+    for (auto &r : k->out_ranges)
+        if (r.off == off && r.count == count) {
+            SMAX_CUDA(cudaEventRecord(r.ev, k->stream));
+            return;
+        }
+    cudaEvent_t e;
+    if (!k->ev_pool.empty()) {
+        e = k->ev_pool.back();
+        k->ev_pool.pop_back();
+    } else {
+        SMAX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    SMAX_CUDA(cudaEventRecord(e, k->stream));
+    k->out_ranges.push_back({off, count, e});
+}
+
+// first element and element count of the output one apply writes
+uint64_t out_offset(const smax_kernel_s *k, uint64_t b_off, uint64_t c_off) { return is_tri(k) ? b_off : c_off; }
+uint64_t out_count(const smax_kernel_s *k) {
+    const uint64_t kk = k->B.n_cols ? k->B.n_cols : 1;
+    switch (k->ktype) {
+    case SMAX_KERNEL_SPMV:
+        if (k->f_scs) return k->A_scs.n_rows_padded;
+        if (k->f_bcrs) return k->A_bcrs.n_rows * k->A_bcrs.hpad;
+        return k->A.n_rows;
+    case SMAX_KERNEL_SPMM: return k->A.n_rows * kk;
+    case SMAX_KERNEL_SPTRSV: return k->A.n_rows;
+    case SMAX_KERNEL_SPTRSM: return k->A.n_rows * kk;
+    default: return 0;
+    }
+}
+
+// CRS SpMV with the warp-stream kernel in host mode, large enough that the
+// kernel time is worth hiding under the download of y: builds (once per
+// upload) row blocks starting at entries that are multiples of 4 (the
+// kernel's 16-byte loads), each with its own plan over the shared device copy
+bool pipe_ready(smax_kernel_s *k) {
+    if (k->ktype != SMAX_KERNEL_SPMV || k->f_scs || k->f_bcrs || k->spmv_variant == 2) return false;
+    if (k->pipe_blocks < 2 || k->dA.n_rows < (1 << 18)) return false;
+    auto &P = k->pipe;
+    if (P.a_version == k->a_version) return P.blocks() > 0;
+    P = smax_kernel_s::SpmvPipe();
+    P.a_version = k->a_version;
+    const int64_t n = k->dA.n_rows, nnz = k->dA.nnz;
+    const int *rp = static_cast<const int *>(k->A.row_ptr);  // the registered host row pointer
+    std::vector<int64_t> r0{0}, e0{0};
+    for (int b = 1; b < k->pipe_blocks; ++b) {
+        const int64_t target = nnz * b / k->pipe_blocks;
+        int64_t r = std::lower_bound(rp, rp + n + 1, (int)target) - rp;
+        int64_t limit = std::min<int64_t>(n, r + 4096);
+        while (r < limit && (rp[r] % 4) != 0) ++r;
+        if (r >= limit || r <= r0.back() || rp[r] <= e0.back()) continue;
+        r0.push_back(r);
+        e0.push_back(rp[r]);
+    }
+    if (r0.size() < 2) return false;
+    r0.push_back(n);
+    e0.push_back(nnz);
+    const int nb = (int)r0.size() - 1;
+    P.plans.resize(nb);
+    P.rps.resize(nb);
+    for (int b = 0; b < nb; ++b) {
+        const int64_t rows = r0[b + 1] - r0[b];
+        std::vector<int> h(rows + 1);
+        for (int64_t i = 0; i <= rows; ++i) h[i] = rp[r0[b] + i] - (int)e0[b];
+        P.rps[b].alloc(sizeof(int) * (rows + 1));
+        SMAX_CUDA(cudaMemcpyAsync(P.rps[b].p, h.data(), sizeof(int) * (rows + 1), cudaMemcpyHostToDevice, k->stream));
+        P.plans[b].build(P.rps[b].as<int>(), rows, e0[b + 1] - e0[b], k->vbytes, k->stream);
+    }
+    P.r0 = std::move(r0);
+    P.e0 = std::move(e0);
+    return true;
+}
+
+template <typename VT> void apply_pipe_t(smax_kernel_s *k, const VT *x, VT *y, uint64_t c_off) {
+    const auto &P = k->pipe;
+    for (int b = 0; b < P.blocks(); ++b) {
+        crs_spmv_stream<VT>(P.plans[b], k->dA.ci() + P.e0[b], k->dA.val.as<VT>() + P.e0[b], x, y + P.r0[b],
+                            k->stream);
+        record_out(k, c_off + (uint64_t)P.r0[b], (uint64_t)(P.r0[b + 1] - P.r0[b]));
+    }
+}
+
+void apply_pipelined(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
+    const void *b = dev_b(k, b_off);
+    void *c = dev_c(k, c_off);
+    if (k->vbytes == 8) apply_pipe_t<double>(k, static_cast<const double *>(b), static_cast<double *>(c), c_off);
+    else apply_pipe_t<float>(k, static_cast<const float *>(b), static_cast<float *>(c), c_off);
+}
+
 void do_initialize(smax_kernel_s *k) {
     double t0 = wall_s();
     if (k->ktype == SMAX_KERNEL_SPGEMM) {
@@ -326,12 +426,12 @@ void do_initialize(smax_kernel_s *k) {
         size_t bb = (size_t)k->B.elems() * k->vbytes, cb = (size_t)k->C.elems() * k->vbytes;
         k->dB.ensure(bb);
         k->dC.ensure(cb);
-        // the kernel's input: B (x / X) for SpMV and SpMM, C (b / B) for solves
-        if (is_tri(k)) {
-            if (cb) SMAX_CUDA(cudaMemcpyAsync(k->dC.p, k->C.val, cb, cudaMemcpyHostToDevice, k->stream));
-        } else {
-            if (bb) SMAX_CUDA(cudaMemcpyAsync(k->dB.p, k->B.val, bb, cudaMemcpyHostToDevice, k->stream));
-        }
+        // the kernel's input: B (x / X) for SpMV and SpMM; C (b / B) for
+        // solves, and their X too (a solve reads the current x for entries
+        // outside its triangle, as the reference's loops do)
+        if (is_tri(k) && cb)
+            SMAX_CUDA(cudaMemcpyAsync(k->dC.p, k->C.val, cb, cudaMemcpyHostToDevice, k->stream));
+        if (bb) SMAX_CUDA(cudaMemcpyAsync(k->dB.p, k->B.val, bb, cudaMemcpyHostToDevice, k->stream));
     }
     SMAX_CUDA(cudaStreamSynchronize(k->stream));
     k->timers["initialize"] += wall_s() - t0;
@@ -361,7 +461,12 @@ void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
     k->timers["apply"] += k->apply_events.trim(512);
     auto ev = k->apply_events.acquire();
     SMAX_CUDA(cudaEventRecord(ev.first, k->stream));
-    apply_core(k, b_off, c_off);
+    if (!k->f_device && pipe_ready(k)) {
+        apply_pipelined(k, b_off, c_off);  // records one output range per row block
+    } else {
+        apply_core(k, b_off, c_off);
+        if (!k->f_device) record_out(k, out_offset(k, b_off, c_off), out_count(k));
+    }
     SMAX_CUDA(cudaEventRecord(ev.second, k->stream));
 }
 
@@ -412,14 +517,23 @@ void do_finalize(smax_kernel_s *k) {
         k->timers["finalize"] += wall_s() - t0;
         return;
     }
-    if (!k->f_device) {
-        if (is_tri(k)) {
-            size_t bb = (size_t)k->B.elems() * k->vbytes;
-            if (bb) SMAX_CUDA(cudaMemcpyAsync(k->B.val, k->dB.p, bb, cudaMemcpyDeviceToHost, k->stream));
-        } else {
-            size_t cb = (size_t)k->C.elems() * k->vbytes;
-            if (cb) SMAX_CUDA(cudaMemcpyAsync(k->C.val, k->dC.p, cb, cudaMemcpyDeviceToHost, k->stream));
+    if (!k->f_device && !k->out_ranges.empty()) {
+        // exactly the ranges apply() wrote, each as soon as it is complete
+        if (!k->copy_stream)
+            SMAX_CUDA(cudaStreamCreateWithFlags(&k->copy_stream, cudaStreamNonBlocking));
+        const bool solve = is_tri(k);
+        char *host = static_cast<char *>(solve ? k->B.val : k->C.val);
+        const char *dev = static_cast<const char *>(solve ? k->dB.p : k->dC.p);
+        const size_t vb = (size_t)k->vbytes;
+        for (const auto &r : k->out_ranges) {
+            SMAX_CUDA(cudaStreamWaitEvent(k->copy_stream, r.ev, 0));
+            if (r.count)
+                SMAX_CUDA(cudaMemcpyAsync(host + r.off * vb, dev + r.off * vb, r.count * vb, cudaMemcpyDeviceToHost,
+                                          k->copy_stream));
         }
+        SMAX_CUDA(cudaStreamSynchronize(k->copy_stream));
+        for (const auto &r : k->out_ranges) k->ev_pool.push_back(r.ev);
+        k->out_ranges.clear();
     }
     SMAX_CUDA(cudaStreamSynchronize(k->stream));
     read_status(k);
@@ -554,6 +668,11 @@ smax_status smax_kernel_set_flag(smax_kernel k, int flag, int value) {
             kk->refine_tol = value;
             break;
         case SMAX_FLAG_SWEEP_CLUSTER: kk->sweep_cluster = v; break;
+        case SMAX_FLAG_SPMV_PIPELINE:
+            require(value >= 0 && value <= 64, SMAX_ERR_BAD_ARG, "pipeline blocks must be in [0, 64]");
+            kk->pipe_blocks = value;
+            kk->pipe.a_version = ~0ull;
+            break;
         case SMAX_FLAG_LEVEL_MERGE:
             require(value >= 0, SMAX_ERR_BAD_ARG, "level merge threshold must be >= 0");
             kk->level_merge = value;

@@ -147,6 +147,28 @@ struct smax_kernel_s {
     bool sweep_cluster = false;     // allow cluster runs in the level-pack solves
     smax::RefineState refine;
 
+    // host-pointer mode: output ranges written by apply() since the last
+    // finalize(), each with the event after which it is complete; finalize
+    // downloads exactly these on copy_stream
+    struct OutRange {
+        uint64_t off, count;
+        cudaEvent_t ev;
+    };
+    std::vector<OutRange> out_ranges;
+    std::vector<cudaEvent_t> ev_pool;
+    cudaStream_t copy_stream = nullptr;
+
+    // CRS SpMV in host-pointer mode: row blocks whose results are downloaded
+    // while later blocks still compute (built on first use)
+    struct SpmvPipe {
+        uint64_t a_version = ~0ull;
+        std::vector<int64_t> r0, e0;           // first row / entry of each block, plus an end sentinel
+        std::vector<smax::CrsStreamPlan> plans;
+        std::vector<smax::DevBuf> rps;         // rebased row pointers
+        int blocks() const { return (int)plans.size(); }
+    } pipe;
+    int pipe_blocks = 4;                        // SMAX_FLAG_SPMV_PIPELINE (0: off)
+
     // stopwatches
     std::map<std::string, double> timers;
     smax::PendingEvents apply_events;

@@ -61,7 +61,9 @@ void upload_crs(DevCRS &d, const RegCRS &r, int vbytes, cudaStream_t st, int64_t
     d.nnz = (int64_t)r.nnz;
     if (r.n_rows >= (1ull << 31) || r.nnz + (uint64_t)pad >= (1ull << 31) || r.n_cols >= (1ull << 31))
         fail(SMAX_ERR_UNSUPPORTED, "int32 indices cannot address this matrix");
-    const int64_t cap = pad > 1 ? (d.nnz + pad - 1) / pad * pad : d.nnz;
+    // one spare slice: a row block's last slice may start mid-array and read up
+    // to one slice past its end (the pipelined SpMV), always inside the buffer
+    const int64_t cap = pad > 1 ? (d.nnz + pad - 1) / pad * pad + pad : d.nnz;
     d.row_ptr.alloc(sizeof(int) * (r.n_rows + 1));
     d.col.alloc(sizeof(int) * cap);
     d.val.alloc((size_t)vbytes * cap);

@@ -64,7 +64,7 @@ class SpMVType(enum.IntEnum):
 FLAG = dict(mat_perm=0, mat_upper_triang=1, mat_lower_triang=2, vec_row_major=3, mat_scs=4, mat_bcrs=5,
             block_column_major=6, kernel_impl=7, device_pointers=8, a_dirty=9,
             spmv_variant=10, solve_mode=11, level_merge=12, spin_limit=13, test_force_timeout=14,
-            refine=15, refine_tol=16, sweep_cluster=17)
+            refine=15, refine_tol=16, sweep_cluster=17, spmv_pipeline=18)
 
 SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED, SOLVE_GRAPH, SOLVE_PERSISTENT = 0, 1, 2, 3, 4
 
