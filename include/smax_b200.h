@@ -26,6 +26,8 @@
  *   - Pointers given to register_* are HOST pointers owned by the caller, as in
  *     the reference (src/kernels/spmv.hpp:89-91), unless the kernel has the
  *     SMAX_FLAG_DEVICE_POINTERS flag, in which case B and C are device pointers.
+ *     A CRS matrix may also be registered as device arrays: initialize copies
+ *     it in the direction its addresses give.
  *   - Index type int32 and value types float32/float64 are supported; other
  *     combinations return SMAX_ERR_UNSUPPORTED_TYPE.
  *   - Streams are passed as void* (a cudaStream_t).
@@ -357,6 +359,74 @@ void smax_free_host(void *p);
 smax_status smax_spmv_crs_noalloc(int float_type, uint64_t n_rows, uint64_t n_cols, uint64_t nnz,
                                   const void *d_row_ptr, const void *d_col, const void *d_val, const void *d_x,
                                   void *d_y, void *stream);
+
+/* ---------------------------------------------------------- solver callers */
+/* The iterative solvers of the reference's applications on device-resident
+ * operators.  The reference runs them as programs that call run() on SpMV and
+ * SpTRSV kernels once per iteration and do the vector arithmetic on the host:
+ *   Jacobi        examples/applications/jacobi/jacobi.cpp:14-130 with
+ *                 jacobi/utils.hpp:7-50 (diagonal moved to the end of each
+ *                 row; x_new = (b - (A x_old - D x_old)) / D)
+ *   Gauss-Seidel  examples/applications/gauss_seidel/gauss_seidel.cpp:13-111
+ *                 on the D+L / U split of examples/examples_common.hpp:283-398
+ *                 (x = (D+L)^-1 (b - U x))
+ * Both run the applications' loop:
+ *   residual = max_i |b_i - (A x)_i|
+ *   while (residual > tol && n_iters < max_iters) {
+ *       one iteration; ++n_iters;
+ *       if (n_iters % check_length == 0) residual = max_i |b_i - (A x)_i|;
+ *   }
+ * NaN entries never become the maximum (applications_common.hpp:122-133).
+ * Jacobi keeps the application's two iterate buffers, swapped after every
+ * iteration; its residual kernel stays bound to the first x_new buffer
+ * (jacobi.cpp:14-24, 96-100), so the residual after an odd iteration count is
+ * that of the latest iterate and after an even count that of the one before.
+ *
+ * create copies the square CRS matrix (int32 indices, host or device arrays)
+ * to the device and validates it: Jacobi needs a diagonal entry with
+ * |a_ii| >= 1e-16 in every row (SMAX_ERR_NO_DIAG / SMAX_ERR_ZERO_DIAG), as
+ * utils.hpp:7-36 does; Gauss-Seidel's D+L part is solved by this platform's
+ * level-scheduled SpTRSV, with the same diagonal checks.  The solver owns its
+ * vectors; solve copies b and x in (host or device arrays, n_rows values of
+ * the solver's type), runs the loop on `stream` (a cudaStream_t; NULL = the
+ * solver's own stream) and copies the solution back into x before it returns.
+ * Drivers (smax_solver_opts.mode), all with the same kernel launches:
+ *   SMAX_SOLVER_DEVICE_LOOP   one CUDA graph: a conditional while node repeats
+ *                             check_length iterations and the residual until a
+ *                             device kernel ends the loop; the host waits once
+ *   SMAX_SOLVER_GRAPH_BLOCKS  one graph launch per check_length iterations and
+ *                             residual; the host reads each residual
+ *   SMAX_SOLVER_PLAIN         the same launches one by one, no graphs */
+typedef struct smax_solver_s *smax_solver;
+#define SMAX_SOLVER_JACOBI 0
+#define SMAX_SOLVER_GAUSS_SEIDEL 1
+#define SMAX_SOLVER_DEVICE_LOOP 0
+#define SMAX_SOLVER_GRAPH_BLOCKS 1
+#define SMAX_SOLVER_PLAIN 2
+
+typedef struct {
+    double tol;       /* the loop runs while residual > tol (the applications' TOL: 1e-8) */
+    int max_iters;    /* MAX_ITERS: 1000 */
+    int check_length; /* CHECK_LENGTH: 5 (>= 1) */
+    int mode;         /* SMAX_SOLVER_* driver */
+} smax_solver_opts;
+
+typedef struct {
+    int n_iters;          /* iterations run */
+    int converged;        /* residual_norm < tol, the applications' test */
+    double residual_norm; /* the last residual measured */
+    int n_checks;         /* residuals measured, the one before the loop included */
+    int host_waits;       /* times the host waited for the device inside the loop */
+} smax_solver_stats;
+
+smax_status smax_solver_create(smax_solver *out, int kind, int float_type, uint64_t n_rows, uint64_t nnz,
+                               const void *row_ptr, const void *col, const void *val);
+smax_status smax_solver_solve(smax_solver s, const void *b, void *x, const smax_solver_opts *opts,
+                              smax_solver_stats *stats, void *stream);
+/* The residuals of the last solve in the order they were measured: writes
+ * min(cap, n_checks) of them to out (host array) and n_checks to *count. */
+smax_status smax_solver_get_history(smax_solver s, double *out, int cap, int *count);
+smax_status smax_solver_destroy(smax_solver s);
 
 #ifdef __cplusplus
 }

@@ -290,6 +290,120 @@ class Oracle:
         getattr(self.lib, f"orc_apply_vec_perm_{_sfx(vec.dtype)}")(len(perm), _p(vec), _p(out), _p(_i32(perm)))
         return out
 
+    # -- the solver applications (examples/applications) --------------------
+    @staticmethod
+    def infty_norm(v):
+        """infty_vec_norm (applications_common.hpp:122-133): the largest |v_i|
+        found by `>` comparisons from 0, so NaNs never win."""
+        a = np.abs(np.asarray(v, dtype=np.float64))
+        a = a[a > 0.0]
+        return float(a.max()) if len(a) else 0.0
+
+    @staticmethod
+    def jacobi_peel(row_ptr, col, val):
+        """peel_diag_crs of the Jacobi application (jacobi/utils.hpp:7-36): the
+        last diagonal entry of each row swapped into the row's last slot;
+        returns (col', val', D).  A missing or |a_ii| < 1e-16 diagonal raises."""
+        rp = np.asarray(row_ptr, dtype=np.int64)
+        n = len(rp) - 1
+        col = np.array(col, dtype=np.int32)
+        val = np.array(val)
+        row_of = np.repeat(np.arange(n), np.diff(rp))
+        d = np.nonzero(col == row_of)[0]
+        last = np.full(n, -1, dtype=np.int64)
+        np.maximum.at(last, row_of[d], d)
+        if n and (last < 0).any():
+            raise ValueError(f"No diag! (row {int(np.argmax(last < 0))})")
+        D = val[last].copy() if n else np.zeros(0, dtype=val.dtype)
+        if n and (np.abs(D) < 1e-16).any():
+            raise ValueError("Zero diag!")
+        end = rp[1:] - 1
+        for arr in (col, val):
+            t = arr[last].copy()
+            arr[last] = arr[end]
+            arr[end] = t
+        return col, val, D
+
+    @staticmethod
+    def split_d_l_u(row_ptr, col, val):
+        """extract_D_L_U (examples/examples_common.hpp:283-398): D+L = entries
+        with col <= row, U = the rest, each row in its own entry order."""
+        rp = np.asarray(row_ptr, dtype=np.int64)
+        n = len(rp) - 1
+        row_of = np.repeat(np.arange(n), np.diff(rp))
+        low = np.asarray(col) <= row_of
+        out = []
+        for m in (low, ~low):
+            r = np.zeros(n + 1, dtype=np.int32)
+            np.cumsum(np.bincount(row_of[m], minlength=n), out=r[1:])
+            out.append((r, np.asarray(col, dtype=np.int32)[m].copy(), np.asarray(val)[m].copy()))
+        return out[0], out[1]
+
+    def jacobi_app(self, row_ptr, col, val, b, x_init, tol=1e-8, max_iters=1000, check_length=5):
+        """The loop of examples/applications/jacobi/jacobi.cpp:14-58 on the
+        matrix as given (the application permutes it first, :82-93):
+          x_old = x_new = x_init; r = |b - A x_new|_inf
+          while r > tol and n < max_iters:
+              x_new = A x_old                                  ("x_new <- Ax_old")
+              x_new = (b - (x_new - D x_old)) / D              (normalize_x)
+              swap(x_old, x_new); n += 1                       (swap_operands)
+              if n % check_length == 0: r = |b - A P|_inf      (P: the first x_new)
+        with A's diagonal moved to each row end (peel_diag_crs).  Returns
+        (latest iterate, n, r, residual history)."""
+        pcol, pval, D = self.jacobi_peel(row_ptr, col, val)
+        rp = _i32(row_ptr)
+        b = np.asarray(b, dtype=pval.dtype)
+        x_old = np.array(x_init, dtype=pval.dtype)
+        x_new = x_old.copy()
+        P = x_new  # the buffer "tmp <- Ax" was registered with
+
+        def resid():
+            return self.infty_norm(b - self.spmv_crs(rp, pcol, pval, P))
+
+        norm = resid()
+        hist = [norm]
+        n = 0
+        while norm > tol and n < max_iters:
+            x_new[:] = self.spmv_crs(rp, pcol, pval, x_old)
+            diag_contrib = D * x_old
+            offdiag_sum = x_new - diag_contrib
+            x_new[:] = (b - offdiag_sum) / D
+            x_old, x_new = x_new, x_old
+            n += 1
+            if n % check_length == 0:
+                norm = resid()
+                hist.append(norm)
+        return x_old.copy(), n, norm, np.array(hist)
+
+    def gauss_seidel_app(self, row_ptr, col, val, b, x_init, tol=1e-8, max_iters=1000, check_length=5):
+        """The loop of examples/applications/gauss_seidel/gauss_seidel.cpp:13-50:
+          r = |b - A x|_inf
+          while r > tol and n < max_iters:
+              tmp = b - U x; x = (D+L)^-1 tmp (the reference's plain forward
+              sweep, sptrsv_cpu_crs_impl.hpp:9-55); n += 1
+              if n % check_length == 0: r = |b - A x|_inf
+        Returns (x, n, r, residual history)."""
+        (lrp, lcol, lval), (urp, ucol, uval) = self.split_d_l_u(row_ptr, col, val)
+        rp = _i32(row_ptr)
+        val = np.asarray(val)
+        b = np.asarray(b, dtype=val.dtype)
+        x = np.array(x_init, dtype=val.dtype)
+
+        def resid():
+            return self.infty_norm(b - self.spmv_crs(rp, col, val, x))
+
+        norm = resid()
+        hist = [norm]
+        n = 0
+        while norm > tol and n < max_iters:
+            tmp = b - self.spmv_crs(urp, ucol, uval, x)
+            x = self.sptrsv(lrp, lcol, lval, tmp)
+            n += 1
+            if n % check_length == 0:
+                norm = resid()
+                hist.append(norm)
+        return x, n, norm, np.array(hist)
+
 
 # --------------------------------------------------------------------------
 # The reference itself (oracle/_ref), where it was built
@@ -340,10 +454,38 @@ class Reference:
         L.ref_time_generate_perm.restype = C.c_double
         L.ref_apply_mat_perm.argtypes = [_INT, _INT, _P, _P, _P, _P, _P, _P, _P, _P]
         L.ref_apply_vec_perm.argtypes = [_INT, _INT, _P, _P, _P]
+        for name in ("ref_jacobi", "ref_gauss_seidel"):
+            f = getattr(L, name)
+            f.argtypes = [_U64, _U64, _P, _P, _P, _P, _P, C.c_double, _INT, _INT, C.POINTER(_INT),
+                          C.POINTER(C.c_double), _P, _INT, C.POINTER(_INT)]
+            f.restype = C.c_double
 
     def _check(self, rc):
         if rc != 0:
             raise RuntimeError(f"reference error: {self.lib.ref_last_error().decode()}")
+
+    def _app(self, fn, row_ptr, col, val, b, x_init, tol, max_iters, check_length):
+        rp, col = _i32(row_ptr), _i32(col)
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.array(x_init, dtype=np.float64)
+        cap = max_iters // max(check_length, 1) + 1
+        hist = np.zeros(cap, dtype=np.float64)
+        it, norm, nch = _INT(0), C.c_double(0.0), _INT(0)
+        t = fn(len(rp) - 1, len(col), _p(col), _p(rp), _p(val), _p(b), _p(x), float(tol), int(max_iters),
+               int(check_length), C.byref(it), C.byref(norm), _p(hist), cap, C.byref(nch))
+        if t < 0:
+            self._check(-1)
+        return x, it.value, norm.value, hist[: min(nch.value, cap)], t
+
+    def jacobi_app(self, row_ptr, col, val, b, x_init, tol=1e-8, max_iters=1000, check_length=5):
+        """The Jacobi program's loop through the reference's kernels (ref_jacobi):
+        (x, n_iters, residual, history, seconds in the loop)."""
+        return self._app(self.lib.ref_jacobi, row_ptr, col, val, b, x_init, tol, max_iters, check_length)
+
+    def gauss_seidel_app(self, row_ptr, col, val, b, x_init, tol=1e-8, max_iters=1000, check_length=5):
+        """The Gauss-Seidel program's loop through the reference's kernels."""
+        return self._app(self.lib.ref_gauss_seidel, row_ptr, col, val, b, x_init, tol, max_iters, check_length)
 
     def set_threads(self, n: int) -> int:
         return self.lib.ref_set_threads(n)

@@ -21,9 +21,12 @@
 #include "error_handler.cpp"
 
 #include <chrono>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <stdexcept>
 #include <string>
+#include <vector>
 
 namespace {
 
@@ -561,6 +564,186 @@ int ref_apply_vec_perm(int vbits, int n, void *vec, void *vec_perm,
                                                (double *)vec_perm, perm);
         return 0;
     });
+}
+
+// ------------------------------------------------------ solver applications --
+// The loops of the reference's iterative-solver programs,
+// examples/applications/jacobi/jacobi.cpp:14-58 and
+// gauss_seidel/gauss_seidel.cpp:13-50, on a caller's matrix (the programs fix
+// a 10x10 Poisson problem), driven through the reference's kernels the way the
+// programs drive them: run() on CPU SpMV / SpTRSV kernels once per step, the
+// vector arithmetic on the host as their helpers do it (subtract_vectors with
+// an OpenMP loop, normalize_x and infty_vec_norm serial,
+// applications_common.hpp:113-133, jacobi/utils.hpp:38-50).  FP64, as the
+// programs.  hist receives up to hist_cap residuals and *n_checks their count;
+// the return value is the seconds spent after the first residual, or -1.
+namespace {
+
+double app_norm(const double *v, uint64_t n) {
+    double m = 0.0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const double a = (v[i] >= 0) ? v[i] : -1 * v[i];
+        if (a > m)
+            m = a;
+    }
+    return m;
+}
+
+void app_subtract(double *out, const double *a, const double *b, uint64_t n) {
+#pragma omp parallel for
+    for (long long i = 0; i < (long long)n; ++i)
+        out[i] = a[i] - 1.0 * b[i];
+}
+
+struct AppLog {
+    double *hist;
+    int cap;
+    int count = 0;
+    void add(double v) {
+        if (count < cap)
+            hist[count] = v;
+        ++count;
+    }
+};
+
+} // namespace
+
+double ref_jacobi(uint64_t n, uint64_t nnz, const int *col, int *row_ptr, const double *val, const double *b,
+                  double *x, double tol, int max_iters, int check_length, int *n_iters, double *final_norm,
+                  double *hist, int hist_cap, int *n_checks) {
+    double t = -1.0;
+    int rc = guarded([&] {
+        // peel_diag_crs (jacobi/utils.hpp:7-36) on a copy of the matrix
+        std::vector<int> pc(col, col + nnz);
+        std::vector<double> pv(val, val + nnz), D(n);
+        for (uint64_t r = 0; r < n; ++r) {
+            const int s = row_ptr[r], e = row_ptr[r + 1] - 1;
+            int dj = -1;
+            for (int j = s; j <= e; ++j)
+                if ((uint64_t)pc[j] == r)
+                    dj = j;
+            if (dj < 0)
+                throw std::runtime_error("No diag!");
+            D[r] = pv[dj];
+            if (std::abs(D[r]) < 1e-16)
+                throw std::runtime_error("Zero diag!");
+            if (dj != e) {
+                std::swap(pc[dj], pc[e]);
+                std::swap(pv[dj], pv[e]);
+            }
+        }
+        std::vector<double> x_new(x, x + n), x_old(x, x + n), tmp(n), residual(n);
+        SMAX::Interface smax;
+        smax.register_kernel("tmp <- Ax", SMAX::KernelType::SPMV, SMAX::PlatformType::CPU);
+        smax.kernel("tmp <- Ax")->register_A(n, n, nnz, pc.data(), row_ptr, pv.data());
+        smax.kernel("tmp <- Ax")->register_B(n, x_new.data());
+        smax.kernel("tmp <- Ax")->register_C(n, tmp.data());
+        smax.register_kernel("x_new <- Ax_old", SMAX::KernelType::SPMV, SMAX::PlatformType::CPU);
+        smax.kernel("x_new <- Ax_old")->register_A(n, n, nnz, pc.data(), row_ptr, pv.data());
+        smax.kernel("x_new <- Ax_old")->register_B(n, x_old.data());
+        smax.kernel("x_new <- Ax_old")->register_C(n, x_new.data());
+        double *xo = x_old.data(), *xn = x_new.data();
+        AppLog log{hist, hist_cap};
+        auto check = [&] {
+            smax.kernel("tmp <- Ax")->run();
+            app_subtract(residual.data(), b, tmp.data(), n);
+            return app_norm(residual.data(), n);
+        };
+        double norm = check();
+        log.add(norm);
+        int it = 0;
+        const double t0 = now_s();
+        while (norm > tol && it < max_iters) {
+            smax.kernel("x_new <- Ax_old")->run();
+            for (uint64_t i = 0; i < n; ++i) {
+                const double diag_contrib = D[i] * xo[i];
+                const double offdiag_sum = xn[i] - diag_contrib;
+                xn[i] = (b[i] - offdiag_sum) / D[i];
+            }
+            smax.kernel("x_new <- Ax_old")->swap_operands();
+            std::swap(xo, xn);
+            ++it;
+            if (it % check_length == 0) {
+                norm = check();
+                log.add(norm);
+            }
+        }
+        t = now_s() - t0;
+        std::memcpy(x, xo, sizeof(double) * n);
+        *n_iters = it;
+        *final_norm = norm;
+        *n_checks = log.count;
+        return 0;
+    });
+    return rc == 0 ? t : -1.0;
+}
+
+double ref_gauss_seidel(uint64_t n, uint64_t nnz, const int *col, const int *row_ptr, const double *val,
+                        const double *b, double *x, double tol, int max_iters, int check_length, int *n_iters,
+                        double *final_norm, double *hist, int hist_cap, int *n_checks) {
+    double t = -1.0;
+    int rc = guarded([&] {
+        // extract_D_L_U (examples/examples_common.hpp:283-398): col <= row to
+        // D+L, the rest to U, in-row order kept
+        std::vector<int> arp(row_ptr, row_ptr + n + 1), acol(col, col + nnz);
+        std::vector<double> aval(val, val + nnz);
+        std::vector<int> lrp(n + 1, 0), urp(n + 1, 0), lcol, ucol;
+        std::vector<double> lval, uval;
+        for (uint64_t r = 0; r < n; ++r) {
+            for (int j = arp[r]; j < arp[r + 1]; ++j) {
+                if ((uint64_t)acol[j] <= r) {
+                    lcol.push_back(acol[j]);
+                    lval.push_back(aval[j]);
+                } else {
+                    ucol.push_back(acol[j]);
+                    uval.push_back(aval[j]);
+                }
+            }
+            lrp[r + 1] = (int)lcol.size();
+            urp[r + 1] = (int)ucol.size();
+        }
+        std::vector<double> xv(x, x + n), tmp(n), residual(n);
+        SMAX::Interface smax;
+        smax.register_kernel("tmp <- Ax", SMAX::KernelType::SPMV, SMAX::PlatformType::CPU);
+        smax.kernel("tmp <- Ax")->register_A(n, n, nnz, acol.data(), arp.data(), aval.data());
+        smax.kernel("tmp <- Ax")->register_B(n, xv.data());
+        smax.kernel("tmp <- Ax")->register_C(n, tmp.data());
+        smax.register_kernel("tmp <- Ux", SMAX::KernelType::SPMV, SMAX::PlatformType::CPU);
+        smax.kernel("tmp <- Ux")->register_A(n, n, (uint64_t)ucol.size(), ucol.data(), urp.data(), uval.data());
+        smax.kernel("tmp <- Ux")->register_B(n, xv.data());
+        smax.kernel("tmp <- Ux")->register_C(n, tmp.data());
+        smax.register_kernel("solve", SMAX::KernelType::SPTRSV);
+        smax.kernel("solve")->register_A(n, n, (uint64_t)lcol.size(), lcol.data(), lrp.data(), lval.data());
+        smax.kernel("solve")->register_B(n, xv.data());
+        smax.kernel("solve")->register_C(n, tmp.data());
+        AppLog log{hist, hist_cap};
+        auto check = [&] {
+            smax.kernel("tmp <- Ax")->run();
+            app_subtract(residual.data(), b, tmp.data(), n);
+            return app_norm(residual.data(), n);
+        };
+        double norm = check();
+        log.add(norm);
+        int it = 0;
+        const double t0 = now_s();
+        while (norm > tol && it < max_iters) {
+            smax.kernel("tmp <- Ux")->run();
+            app_subtract(tmp.data(), b, tmp.data(), n);
+            smax.kernel("solve")->run();
+            ++it;
+            if (it % check_length == 0) {
+                norm = check();
+                log.add(norm);
+            }
+        }
+        t = now_s() - t0;
+        std::memcpy(x, xv.data(), sizeof(double) * n);
+        *n_iters = it;
+        *final_norm = norm;
+        *n_checks = log.count;
+        return 0;
+    });
+    return rc == 0 ? t : -1.0;
 }
 
 } // extern "C"

@@ -69,6 +69,10 @@ SIGNATURES = {
     "smax_utils_apply_vec_perm": (I32, [I32, U64, P, P, P]),
     "smax_free_host": (None, [P]),
     "smax_spmv_crs_noalloc": (I32, [I32, U64, U64, U64, P, P, P, P, P, P]),
+    "smax_solver_create": (I32, [PP, I32, I32, U64, U64, P, P, P]),
+    "smax_solver_solve": (I32, [P, P, P, P, P, P]),
+    "smax_solver_get_history": (I32, [P, P, I32, C.POINTER(I32)]),
+    "smax_solver_destroy": (I32, [P]),
 }
 
 
@@ -85,6 +89,17 @@ class FormatChoice(C.Structure):
     _fields_ = [("format", C.c_int), ("spmv_variant", C.c_int), ("C", C.c_int), ("sigma", C.c_int),
                 ("b_height", C.c_int), ("b_width", C.c_int), ("n_candidates", C.c_int), ("seconds", C.c_double),
                 ("crs_seconds", C.c_double)]
+
+
+class SolverOpts(C.Structure):
+    """struct smax_solver_opts"""
+    _fields_ = [("tol", C.c_double), ("max_iters", C.c_int), ("check_length", C.c_int), ("mode", C.c_int)]
+
+
+class SolverStats(C.Structure):
+    """struct smax_solver_stats"""
+    _fields_ = [("n_iters", C.c_int), ("converged", C.c_int), ("residual_norm", C.c_double),
+                ("n_checks", C.c_int), ("host_waits", C.c_int)]
 
 
 def struct_dict(s) -> dict:

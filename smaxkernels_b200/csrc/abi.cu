@@ -199,8 +199,8 @@ void tri_upload(smax_kernel_s *k) {
     // the reference moves each diagonal entry to the end of its row in the
     // caller's arrays (sptrsv_cpu_core.hpp:21-38); mirror that
     if (k->A.nnz) {
-        SMAX_CUDA(cudaMemcpyAsync(k->A.col, k->dA.col.p, sizeof(int) * k->A.nnz, cudaMemcpyDeviceToHost, st));
-        SMAX_CUDA(cudaMemcpyAsync(k->A.val, k->dA.val.p, (size_t)k->vbytes * k->A.nnz, cudaMemcpyDeviceToHost, st));
+        SMAX_CUDA(cudaMemcpyAsync(k->A.col, k->dA.col.p, sizeof(int) * k->A.nnz, cudaMemcpyDefault, st));
+        SMAX_CUDA(cudaMemcpyAsync(k->A.val, k->dA.val.p, (size_t)k->vbytes * k->A.nnz, cudaMemcpyDefault, st));
     }
     SMAX_CUDA(cudaStreamSynchronize(st));
     k->tri_plan_valid = false;
@@ -349,6 +349,14 @@ bool pipe_ready(smax_kernel_s *k) {
     if (P.a_version == k->a_version) return P.blocks() > 0;
     P = smax_kernel_s::SpmvPipe();
     P.a_version = k->a_version;
+    // the row blocks are cut on the host copy of row_ptr: A registered as
+    // device arrays is not pipelined
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, k->A.row_ptr) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    if (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged) return false;
     const int64_t n = k->dA.n_rows, nnz = k->dA.nnz;
     const int *rp = static_cast<const int *>(k->A.row_ptr);  // the registered host row pointer
     std::vector<int64_t> r0{0}, e0{0};

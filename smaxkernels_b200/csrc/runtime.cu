@@ -72,11 +72,13 @@ void upload_crs(DevCRS &d, const RegCRS &r, int vbytes, cudaStream_t st, int64_t
         SMAX_CUDA(cudaMemsetAsync(static_cast<char *>(d.val.p) + (size_t)vbytes * d.nnz, 0,
                                   (size_t)vbytes * (cap - d.nnz), st));
     }
-    SMAX_CUDA(cudaMemcpyAsync(d.row_ptr.p, r.row_ptr, sizeof(int) * (r.n_rows + 1), cudaMemcpyHostToDevice, st));
+    // the registered arrays may be host or device memory: the copy direction
+    // follows from the addresses (unified addressing)
+    SMAX_CUDA(cudaMemcpyAsync(d.row_ptr.p, r.row_ptr, sizeof(int) * (r.n_rows + 1), cudaMemcpyDefault, st));
     if (r.nnz) {
-        SMAX_CUDA(cudaMemcpyAsync(d.col.p, r.col, sizeof(int) * r.nnz, cudaMemcpyHostToDevice, st));
+        SMAX_CUDA(cudaMemcpyAsync(d.col.p, r.col, sizeof(int) * r.nnz, cudaMemcpyDefault, st));
         // a pattern-only upload (val == nullptr) leaves the values unset
-        if (r.val) SMAX_CUDA(cudaMemcpyAsync(d.val.p, r.val, (size_t)vbytes * r.nnz, cudaMemcpyHostToDevice, st));
+        if (r.val) SMAX_CUDA(cudaMemcpyAsync(d.val.p, r.val, (size_t)vbytes * r.nnz, cudaMemcpyDefault, st));
     }
 }
 

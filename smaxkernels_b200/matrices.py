@@ -13,6 +13,10 @@ reference, so every comparison is made on identical inputs.
                              columns uniform without repeats, sorted; values U[-1,1].
 * :func:`stencil27`        -- 27-point 3D stencil, values U[0.5,1], diagonal 27.
 * :func:`laplace2d_5pt`    -- 5-point 2D Laplacian, diagonal 4, off-diagonals -1.
+* :func:`poisson2d_app`    -- the same operator in the row layout of the solver
+                             applications (examples/applications/
+                             applications_common.hpp:61-111): in-row order left,
+                             bottom, diagonal, top, right (not sorted).
 * :func:`lower_triangle`   -- D+L split of a CRS matrix (entries with col <= row),
                              as examples/examples_common.hpp:282-398 extract_D_L_U.
 * :func:`random_symmetric_permutation` -- P A P^T for a seeded random P with the
@@ -69,6 +73,21 @@ def laplace3d_7pt(nx: int, dtype=np.float64):
 def laplace2d_5pt(nx: int, dtype=np.float64):
     offs = [(0, 0), (-1, 0), (1, 0), (0, -1), (0, 1)]
     return _stencil((nx, nx), offs, 4.0, lambda m: np.full(m, -1.0), dtype)
+
+
+def poisson2d_app(nx: int, dtype=np.float64):
+    """create2DPoissonMatrixCRS(nx): row i*nx + j holds, in this order, the
+    entries of row-1 (j > 0), row-nx (i > 0), the diagonal 4, row+nx
+    (i < nx-1) and row+1 (j < nx-1), off-diagonals -1."""
+    nx = int(nx)
+    r = np.arange(nx * nx, dtype=np.int64)
+    i, j = r // nx, r % nx
+    parts = [(j > 0, r - 1, -1.0), (i > 0, r - nx, -1.0), (np.ones_like(r, bool), r, 4.0),
+             (i < nx - 1, r + nx, -1.0), (j < nx - 1, r + 1, -1.0)]
+    M = np.stack([p[0] for p in parts], axis=1)
+    Cc = np.stack([p[1] for p in parts], axis=1)
+    V = np.stack([np.full(len(r), p[2]) for p in parts], axis=1)
+    return _finish(M.sum(axis=1), Cc[M], V[M].astype(dtype))
 
 
 def stencil27(nx: int, seed: int = 2, dtype=np.float64):

@@ -11,6 +11,14 @@ Usage (from the repository root, where the reference checkout exists):
    values (``x[i] = 1.0``), type aliases and flag setter calls.  Nothing is
    retyped by hand; the values are parsed from the test sources as text.
 
+3. solver_apps.json -- the printed output of the reference's two iterative-
+   solver applications, examples/applications/{jacobi,gauss_seidel}, built
+   unmodified by ``make -C oracle apps`` (oracle/_ref/jacobi, gauss_seidel)
+   and run with one OpenMP thread (the BFS permutation the Jacobi program
+   prints is thread-order dependent): the permutation, the residual printed
+   every CHECK_LENGTH iterations ("%f"), the iteration count and the final
+   residual (6 significant digits).
+
 2. bcrs_laplace.json -- examples/tests/spmv_bcrs_laplace_test.hpp builds its
    input in code (a 16x16 tridiagonal 2/-1 matrix, x_i = 1/((i+3)%23+1),
    4x8 blocks in both in-block orders).  The same construction is restated
@@ -120,6 +128,34 @@ def laplace_fixture() -> dict:
     return fx
 
 
+def solver_apps_fixture() -> dict:
+    import subprocess
+    out = {}
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    for app in ("jacobi", "gauss_seidel"):
+        exe = os.path.join(REPO, "oracle", "_ref", app)
+        run = subprocess.run([exe], capture_output=True, text=True, env=env, cwd=os.path.join(REPO, "oracle", "_ref"),
+                             check=True)
+        rec = {"program": f"examples/applications/{app}/{app}.cpp", "domain_size": 10, "tol": 1e-8,
+               "max_iters": 1000, "check_length": 5, "iters": [], "residuals": []}
+        for line in run.stdout.splitlines():
+            m = re.match(r"iter: (\d+), residual_norm = (\S+)", line)
+            if m:
+                rec["iters"].append(int(m.group(1)))
+                rec["residuals"].append(m.group(2))
+            m = re.match(r"Using permutation vector: \[(.*)\]", line)
+            if m:
+                rec["perm"] = [int(t) for t in m.group(1).split(",")]
+            m = re.match(r".* solver converged after (\d+) iterations", line)
+            if m:
+                rec["converged_after"] = int(m.group(1))
+            m = re.match(r"Final residual norm: (\S+)", line)
+            if m:
+                rec["final_residual"] = m.group(1)
+        out[app] = rec
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default="/root/reference")
@@ -133,6 +169,8 @@ def main():
         json.dump(data, f, indent=1, sort_keys=True)
     with open(os.path.join(HERE, "bcrs_laplace.json"), "w") as f:
         json.dump(laplace_fixture(), f, indent=1)
+    with open(os.path.join(HERE, "solver_apps.json"), "w") as f:
+        json.dump(solver_apps_fixture(), f, indent=1)
     print("wrote", len(data), "test fixtures")
 
 

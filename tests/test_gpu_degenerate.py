@@ -4,10 +4,7 @@ or trivial) result, never an error or a device fault."""
 import numpy as np
 import pytest
 
-from oracle.oracle import Oracle
-
 pytestmark = pytest.mark.gpu
-O = Oracle()
 
 
 def _k(ktype, vt=np.float64):
