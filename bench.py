@@ -204,7 +204,7 @@ def config_dict(nnz, vbytes, world):
 # line per case, same keys as the headline line.  Single GPU.
 # ---------------------------------------------------------------------------
 EXTRA_WORKLOADS = ("spmv_laplace64", "scs_spmv", "bcrs_spmv", "spmm", "spgemm", "sptrsv", "sptrsv_batch",
-                   "sptrsv_refine", "adjoint")
+                   "sptrsv_refine", "adjoint", "solvers", "cusparse")
 
 
 class Bench:
@@ -693,6 +693,241 @@ def wl_adjoint(b: Bench):
         torch.cuda.empty_cache()
 
 
+def _solver_iter_bytes(kind, n, nnz, nnz_u, nnz_l, vb, check_length):
+    """Algorithmic bytes of one iteration (the residual every check_length
+    iterations spread over them): each stored array and vector once."""
+    resid = (vb + 4) * nnz + 4 * (n + 1) + 2 * vb * n
+    if kind == "jacobi":  # A, x gathered once, D, b, x_new written
+        it = (vb + 4) * nnz + 4 * (n + 1) + 4 * vb * n
+    else:  # tmp = b - U x, then the D+L solve (b, x, D)
+        it = (vb + 4) * nnz_u + 4 * (n + 1) + 3 * vb * n + _tri_bytes(n, nnz_l, vb)
+    return it + resid / check_length
+
+
+def wl_solvers(b: Bench):
+    """The reference's Jacobi and Gauss-Seidel programs on device-resident
+    operators: (1) the programs' own 10x10 Poisson problem to convergence,
+    wall-clock time to solution for each driver next to the reference loop on
+    the host; (2) the same operators on a 2048^2 grid, a fixed number of
+    iterations (tol 0), per-iteration time and algorithmic GB/s."""
+    import time as _time
+    from smaxkernels_b200 import Interface
+    from smaxkernels_b200 import matrices as M
+    from smaxkernels_b200.solvers import Solver
+    torch = b.torch
+    st_ptr = b.stream.cuda_stream
+
+    def problem(kind, nx):
+        rp, col, val = M.poisson2d_app(nx)
+        n = len(rp) - 1
+        if kind == "jacobi":  # the program permutes A by BFS first (jacobi.cpp:82-91)
+            smax = Interface()
+            perm, inv = np.zeros(n, np.int32), np.zeros(n, np.int32)
+            smax.utils.generate_perm(n, rp, col, perm, inv, "BFS")
+            prp, pcol, pval = np.zeros(n + 1, np.int32), np.zeros(len(col), np.int32), np.zeros(len(col))
+            smax.utils.apply_mat_perm(n, rp, col, val, prp, pcol, pval, perm, inv)
+            smax.close()
+            return prp, pcol, pval, np.ones(n), (np.ones(n) if kind == "jacobi" else np.zeros(n))
+        return rp, col, val, np.ones(n), np.zeros(n)
+
+    for kind in ("jacobi", "gauss_seidel"):
+        rp, col, val, rhs, x0 = problem(kind, 10)
+        n = len(rp) - 1
+        bd, x0d = b.dev(rhs), b.dev(x0)
+        xd = x0d.clone()
+        res = {}
+        with Solver(kind, rp, col, val) as s:
+            for mode in ("device_loop", "graph_blocks", "plain"):
+                def run():
+                    xd.copy_(x0d)
+                    return s.solve(bd, xd, mode=mode, stream=st_ptr)
+                for _ in range(3):
+                    run()
+                ts = []
+                for _ in range(30):
+                    t0 = _time.perf_counter()
+                    stt = run()
+                    ts.append(_time.perf_counter() - t0)
+                res[mode] = (float(np.median(ts)), stt)
+        cpu = None
+        if b.ref is not None:
+            fn = b.ref.jacobi_app if kind == "jacobi" else b.ref.gauss_seidel_app
+            tc = [fn(rp, col, val, rhs, x0)[4] for _ in range(20)]
+            cpu = {"value": round(float(np.median(tc)) * 1e3, 5), "unit": "ms", "cores": b.threads,
+                   "kind": "reference", "sample": "the program's loop through the reference's kernels, median of 20"}
+        t, stt = res["device_loop"]
+        b.emit(f"solver_{kind}_poisson2d_10_program", "time to solution (wall clock, host-synchronous call)",
+               t * 1e3, "ms", t, 30, "f64", {"n_rows": n, "nnz": len(col), "tol": 1e-8, "check_length": 5,
+                                            "driver": "device_loop"}, None, None, cpu, higher=False,
+               n_iters=stt["n_iters"], residual=stt["residual_norm"],
+               graph_blocks_ms=round(res["graph_blocks"][0] * 1e3, 4), plain_ms=round(res["plain"][0] * 1e3, 4))
+
+    side = b.args.solver_side
+    for kind in ("jacobi", "gauss_seidel"):
+        iters = b.args.solver_iters if kind == "jacobi" else max(2, b.args.solver_iters // 20)
+        rp, col, val, rhs, _ = problem(kind, side)
+        n, nnz = len(rp) - 1, len(col)
+        row_of = np.repeat(np.arange(n), np.diff(rp))
+        nnz_l = int((col <= row_of).sum())
+        nnz_u = nnz - nnz_l
+        del row_of
+        rhs = M.uniform_vector(n, 4)
+        bd, x0d = b.dev(rhs), b.zeros(n, np.float64)
+        xd = x0d.clone()
+        cl = 5
+        with Solver(kind, rp, col, val) as s:
+            def run():
+                xd.copy_(x0d)
+                s.solve(bd, xd, tol=0.0, max_iters=iters, check_length=cl, stream=st_ptr)
+            with b.clocks() as clk:
+                t, reps = b.time(run, budget_s=3.0, max_reps=20)
+        t_it = t / iters
+        nbytes = _solver_iter_bytes(kind, n, nnz, nnz_u, nnz_l, 8, cl)
+        cpu = None
+        if b.ref is not None:
+            fn = b.ref.jacobi_app if kind == "jacobi" else b.ref.gauss_seidel_app
+            k_cpu = 5 if kind == "jacobi" else 3
+            tc = fn(rp, col, val, rhs, np.zeros(n), 0.0, k_cpu, cl)[4] / k_cpu
+            cpu = {"value": round(nbytes / tc / 1e9, 3), "unit": "GB/s", "cores": b.threads, "kind": "reference",
+                   "sample": f"{k_cpu} iterations of the program's loop through the reference's kernels",
+                   "ms_per_iteration": round(tc * 1e3, 4)}
+        kern = "jacobi_kernel" if kind == "jacobi" else "rhs_kernel + level-pack SpTRSV (sweep_kernel)"
+        b.emit(f"solver_{kind}_poisson2d_{side}", "solver iteration GB/s (algorithmic bytes)", nbytes / t_it / 1e9,
+               "GB/s", t_it, reps, "f64", {"n_rows": n, "nnz": nnz, "iterations": iters, "check_length": cl,
+                                          "driver": "device_loop", "inputs": "larger than L2"},
+               clk.summary(), b.hbm(nbytes, t_it, kern), cpu, ms_per_iteration=round(t_it * 1e3, 5))
+        torch.cuda.empty_cache()
+
+
+def wl_cusparse(b: Bench):
+    """cuSPARSE, called through torch.sparse with the library's default
+    algorithm choice, on the matrices of this platform's workloads (the
+    reference's examples/benchmarks/cusparse_benchmarks measure the same
+    operations: CSR SpMV, BSR SpMV, CSR SpMM).  One line per case: cuSPARSE's
+    GB/s (the same algorithmic bytes as this platform's line), with this
+    platform's time for the same operation on the same device arrays beside it."""
+    from smaxkernels_b200 import KernelType
+    from smaxkernels_b200 import matrices as M
+    from smaxkernels_b200.matrices import crs_bytes
+    torch = b.torch
+    f64 = torch.float64
+
+    def csr(rp, col, val, n_cols):
+        return torch.sparse_csr_tensor(b.dev(rp.astype(np.int32)), b.dev(col.astype(np.int32)), b.dev(val),
+                                       size=(len(rp) - 1, n_cols))
+
+    def line(name, what, nbytes, t_lib, t_ours, reps, config, clk, kern_lib, extra=None):
+        b.emit(name, f"cuSPARSE {what} GB/s (through torch.sparse)", nbytes / t_lib / 1e9, "GB/s", t_lib, reps,
+               "f64", config, clk, b.hbm(nbytes, t_lib, kern_lib), None,
+               ours_ms=round(t_ours * 1e3, 5), cusparse_ms=round(t_lib * 1e3, 5),
+               ours_over_cusparse=round(t_lib / t_ours, 3), **(extra or {}))
+
+    # CSR SpMV: the headline matrix and the 7-point 64^3 Laplacian
+    for name, (rp, col, val), x in (
+            ("lognormal_4194304", M.lognormal_random(1 << 22, seed=1), None),
+            ("laplace3d_64", M.laplace3d_7pt(64), None)):
+        n, nnz = len(rp) - 1, len(col)
+        xd = b.dev(M.uniform_vector(n, 100))
+        yd = b.zeros(n, np.float64)
+        A = csr(rp, col, val, n)
+        smax, k = b.kernel(KernelType.SPMV, np.float64)
+        y2 = b.zeros(n, np.float64)
+        k.register_A(n, n, nnz, col, rp, val)
+        k.register_B(n, xd)
+        k.register_C(n, y2)
+        k.set_stream(b.stream.cuda_stream)
+        k.initialize()
+        with b.clocks() as clk:
+            t_lib, reps = b.time(lambda: torch.mv(A, xd, out=yd))
+            t_ours, _ = b.time(k.apply)
+        err = float(torch.linalg.norm(yd - y2) / torch.linalg.norm(y2))
+        line(f"cusparse_csr_spmv_f64_{name}", "CSR SpMV", crs_bytes(n, nnz, n, 8), t_lib, t_ours, reps,
+             {"n_rows": n, "nnz": nnz, "library_call": "torch.mv(sparse_csr, x)"}, clk.summary(),
+             "cusparse SpMV (CSR)", {"rel_diff_vs_ours": err})
+        smax.close()
+        del A, xd, yd, y2
+        torch.cuda.empty_cache()
+
+    # CSR SpMM, 27-point 128^3, k = 16, row-major X
+    rp, col, val = M.stencil27(128)
+    n, nnz = len(rp) - 1, len(col)
+    kv = 16
+    X = b.dev(np.random.default_rng(2).uniform(-1, 1, n * kv))
+    A = csr(rp, col, val, n)
+    Y = torch.zeros(n, kv, dtype=f64, device="cuda")
+    smax, k = b.kernel(KernelType.SPMM, np.float64, lambda k: k.set_vec_row_major(True))
+    Y2 = b.zeros(n * kv, np.float64)
+    k.register_A(n, n, nnz, col, rp, val)
+    k.register_B(n, kv, X)
+    k.register_C(n, kv, Y2)
+    k.set_stream(b.stream.cuda_stream)
+    k.initialize()
+    X2 = X.view(n, kv)
+    with b.clocks() as clk:
+        t_lib, reps = b.time(lambda: torch.mm(A, X2, out=Y))
+        t_ours, _ = b.time(k.apply)
+    err = float(torch.linalg.norm(Y.reshape(-1) - Y2) / torch.linalg.norm(Y2))
+    line("cusparse_csr_spmm_k16_f64_stencil27_128", "CSR SpMM", (8 + 4) * nnz + 4 * (n + 1) + 2 * 8 * n * kv,
+         t_lib, t_ours, reps, {"n_rows": n, "nnz": nnz, "k": kv, "library_call": "torch.mm(sparse_csr, X)"},
+         clk.summary(), "cusparse SpMM (CSR)", {"rel_diff_vs_ours": err})
+    smax.close()
+    del A, X, Y, Y2, X2
+    torch.cuda.empty_cache()
+
+    # SpGEMM C = A*A, 7-point 96^3
+    rp, col, val = M.laplace3d_7pt(96)
+    n, nnz = len(rp) - 1, len(col)
+    A = csr(rp, col, val, n)
+    smax, k = b.kernel(KernelType.SPGEMM, np.float64)
+    k.register_A(n, n, nnz, col, rp, val)
+    k.register_B(n, n, nnz, col, rp, val)
+    k.register_C()
+    k.set_stream(b.stream.cuda_stream)
+    k.initialize()
+    k.apply()
+    k.finalize()
+    nnz_c = int(k.result()[2])
+    a_bytes = 12 * nnz + 4 * (n + 1)
+    nbytes = 4 * a_bytes + 12 * nnz_c + 4 * (n + 1)
+    with b.clocks() as clk:
+        t_lib, reps = b.time(lambda: torch.mm(A, A), budget_s=2.0, max_reps=100)
+        t_ours, _ = b.time(k.apply, budget_s=2.0, max_reps=100)
+    C = torch.mm(A, A)
+    line("cusparse_spgemm_f64_laplace3d_96", "SpGEMM", nbytes, t_lib, t_ours, reps,
+         {"n_rows": n, "nnz_a": nnz, "nnz_c": nnz_c, "library_call": "torch.mm(sparse_csr, sparse_csr)"},
+         clk.summary(), "cusparse SpGEMM", {"library_nnz_c": int(C._nnz())})
+    smax.close()
+    del A, C
+    torch.cuda.empty_cache()
+
+    # BSR 4x4 SpMV of the 7-point 64^3 Laplacian (the reference's harness uses
+    # square blocks only)
+    rp, col, val = M.laplace3d_7pt(64)
+    n, nnz = len(rp) - 1, len(col)
+    smax, k = b.kernel(KernelType.SPMV, np.float64, lambda k: k.set_mat_bcrs(True))
+    bc = smax.utils.convert_crs_to_bcrs(n, n, nnz, col, rp, val, 4, 4, 4, 4, False)
+    xd, yd, y2 = b.dev(M.uniform_vector(n, 100)), b.zeros(n, np.float64), b.zeros(n, np.float64)
+    k.register_A(bc["n_rows"], bc["n_cols"], bc["n_blocks"], 4, 4, 4, 4, bc["col"], bc["row_ptr"], bc["val"])
+    k.register_B(n, xd)
+    k.register_C(n, y2)
+    k.set_stream(b.stream.cuda_stream)
+    k.initialize()
+    nb = bc["n_blocks"]
+    try:
+        Ab = torch.sparse_bsr_tensor(b.dev(bc["row_ptr"]), b.dev(bc["col"]), b.dev(bc["val"]).view(nb, 4, 4),
+                                     size=(n, n))
+        with b.clocks() as clk:
+            t_lib, reps = b.time(lambda: torch.mv(Ab, xd, out=yd))
+            t_ours, _ = b.time(k.apply)
+        err = float(torch.linalg.norm(yd - y2) / torch.linalg.norm(y2))
+        line("cusparse_bsr4x4_spmv_f64_laplace3d_64", "BSR SpMV", (16 * 8 + 4) * nb + 4 * (n // 4 + 1) + 16 * n,
+             t_lib, t_ours, reps, {"n_rows": n, "n_blocks": nb, "library_call": "torch.mv(sparse_bsr, x)"},
+             clk.summary(), "cusparse bsrmv", {"rel_diff_vs_ours": err})
+    except RuntimeError as e:
+        log(f"[bench] BSR SpMV through torch.sparse unavailable: {e}")
+    smax.close()
+
+
 def run_extra(args):
     import torch
     torch.cuda.set_device(0)
@@ -725,6 +960,9 @@ def main():
     ap.add_argument("--extra-dtype", default="both", choices=("both", "f64", "f32"),
                     help="scs_spmv / spmm workloads: value types to run")
     ap.add_argument("--spmm-k", default="16,64", help="spmm workload: vector counts")
+    ap.add_argument("--solver-side", type=int, default=2048, help="solvers workload: grid side of the large case")
+    ap.add_argument("--solver-iters", type=int, default=200,
+                    help="solvers workload: Jacobi iterations of the large case (Gauss-Seidel: 1/20 of it)")
     args = ap.parse_args()
     globals()["N_ROWS"] = args.rows
     if args.impl == "reference":

@@ -336,6 +336,26 @@ smax_status smax_utils_apply_mat_perm(int int_type, int float_type, uint64_t n_r
 smax_status smax_utils_apply_vec_perm(int float_type, uint64_t n_rows, const void *vec, void *vec_perm,
                                       const int *perm);
 
+/* Matrix Market ingestion, as the reference's examples read matrices
+ * (COOMatrix::read_from_mtx without fast_matrix_market and
+ * CRSMatrix::convert_coo_to_crs, examples/matrix_structs.hpp:52-180, 338-387;
+ * examples/mmio.cpp): a coordinate file with real, integer or pattern values
+ * (pattern entries get 0.01) and general or symmetric storage (every
+ * off-diagonal entry of a symmetric file is followed by its mirror); entries
+ * stably sorted by row only, so each row keeps the file's order.  The text is
+ * parsed on the host (threads over line-aligned slices), the sort and the row
+ * pointer run on the GPU.  Outputs are new[] arrays (int32 row_ptr and col,
+ * values of float_type).  SMAX_ERR_UNSUPPORTED for other formats, BAD_ARG
+ * for malformed text, COL_OOB / BAD_ARG for indices outside the size line's
+ * dimensions. */
+smax_status smax_utils_read_mtx(const char *path, int float_type, uint64_t *n_rows, uint64_t *n_cols, uint64_t *nnz,
+                                void **row_ptr, void **col, void **val);
+/* COO (0-based int32 I, J; double values; host or device arrays) to CRS with
+ * the same stable by-row order (convert_coo_to_crs after sort_perm). */
+smax_status smax_utils_convert_coo_to_crs(int float_type, uint64_t n_rows, uint64_t n_cols, uint64_t nnz,
+                                          const int *I, const int *J, const double *val, void **row_ptr,
+                                          void **col, void **val_out);
+
 /* Releases an array returned by an smax_utils_* function. */
 void smax_free_host(void *p);
 

@@ -290,6 +290,61 @@ class Oracle:
         getattr(self.lib, f"orc_apply_vec_perm_{_sfx(vec.dtype)}")(len(perm), _p(vec), _p(out), _p(_i32(perm)))
         return out
 
+    # -- Matrix Market ingestion (examples/matrix_structs.hpp) -----------------
+    @staticmethod
+    def read_mtx(path):
+        """COOMatrix::read_from_mtx without fast_matrix_market
+        (examples/matrix_structs.hpp:52-180, mmio.cpp:56-163, mmio.hpp:127-214)
+        and convert_coo_to_crs (:338-387): banner checks, '%' comment lines,
+        the size line, entries in file order (pattern values 0.01), symmetric
+        mirrors right after each off-diagonal entry, a stable sort by row and
+        the row pointer by counting.  Returns (n_rows, n_cols, nnz, row_ptr,
+        col, val); raises ValueError where the reference reports an error."""
+        with open(path, "r") as f:
+            text = f.read()
+        lines = text.split("\n")
+        tok = lines[0].split()
+        if len(tok) < 5 or not tok[0].startswith("%%MatrixMarket"):
+            raise ValueError("banner")
+        obj, fmt, data, sym = (t.lower() for t in tok[1:5])
+        if obj != "matrix" or fmt != "coordinate" or data not in ("real", "integer", "pattern") or \
+                sym not in ("general", "symmetric"):
+            raise ValueError("unsupported")
+        i = 1
+        while True:
+            if i >= len(lines):
+                raise ValueError("premature end of file")
+            ln = lines[i]
+            i += 1
+            if ln.startswith("%"):
+                continue
+            parts = ln.split()
+            if len(parts) >= 3:
+                M, N, nz = (int(p) for p in parts[:3])
+                break
+            if parts:
+                raise ValueError("size line")
+        rest = " ".join(lines[i:]).split()
+        step = 2 if data == "pattern" else 3
+        if len(rest) < step * nz:
+            raise ValueError("premature end of file")
+        I, J, V = [], [], []
+        for e in range(nz):
+            r, c = int(rest[step * e]) - 1, int(rest[step * e + 1]) - 1
+            v = 0.01 if data == "pattern" else float(rest[step * e + 2])
+            I.append(r)
+            J.append(c)
+            V.append(v)
+            if sym == "symmetric" and r != c:
+                I.append(c)
+                J.append(r)
+                V.append(v)
+        I = np.array(I, dtype=np.int64)
+        order = np.argsort(I, kind="stable")
+        row_ptr = np.zeros(M + 1, dtype=np.int32)
+        np.cumsum(np.bincount(I, minlength=M)[:M], out=row_ptr[1:])
+        return (M, N, len(I), row_ptr, np.array(J, dtype=np.int32)[order], np.array(V, dtype=np.float64)[order])
+
     # -- the solver applications (examples/applications) --------------------
     @staticmethod
     def infty_norm(v):
@@ -454,6 +509,8 @@ class Reference:
         L.ref_time_generate_perm.restype = C.c_double
         L.ref_apply_mat_perm.argtypes = [_INT, _INT, _P, _P, _P, _P, _P, _P, _P, _P]
         L.ref_apply_vec_perm.argtypes = [_INT, _INT, _P, _P, _P]
+        L.ref_read_mtx.argtypes = [C.c_char_p, C.POINTER(_U64), C.POINTER(_U64), C.POINTER(_U64),
+                                   C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]
         for name in ("ref_jacobi", "ref_gauss_seidel"):
             f = getattr(L, name)
             f.argtypes = [_U64, _U64, _P, _P, _P, _P, _P, C.c_double, _INT, _INT, C.POINTER(_INT),
@@ -477,6 +534,17 @@ class Reference:
         if t < 0:
             self._check(-1)
         return x, it.value, norm.value, hist[: min(nch.value, cap)], t
+
+    def read_mtx(self, path):
+        """The examples' reader + convert_coo_to_crs (ref_read_mtx):
+        (n_rows, n_cols, nnz, row_ptr, col, val)."""
+        nr, nc, nz = _U64(0), _U64(0), _U64(0)
+        rp, col, val = _P(), _P(), _P()
+        self._check(self.lib.ref_read_mtx(os.fsencode(path), C.byref(nr), C.byref(nc), C.byref(nz), C.byref(rp),
+                                          C.byref(col), C.byref(val)))
+        n, z = nr.value, nz.value
+        return (n, nc.value, z, self._take_int(rp.value, n + 1), self._take_int(col.value, z),
+                self._take_val(val.value, z, np.float64))
 
     def jacobi_app(self, row_ptr, col, val, b, x_init, tol=1e-8, max_iters=1000, check_length=5):
         """The Jacobi program's loop through the reference's kernels (ref_jacobi):

@@ -19,6 +19,9 @@
 
 #include "interface.cpp"
 #include "error_handler.cpp"
+// the examples' Matrix Market reader and COO/CRS structs (examples/)
+#include "mmio.cpp"
+#include "matrix_structs.hpp"
 
 #include <chrono>
 #include <cmath>
@@ -744,6 +747,30 @@ double ref_gauss_seidel(uint64_t n, uint64_t nnz, const int *col, const int *row
         return 0;
     });
     return rc == 0 ? t : -1.0;
+}
+
+// ------------------------------------------------------ Matrix Market reader --
+// The examples' reader, COOMatrix::read_from_mtx without fast_matrix_market
+// (examples/matrix_structs.hpp:52-180), then CRSMatrix::convert_coo_to_crs
+// (:338-387), FP64.  The arrays are new[] (ref_free_int / ref_free_val).
+int ref_read_mtx(const char *path, uint64_t *n_rows, uint64_t *n_cols, uint64_t *nnz, int **row_ptr, int **col,
+                 double **val) {
+    return guarded([&] {
+        COOMatrix coo;
+        coo.read_from_mtx(path);
+        CRSMatrix<int, double> crs;
+        crs.convert_coo_to_crs(&coo);
+        *n_rows = crs.n_rows;
+        *n_cols = crs.n_cols;
+        *nnz = crs.nnz;
+        *row_ptr = crs.row_ptr;
+        *col = crs.col;
+        *val = crs.val;
+        crs.row_ptr = nullptr;
+        crs.col = nullptr;
+        crs.val = nullptr;
+        return 0;
+    });
 }
 
 } // extern "C"

@@ -67,6 +67,8 @@ SIGNATURES = {
     "smax_utils_generate_perm": (I32, [P, I32, U64, P, P, P, P, C.c_char_p]),
     "smax_utils_apply_mat_perm": (I32, [I32, I32, U64, P, P, P, P, P, P, P, P]),
     "smax_utils_apply_vec_perm": (I32, [I32, U64, P, P, P]),
+    "smax_utils_read_mtx": (I32, [C.c_char_p, I32, PU64, PU64, PU64, PP, PP, PP]),
+    "smax_utils_convert_coo_to_crs": (I32, [I32, U64, U64, U64, P, P, P, PP, PP, PP]),
     "smax_free_host": (None, [P]),
     "smax_spmv_crs_noalloc": (I32, [I32, U64, U64, U64, P, P, P, P, P, P]),
     "smax_solver_create": (I32, [PP, I32, I32, U64, U64, P, P, P]),

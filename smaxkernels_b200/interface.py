@@ -21,6 +21,7 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
+import os
 
 import numpy as np
 
@@ -462,6 +463,28 @@ class Utils:
 
 
     # -- level sets and permutations (src/utils/permutations.hpp) --------------
+    def read_mtx(self, path: str, dtype=np.float64):
+        """A Matrix Market file as CRS (n_rows, n_cols, nnz, row_ptr, col, val),
+        read as the reference's examples read it (smax_utils_read_mtx)."""
+        nr, nc, nz = C.c_uint64(0), C.c_uint64(0), C.c_uint64(0)
+        ptrs = [C.c_void_p() for _ in range(3)]
+        check(lib.smax_utils_read_mtx(os.fsencode(path), _ftype(np.dtype(dtype)), C.byref(nr), C.byref(nc),
+                                      C.byref(nz), *[C.byref(p) for p in ptrs]))
+        n, m, z = nr.value, nc.value, nz.value
+        return (n, m, z, _take(ptrs[0].value, n + 1, np.int32), _take(ptrs[1].value, z, np.int32),
+                _take(ptrs[2].value, z, np.dtype(dtype)))
+
+    def convert_coo_to_crs(self, n_rows, n_cols, I, J, val, dtype=np.float64):
+        """COO (0-based) to CRS, entries stably sorted by row (file order kept
+        within a row): (row_ptr, col, val)."""
+        I, J = _i32(I), _i32(J)
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        ptrs = [C.c_void_p() for _ in range(3)]
+        check(lib.smax_utils_convert_coo_to_crs(_ftype(np.dtype(dtype)), int(n_rows), int(n_cols), len(I), _ptr(I),
+                                                _ptr(J), _ptr(val), *[C.byref(p) for p in ptrs]))
+        return (_take(ptrs[0].value, int(n_rows) + 1, np.int32), _take(ptrs[1].value, len(I), np.int32),
+                _take(ptrs[2].value, len(I), np.dtype(dtype)))
+
     def build_symmetric_crs(self, row_ptr, col, n_rows):
         """Pattern of A + A^T: returns (sym_row_ptr, sym_col, sym_nnz)."""
         row_ptr, col = _i32(row_ptr), _i32(col)

@@ -2,10 +2,13 @@
 restatement of the reference's solver programs and against those programs'
 printed output (tests/golden/solver_apps.json).
 
-Tolerances: iteration counts are equal; residual histories agree with the
-oracle to 1e-9 relative (the GPU sums rows in another order, so rounding
-differs in the last bits and grows through the iterations); solutions agree
-to 1e-12 normwise relative (FP64), 1e-4 (FP32).
+Tolerances: iteration counts are equal; solutions agree to 1e-12 normwise
+relative (FP64), 1e-4 (FP32).  The GPU sums rows in another order, so x
+differs from the oracle's in the last bits; a residual |b - A x| near the
+tolerance is a difference of nearly equal numbers and carries that rounding
+at ~1e-15 absolute.  Residuals are therefore compared to 1e-9 relative plus
+1e-12 of the first residual, and to the programs' printed digits within their
+rounding ("%f": 5e-7 absolute; "%g": 1e-5 relative).
 """
 import json
 import os
@@ -48,6 +51,11 @@ def app_problem(kind, nx=10, gpu_perm=True):
     return rp, col, val, np.ones(n), np.zeros(n), None
 
 
+def check_hist(h, ho):
+    assert len(h) == len(ho)
+    np.testing.assert_allclose(h, ho, rtol=1e-9, atol=1e-12 * max(float(ho[0]), 1e-300))
+
+
 def oracle_run(kind, *a, **kw):
     return (O.jacobi_app if kind == "jacobi" else O.gauss_seidel_app)(*a, **kw)
 
@@ -64,12 +72,12 @@ def test_the_programs_problem(kind, mode):
         st = s.solve(b, x, tol=g["tol"], max_iters=g["max_iters"], check_length=g["check_length"], mode=mode)
         hist = s.history()
     assert st["n_iters"] == g["converged_after"] and st["converged"] == 1
-    assert ["%f" % h for h in hist] == g["residuals"]
-    assert "%g" % st["residual_norm"] == g["final_residual"]
+    np.testing.assert_allclose(hist, [float(r) for r in g["residuals"]], rtol=0, atol=5e-7 + 1e-12)
+    assert abs(st["residual_norm"] / float(g["final_residual"]) - 1.0) <= 1e-5
     assert st["n_checks"] == len(g["residuals"])
     xo, n_o, norm_o, hist_o = oracle_run(kind, rp, col, val, b, x0)
     assert rel(x, xo) <= 1e-12
-    np.testing.assert_allclose(hist, hist_o, rtol=1e-9, atol=0)
+    check_hist(hist, hist_o)
     if mode == "device_loop":
         assert st["host_waits"] == 1
 
@@ -93,7 +101,7 @@ def test_loop_shapes_against_the_oracle(kind, nx, max_iters, check_length, tol):
             st = s.solve(b, x, tol=tol, max_iters=max_iters, check_length=check_length, mode=mode)
             assert st["n_iters"] == n_o, mode
             assert st["n_checks"] == len(hist_o)
-            np.testing.assert_allclose(s.history(), hist_o, rtol=1e-9, atol=1e-300)
+            check_hist(s.history(), hist_o)
             assert rel(x, xo) <= 1e-12, mode
             results.append(x)
     # every driver issues the same launches: identical results
@@ -161,7 +169,7 @@ def test_larger_grid_fixed_iterations(kind):
     x = x0.copy()
     with Solver(kind, rp, col, val) as s:
         st = s.solve(b, x, tol=0.0, max_iters=50, check_length=10)
-        np.testing.assert_allclose(s.history(), hist_o, rtol=1e-9)
+        check_hist(s.history(), hist_o)
     assert st["n_iters"] == 50 and st["converged"] == 0
     assert rel(x, xo) <= 1e-12
 
