@@ -204,7 +204,7 @@ def config_dict(nnz, vbytes, world):
 # line per case, same keys as the headline line.  Single GPU.
 # ---------------------------------------------------------------------------
 EXTRA_WORKLOADS = ("spmv_laplace64", "scs_spmv", "bcrs_spmv", "spmm", "spgemm", "sptrsv", "sptrsv_batch",
-                   "sptrsv_refine", "adjoint", "solvers", "cusparse")
+                   "sptrsv_refine", "adjoint", "solvers", "cusparse", "mtx", "colour")
 
 
 class Bench:
@@ -763,9 +763,21 @@ def wl_solvers(b: Bench):
                graph_blocks_ms=round(res["graph_blocks"][0] * 1e3, 4), plain_ms=round(res["plain"][0] * 1e3, 4))
 
     side = b.args.solver_side
-    for kind in ("jacobi", "gauss_seidel"):
-        iters = b.args.solver_iters if kind == "jacobi" else max(2, b.args.solver_iters // 20)
-        rp, col, val, rhs, _ = problem(kind, side)
+    for kind in ("jacobi", "gauss_seidel", "gauss_seidel_pc"):
+        iters = b.args.solver_iters if kind != "gauss_seidel" else max(2, b.args.solver_iters // 20)
+        if kind == "gauss_seidel_pc":
+            # multicolour Gauss-Seidel: the matrix in PC colour order, so the
+            # D+L solve has one level per colour
+            rp0, col0, val0, _, _ = problem("gauss_seidel", side)
+            n0 = len(rp0) - 1
+            smax = Interface()
+            perm, inv = np.zeros(n0, np.int32), np.zeros(n0, np.int32)
+            smax.utils.generate_perm(n0, rp0, col0, perm, inv, "PC")
+            rp, col, val = np.zeros(n0 + 1, np.int32), np.zeros(len(col0), np.int32), np.zeros(len(col0))
+            smax.utils.apply_mat_perm(n0, rp0, col0, val0, rp, col, val, perm, inv)
+            smax.close()
+        else:
+            rp, col, val, rhs, _ = problem(kind, side)
         n, nnz = len(rp) - 1, len(col)
         row_of = np.repeat(np.arange(n), np.diff(rp))
         nnz_l = int((col <= row_of).sum())
@@ -775,14 +787,15 @@ def wl_solvers(b: Bench):
         bd, x0d = b.dev(rhs), b.zeros(n, np.float64)
         xd = x0d.clone()
         cl = 5
-        with Solver(kind, rp, col, val) as s:
+        skind = "jacobi" if kind == "jacobi" else "gauss_seidel"
+        with Solver(skind, rp, col, val) as s:
             def run():
                 xd.copy_(x0d)
                 s.solve(bd, xd, tol=0.0, max_iters=iters, check_length=cl, stream=st_ptr)
             with b.clocks() as clk:
                 t, reps = b.time(run, budget_s=3.0, max_reps=20)
         t_it = t / iters
-        nbytes = _solver_iter_bytes(kind, n, nnz, nnz_u, nnz_l, 8, cl)
+        nbytes = _solver_iter_bytes(skind, n, nnz, nnz_u, nnz_l, 8, cl)
         cpu = None
         if b.ref is not None:
             fn = b.ref.jacobi_app if kind == "jacobi" else b.ref.gauss_seidel_app
@@ -926,6 +939,94 @@ def wl_cusparse(b: Bench):
     except RuntimeError as e:
         log(f"[bench] BSR SpMV through torch.sparse unavailable: {e}")
     smax.close()
+
+
+def wl_mtx(b: Bench):
+    """Matrix Market ingestion: the 7-point 64^3 Laplacian written as a
+    coordinate file with its entries in scrambled order (1.8 M entries, full
+    17-digit values), read back as CRS by this platform (threads parse
+    line-aligned slices, the GPU sorts) and by the reference's own reader
+    (examples/matrix_structs.hpp, fscanf) on the host."""
+    import tempfile
+    import time as _time
+    from smaxkernels_b200 import Interface
+    from smaxkernels_b200 import matrices as M
+    rp, col, val = M.laplace3d_7pt(64)
+    n, nnz = len(rp) - 1, len(col)
+    row_of = np.repeat(np.arange(n), np.diff(rp))
+    order = np.random.default_rng(7).permutation(nnz)
+    vals = np.random.default_rng(8).uniform(-1, 1, nnz)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "laplace3d_64.mtx")
+        with open(path, "w") as f:
+            f.write("%%MatrixMarket matrix coordinate real general\n")
+            f.write(f"{n} {n} {nnz}\n")
+            np.savetxt(f, np.column_stack([row_of[order] + 1, col[order] + 1, vals[order]]),
+                       fmt=["%d", "%d", "%.17g"])
+        size = os.path.getsize(path)
+        smax = Interface()
+        smax.utils.read_mtx(path)  # warm-up (CUDA context, allocator)
+        ts = []
+        for _ in range(5):
+            t0 = _time.perf_counter()
+            got = smax.utils.read_mtx(path)
+            ts.append(_time.perf_counter() - t0)
+        t = float(np.median(ts))
+        cpu = None
+        if b.ref is not None:
+            t0 = _time.perf_counter()
+            ref = b.ref.read_mtx(path)
+            tc = _time.perf_counter() - t0
+            assert np.array_equal(ref[4], got[4]) and np.array_equal(ref[5], got[5])
+            cpu = {"value": round(size / tc / 1e6, 3), "unit": "MB/s", "cores": 1, "kind": "reference",
+                   "sample": "one read of the same file by the reference's reader (fscanf, one thread)",
+                   "seconds": round(tc, 3)}
+        b.emit("mtx_read_laplace3d_64", "Matrix Market ingestion MB/s (text bytes, wall clock)", size / t / 1e6,
+               "MB/s", t, 5, "f64", {"n_rows": n, "nnz": nnz, "file_bytes": size, "parse_threads": os.cpu_count()},
+               None, None, cpu, entries_per_s=round(nnz / t, 1))
+        smax.close()
+
+
+def wl_colour(b: Bench):
+    """generate_perm with the colourings SC, PC and PC_BAL on the GPU: the
+    5-point 2048^2 Laplacian (4.2 M rows, 2 colours) and the irregular
+    lognormal 2^20 matrix; wall clock per call (host arrays in and out), next
+    to the reference's generate_perm on one OpenMP thread (the setting in
+    which its colourings are deterministic; the GPU result equals it)."""
+    import time as _time
+    from smaxkernels_b200 import Interface
+    from smaxkernels_b200 import matrices as M
+    cases = (("laplace2d_2048", lambda: M.laplace2d_5pt(2048)),
+             ("lognormal_1048576", lambda: M.lognormal_random(1 << 20, seed=1)))
+    for name, make in cases:
+        rp, col, _ = make()
+        n, nnz = len(rp) - 1, len(col)
+        for t in ("SC", "PC", "PC_BAL"):
+            smax = Interface()
+            perm, inv = np.zeros(n, np.int32), np.zeros(n, np.int32)
+            smax.utils.generate_perm(n, rp, col, perm, inv, t)  # warm-up
+            ts = []
+            for _ in range(3):
+                t0 = _time.perf_counter()
+                smax.utils.generate_perm(n, rp, col, perm, inv, t)
+                ts.append(_time.perf_counter() - t0)
+            n_col = smax.get_n_levels()
+            smax.close()
+            tg = float(np.median(ts))
+            cpu = None
+            if b.ref is not None:
+                b.ref.set_threads(1)
+                t0 = _time.perf_counter()
+                rperm, _, rlvl = b.ref.generate_perm(rp, col, t)
+                tc = _time.perf_counter() - t0
+                b.ref.set_threads(os.cpu_count() or 1)
+                same = bool(np.array_equal(rperm, perm) and len(rlvl) == n_col + 1)
+                cpu = {"value": round(tc * 1e3, 3), "unit": "ms", "cores": 1, "kind": "reference",
+                       "sample": "one generate_perm call of the reference on one OpenMP thread",
+                       "identical_permutation": same}
+            b.emit(f"colour_{t.lower()}_{name}", "generate_perm time (wall clock, host arrays)", tg * 1e3, "ms", tg,
+                   3, "int32", {"n_rows": n, "nnz": nnz, "type": t}, None, None, cpu, higher=False,
+                   n_colours=n_col)
 
 
 def run_extra(args):

@@ -315,14 +315,23 @@ smax_status smax_utils_convert_crs_to_bcrs(int int_type, int float_type, uint64_
 smax_status smax_utils_build_symmetric_crs(int int_type, uint64_t n_rows, const void *row_ptr, const void *col,
                                            void **sym_row_ptr, void **sym_col, uint64_t *sym_nnz);
 
-/* Utils::generate_perm (src/utils/permutations.hpp:485-584) for types "BFS"
- * (the default of the reference; queue order of its one-thread BFS), "RS"
- * (rows stably sorted by level) and "NONE"; computed on the GPU.  perm and
+/* Utils::generate_perm (src/utils/permutations.hpp:485-584) for every type
+ * of the reference, computed on the GPU: "BFS" (the default; queue order of
+ * its one-thread BFS), "RS" (rows stably sorted by level), the colourings
+ * "SC", "PC" and "PC_BAL" (rows stably sorted by colour, one level per
+ * colour; the results the reference gives with one OpenMP thread, whose
+ * colourings otherwise depend on thread timing) and "NONE".  perm and
  * inv_perm are caller arrays of n_rows ints; the level pointer is stored in
- * ctx (smax_ctx_get_n_levels / smax_ctx_get_level_ptr_at).  The colourings
- * "SC", "PC", "PC_BAL" return SMAX_ERR_UNSUPPORTED. */
+ * ctx (smax_ctx_get_n_levels / smax_ctx_get_level_ptr_at). */
 smax_status smax_utils_generate_perm(smax_ctx ctx, int int_type, uint64_t n_rows, const void *row_ptr,
                                      const void *col, int *perm, int *inv_perm, const char *type);
+
+/* Utils::sanity_check_perm (src/utils/permutations.hpp:794-818): *valid = 1
+ * when no row shares a colour other than 0 with a lower neighbour of the CRS
+ * pattern (colors: n_rows ints, host); else 0 and *first_bad_row (may be
+ * NULL) = the lowest such row. */
+smax_status smax_utils_sanity_check_perm(int int_type, uint64_t n_rows, const void *row_ptr, const void *col,
+                                         const int *colors, int *valid, int64_t *first_bad_row);
 
 /* Utils::apply_mat_perm (src/utils/permutations.hpp:820-861): row r of the
  * result is row perm[r], columns mapped through inv_perm; output arrays are the

@@ -275,6 +275,111 @@ class Oracle:
             raise ValueError("generate_perm")
         return perm, inv, lvl_ptr[: nl + 1].copy()
 
+    # -- colourings (one OpenMP thread's results) ------------------------------
+    @staticmethod
+    def colour_sc(srp, scol):
+        """generate_color_perm (src/utils/permutations.hpp:588-647) with one
+        thread, on the symmetric pattern: (n_colours, colour[n])."""
+        from collections import deque
+        n = len(srp) - 1
+        srp, scol = list(map(int, srp)), list(map(int, scol))
+        color = [-2] * n
+        usable = [-1] * n
+        q = deque()
+        for s_ in range(n):
+            if all(scol[j] >= s_ for j in range(srp[s_], srp[s_ + 1])):
+                q.append(s_)
+                color[s_] = -1
+        max_color = 0
+        while q:
+            u = q.popleft()
+            for j in range(srp[u], srp[u + 1]):
+                v = scol[j]
+                if color[v] == -2:
+                    color[v] = -1
+                    q.append(v)
+                elif color[v] >= 0:
+                    usable[color[v]] = u
+            for c in range(n):
+                if usable[c] != u:
+                    color[u] = c
+                    max_color = max(max_color, c)
+                    break
+        return max_color + 1, np.array(color, dtype=np.int32)
+
+    @staticmethod
+    def colour_pc(srp, scol):
+        """generate_color_perm_par (:649-714) with one thread: rows in order,
+        each the smallest colour its neighbours do not hold (unset = -1)."""
+        n = len(srp) - 1
+        srp, scol = list(map(int, srp)), list(map(int, scol))
+        colors = [-1] * n
+        max_color = 0
+        for row in range(n):
+            forbidden = {colors[scol[j]] for j in range(srp[row], srp[row + 1])}
+            spec = 0
+            while spec in forbidden:
+                spec += 1
+            colors[row] = spec
+            max_color = max(max_color, spec)
+        return max_color + 1, np.array(colors, dtype=np.int32)
+
+    @staticmethod
+    def colour_balance(srp, scol, colors, num_colors):
+        """generate_color_perm_bal (:716-792) with one thread, in place on a PC
+        colouring.  The reference's search reads color_size past num_colors
+        when every colour is ruled out; it then never moves the row, which is
+        what stopping the search at num_colors gives."""
+        n = len(srp) - 1
+        srp, scol = list(map(int, srp)), list(map(int, scol))
+        colors = [int(c) for c in colors]
+        b = float(n // num_colors)
+        size = [0] * num_colors
+        for c in colors:
+            size[c] += 1
+        for row in range(n):
+            if size[colors[row]] <= b:
+                continue
+            forbidden = {colors[scol[j]] for j in range(srp[row], srp[row + 1])}
+            spec = 0
+            while spec < num_colors and (spec in forbidden or size[spec] >= b):
+                spec += 1
+            if spec >= num_colors:
+                continue
+            size[colors[row]] -= 1
+            colors[row] = spec
+            size[spec] += 1
+        return num_colors, np.array(colors, dtype=np.int32)
+
+    @staticmethod
+    def colours_valid(row_ptr, col, colors):
+        """sanity_check_perm (:794-818)."""
+        n = len(row_ptr) - 1
+        for r in range(n):
+            for j in range(int(row_ptr[r]), int(row_ptr[r + 1])):
+                c = int(col[j])
+                if c < r and colors[r] == colors[c] and colors[r] != 0:
+                    return False
+        return True
+
+    def colour_perm(self, row_ptr, col, type_):
+        """generate_perm for "SC", "PC", "PC_BAL": (perm, inv_perm, lvl_ptr,
+        colour) -- the identity stably sorted by colour, one level per colour."""
+        srp, scol = self.build_symmetric(row_ptr, col)
+        if type_ == "SC":
+            nc, colour = self.colour_sc(srp, scol)
+        else:
+            nc, colour = self.colour_pc(srp, scol)
+            if type_ == "PC_BAL":
+                nc, colour = self.colour_balance(srp, scol, colour, nc)
+        n = len(colour)
+        perm = np.argsort(colour, kind="stable").astype(np.int32)
+        inv = np.zeros(n, dtype=np.int32)
+        inv[perm] = np.arange(n, dtype=np.int32)
+        lvl_ptr = np.zeros(nc + 1, dtype=np.int32)
+        np.cumsum(np.bincount(colour, minlength=nc)[:nc], out=lvl_ptr[1:])
+        return perm, inv, lvl_ptr, colour
+
     def apply_mat_perm(self, row_ptr, col, val, perm, inv_perm):
         rp = _i32(row_ptr)
         n = len(rp) - 1

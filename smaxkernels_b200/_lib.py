@@ -65,6 +65,7 @@ SIGNATURES = {
                                        + [PP] * 3),
     "smax_utils_build_symmetric_crs": (I32, [I32, U64, P, P, PP, PP, PU64]),
     "smax_utils_generate_perm": (I32, [P, I32, U64, P, P, P, P, C.c_char_p]),
+    "smax_utils_sanity_check_perm": (I32, [I32, U64, P, P, P, C.POINTER(I32), C.POINTER(C.c_int64)]),
     "smax_utils_apply_mat_perm": (I32, [I32, I32, U64, P, P, P, P, P, P, P, P]),
     "smax_utils_apply_vec_perm": (I32, [I32, U64, P, P, P]),
     "smax_utils_read_mtx": (I32, [C.c_char_p, I32, PU64, PU64, PU64, PP, PP, PP]),

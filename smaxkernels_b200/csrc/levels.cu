@@ -96,15 +96,19 @@ __global__ void sym_fill(const int *__restrict__ rp, const int *__restrict__ col
 // the releases v receives in the sweep (duplicates counted on both sides)
 // With rev, edges run from higher to lower rows (levels of an upper
 // triangular dependency structure).
-__device__ __forceinline__ bool ahead(int v, int u, bool rev) { return rev ? v < u : v > u; }
+// With prio, "ahead" is a larger priority instead of a larger row index.
+__device__ __forceinline__ bool ahead(int v, int u, bool rev, const int *prio) {
+    if (prio) return prio[v] > prio[u];
+    return rev ? v < u : v > u;
+}
 
 __global__ void incoming_degree(const int *__restrict__ srp, const int *__restrict__ scol, int64_t n,
-                                int *__restrict__ deg, bool rev) {
+                                int *__restrict__ deg, bool rev, const int *__restrict__ prio) {
     const int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n) return;
     for (int j = srp[u]; j < srp[u + 1]; ++j) {
         const int v = scol[j];
-        if (ahead(v, (int)u, rev)) atomicAdd(deg + v, 1);
+        if (ahead(v, (int)u, rev, prio)) atomicAdd(deg + v, 1);
     }
 }
 
@@ -125,14 +129,15 @@ __global__ void roots_kernel(const int *__restrict__ deg, int64_t n, int *__rest
 // neighbours; the last release of a node puts it into the next frontier.
 __global__ void level_step(const int *__restrict__ srp, const int *__restrict__ scol, const int *__restrict__ cur,
                            const int *__restrict__ cur_count, int *__restrict__ nxt, int *__restrict__ nxt_count,
-                           int *__restrict__ deg, int *__restrict__ lvl, int level, bool rev) {
+                           int *__restrict__ deg, int *__restrict__ lvl, int level, bool rev,
+                           const int *__restrict__ prio) {
     const int cnt = *cur_count;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += stride) {
         const int u = cur[i];
         for (int j = srp[u]; j < srp[u + 1]; ++j) {
             const int v = scol[j];
-            if (ahead(v, u, rev) && atomicSub(deg + v, 1) == 1) {
+            if (ahead(v, u, rev, prio) && atomicSub(deg + v, 1) == 1) {
                 lvl[v] = level + 1;
                 nxt[atomicAdd(nxt_count, 1)] = v;
             }
@@ -148,7 +153,7 @@ __global__ void __launch_bounds__(kSmallThreads) level_sweep_small(const int *__
                                                                    int *__restrict__ frontier,
                                                                    int *__restrict__ count, int *__restrict__ deg,
                                                                    int *__restrict__ lvl, int *__restrict__ level_io,
-                                                                   bool rev) {
+                                                                   bool rev, const int *__restrict__ prio) {
     __shared__ int buf[2][kSmallCap];
     __shared__ int cnt[2];
     __shared__ int overflow;
@@ -168,7 +173,7 @@ __global__ void __launch_bounds__(kSmallThreads) level_sweep_small(const int *__
             const int u = buf[cur][i];
             for (int j = srp[u]; j < srp[u + 1]; ++j) {
                 const int v = scol[j];
-                if (ahead(v, u, rev) && atomicSub(deg + v, 1) == 1) {
+                if (ahead(v, u, rev, prio) && atomicSub(deg + v, 1) == 1) {
                     lvl[v] = level + 1;
                     const int p = atomicAdd(&cnt[cur ^ 1], 1);
                     if (p < kSmallCap) buf[cur ^ 1][p] = v;
@@ -214,12 +219,19 @@ __global__ void inverse_kernel(const int *__restrict__ perm, int64_t n, int *__r
 // of v in w*'s symmetric row).  pos[] holds the final positions of all nodes
 // of earlier levels; it is written by the same kernel, so it is read through
 // L2 (__ldcg), never through the non-coherent read-only path.
+// With First, w* is instead v's first-dequeued neighbour of any index among
+// the nodes placed before this level (pos < placed_end; unplaced nodes hold
+// INT_MAX): the queue order of a FIFO breadth-first search from a root set.
+template <bool First>
 __device__ __forceinline__ unsigned long long bfs_key(const int *__restrict__ srp, const int *__restrict__ scol,
-                                                      const int *pos, int v) {
-    int best = -1, wstar = -1;
+                                                      const int *pos, int v, int placed_end) {
+    int best = First ? 0x7fffffff : -1, wstar = -1;
     for (int j = srp[v]; j < srp[v + 1]; ++j) {
         const int w = scol[j];
-        if (w < v) {
+        if constexpr (First) {
+            const int p = __ldcg(pos + w);
+            if (p < placed_end && p < best) { best = p; wstar = w; }
+        } else if (w < v) {
             const int p = __ldcg(pos + w);
             if (p > best) { best = p; wstar = w; }
         }
@@ -233,6 +245,7 @@ __device__ __forceinline__ unsigned long long bfs_key(const int *__restrict__ sr
 
 // Small levels [l0, l1): one CTA; each level's nodes (contiguous in `order`,
 // the (level, row)-sorted nodes) are sorted by their BFS keys in shared memory.
+template <bool First>
 __global__ void __launch_bounds__(kSmallThreads) bfs_small_levels(const int *__restrict__ srp,
                                                                   const int *__restrict__ scol,
                                                                   const int *__restrict__ lvl_ptr,
@@ -251,7 +264,7 @@ __global__ void __launch_bounds__(kSmallThreads) bfs_small_levels(const int *__r
             const int e = threadIdx.x * IPT + i;  // blocked arrangement
             if (e < m) {
                 const int v = order[a + e];
-                keys[i] = bfs_key(srp, scol, pos, v);
+                keys[i] = bfs_key<First>(srp, scol, pos, v, a);
                 vals[i] = v;
             } else {
                 keys[i] = ~0ull;
@@ -271,13 +284,14 @@ __global__ void __launch_bounds__(kSmallThreads) bfs_small_levels(const int *__r
     }
 }
 
+template <bool First>
 __global__ void bfs_keys_level(const int *__restrict__ srp, const int *__restrict__ scol,
                                const int *__restrict__ order, int a, int m, const int *pos,
                                unsigned long long *__restrict__ keys, int *__restrict__ vals) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
     const int v = order[a + i];
-    keys[i] = bfs_key(srp, scol, pos, v);
+    keys[i] = bfs_key<First>(srp, scol, pos, v, a);
     vals[i] = v;
 }
 
@@ -396,13 +410,13 @@ void build_symmetric(const DevCRS &a, DevBuf &srp, DevBuf &scol, int64_t &sym_nn
     SMAX_CUDA(cudaStreamSynchronize(st));
 }
 
-int rs_levels(const int *srp, const int *scol, int64_t n, DevBuf &lvl, cudaStream_t st, bool rev) {
+int rs_levels(const int *srp, const int *scol, int64_t n, DevBuf &lvl, cudaStream_t st, bool rev, const int *prio) {
     lvl.alloc(sizeof(int) * (n ? n : 1));
     if (n == 0) return 1;  // the reference reports one level for an empty matrix
     DevBuf deg(sizeof(int) * n), fr0(sizeof(int) * n), fr1(sizeof(int) * n), cnts(sizeof(int) * 4);
     const unsigned g = ceil_div_u(n, 256);
     SMAX_CUDA(cudaMemsetAsync(deg.p, 0, sizeof(int) * n, st));
-    incoming_degree<<<g, 256, 0, st>>>(srp, scol, n, deg.as<int>(), rev);
+    incoming_degree<<<g, 256, 0, st>>>(srp, scol, n, deg.as<int>(), rev, prio);
     fill_int<<<g, 256, 0, st>>>(lvl.as<int>(), n, -1);
     SMAX_CUDA(cudaMemsetAsync(cnts.p, 0, sizeof(int) * 4, st));
     roots_kernel<<<g, 256, 0, st>>>(deg.as<int>(), n, fr0.as<int>(), cnts.as<int>(), lvl.as<int>());
@@ -421,7 +435,7 @@ int rs_levels(const int *srp, const int *scol, int64_t n, DevBuf &lvl, cudaStrea
         if (h[0] <= kSmallCap) {
             SMAX_CUDA(cudaMemcpyAsync(cnt + 2, &level, sizeof(int), cudaMemcpyHostToDevice, st));
             level_sweep_small<<<1, kSmallThreads, 0, st>>>(srp, scol, cur, ccur, deg.as<int>(), lvl.as<int>(),
-                                                           cnt + 2, rev);
+                                                           cnt + 2, rev, prio);
             SMAX_CUDA(cudaGetLastError());
             SMAX_CUDA(cudaMemcpyAsync(h, ccur, sizeof(int), cudaMemcpyDeviceToHost, st));
             SMAX_CUDA(cudaMemcpyAsync(h + 1, cnt + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -430,7 +444,7 @@ int rs_levels(const int *srp, const int *scol, int64_t n, DevBuf &lvl, cudaStrea
         } else {
             SMAX_CUDA(cudaMemsetAsync(cnxt, 0, sizeof(int), st));
             level_step<<<grid, 256, 0, st>>>(srp, scol, cur, ccur, nxt, cnxt, deg.as<int>(), lvl.as<int>(), level,
-                                             rev);
+                                             rev, prio);
             SMAX_CUDA(cudaGetLastError());
             std::swap(cur, nxt);
             std::swap(ccur, cnxt);
@@ -469,11 +483,15 @@ void level_order(const int *lvl, int64_t n, int n_levels, DevBuf &order, std::ve
 }
 
 void bfs_order(const int *srp, const int *scol, int64_t n, const std::vector<int> &lvl_ptr, const int *order,
-               DevBuf &perm, cudaStream_t st) {
+               DevBuf &perm, cudaStream_t st, bool first_discoverer) {
     perm.alloc(sizeof(int) * (n ? n : 1));
     if (n == 0) return;
     const int L = (int)lvl_ptr.size() - 1;
     DevBuf pos(sizeof(int) * n), dlp(sizeof(int) * (L + 1));
+    if (first_discoverer) {
+        fill_int<<<ceil_div_u(n, 256), 256, 0, st>>>(pos.as<int>(), n, 0x7fffffff);
+        SMAX_CUDA(cudaGetLastError());
+    }
     SMAX_CUDA(cudaMemcpyAsync(dlp.p, lvl_ptr.data(), sizeof(int) * (L + 1), cudaMemcpyHostToDevice, st));
     // level 0: the roots, queued in ascending order == (level, row) order
     const int m0 = lvl_ptr[1] - lvl_ptr[0];
@@ -487,8 +505,12 @@ void bfs_order(const int *srp, const int *scol, int64_t n, const std::vector<int
         if (lvl_ptr[l + 1] - lvl_ptr[l] <= kSmallCap) {
             int l1 = l;
             while (l1 < L && lvl_ptr[l1 + 1] - lvl_ptr[l1] <= kSmallCap) ++l1;
-            bfs_small_levels<<<1, kSmallThreads, 0, st>>>(srp, scol, dlp.as<int>(), order, l, l1, pos.as<int>(),
-                                                          perm.as<int>());
+            if (first_discoverer)
+                bfs_small_levels<true><<<1, kSmallThreads, 0, st>>>(srp, scol, dlp.as<int>(), order, l, l1,
+                                                                    pos.as<int>(), perm.as<int>());
+            else
+                bfs_small_levels<false><<<1, kSmallThreads, 0, st>>>(srp, scol, dlp.as<int>(), order, l, l1,
+                                                                     pos.as<int>(), perm.as<int>());
             SMAX_CUDA(cudaGetLastError());
             l = l1;
         } else {
@@ -497,8 +519,12 @@ void bfs_order(const int *srp, const int *scol, int64_t n, const std::vector<int
             kout.ensure(sizeof(unsigned long long) * m);
             vin.ensure(sizeof(int) * m);
             vout.ensure(sizeof(int) * m);
-            bfs_keys_level<<<ceil_div_u(m, 256), 256, 0, st>>>(srp, scol, order, a, m, pos.as<int>(),
-                                                               kin.as<unsigned long long>(), vin.as<int>());
+            if (first_discoverer)
+                bfs_keys_level<true><<<ceil_div_u(m, 256), 256, 0, st>>>(srp, scol, order, a, m, pos.as<int>(),
+                                                                         kin.as<unsigned long long>(), vin.as<int>());
+            else
+                bfs_keys_level<false><<<ceil_div_u(m, 256), 256, 0, st>>>(srp, scol, order, a, m, pos.as<int>(),
+                                                                          kin.as<unsigned long long>(), vin.as<int>());
             SMAX_CUDA(cudaGetLastError());
             size_t tb = 0;
             SMAX_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kin.as<unsigned long long>(),

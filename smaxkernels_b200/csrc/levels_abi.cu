@@ -74,9 +74,8 @@ smax_status smax_utils_generate_perm(smax_ctx ctx, int int_type, uint64_t n_rows
         if (int_type != SMAX_INT32) fail(SMAX_ERR_UNSUPPORTED_TYPE, "only int32 indices are supported");
         if (!ctx || !row_ptr || (n_rows && (!perm || !inv_perm)) || !type) fail(SMAX_ERR_BAD_ARG, "null argument");
         const std::string t(type);
-        if (t == "SC" || t == "PC" || t == "PC_BAL")
-            fail(SMAX_ERR_UNSUPPORTED, "colouring permutations (" + t + ") are not available on this platform");
-        if (t != "BFS" && t != "RS" && t != "NONE")
+        const bool colouring = t == "SC" || t == "PC" || t == "PC_BAL";
+        if (t != "BFS" && t != "RS" && t != "NONE" && !colouring)
             fail(SMAX_ERR_BAD_ARG, "Permutation type: " + t + " does not exist. Please choose a type in: BFS, RS, "
                                    "SC, PC, PC_BAL, NONE.");
         if (n_rows >= (1ull << 31)) fail(SMAX_ERR_UNSUPPORTED, "int32 indices cannot address this matrix");
@@ -97,7 +96,16 @@ smax_status smax_utils_generate_perm(smax_ctx ctx, int int_type, uint64_t n_rows
             DevBuf srp, scol, lvl, order;
             int64_t snnz = 0;
             build_symmetric(a, srp, scol, snnz, s.s);
-            const int nl = rs_levels(srp.as<int>(), scol.as<int>(), n, lvl, s.s);
+            int nl = 0;
+            if (t == "SC") {
+                nl = colour_sc(srp.as<int>(), scol.as<int>(), n, lvl, s.s);
+            } else if (colouring) {
+                nl = colour_pc(srp.as<int>(), scol.as<int>(), n, lvl, s.s);
+                if (t == "PC_BAL") nl = colour_balance(srp.as<int>(), scol.as<int>(), n, lvl, nl, s.s);
+            } else {
+                nl = rs_levels(srp.as<int>(), scol.as<int>(), n, lvl, s.s);
+            }
+            // every type but BFS: the identity stably sorted by level (colour)
             level_order(lvl.as<int>(), n, nl, order, lvl_ptr, s.s);
             if (n > 0 && lvl_ptr.back() != n) fail(SMAX_ERR_STATE, "level sweep did not reach every row");
             const int *p = order.as<int>();
@@ -113,6 +121,23 @@ smax_status smax_utils_generate_perm(smax_ctx ctx, int int_type, uint64_t n_rows
         ctx->lvl_ptr = std::move(lvl_ptr);
         ctx->n_levels = (int)ctx->lvl_ptr.size() - 1;
         ctx->levels_version++;
+    });
+}
+
+smax_status smax_utils_sanity_check_perm(int int_type, uint64_t n_rows, const void *row_ptr, const void *col,
+                                         const int *colors, int *valid, int64_t *first_bad_row) {
+    return guarded([&] {
+        if (int_type != SMAX_INT32) fail(SMAX_ERR_UNSUPPORTED_TYPE, "only int32 indices are supported");
+        if (!row_ptr || !valid || (n_rows && !colors)) fail(SMAX_ERR_BAD_ARG, "null argument");
+        const int64_t n = (int64_t)n_rows;
+        Stream s;
+        DevCRS a;
+        upload_pattern(a, n_rows, row_ptr, col, nullptr, 4, s.s);
+        DevBuf dc(sizeof(int) * (n ? n : 1));
+        if (n) SMAX_CUDA(cudaMemcpyAsync(dc.p, colors, sizeof(int) * n, cudaMemcpyHostToDevice, s.s));
+        int64_t bad = -1;
+        *valid = colours_valid(a.rp(), a.ci(), n, dc.as<int>(), &bad, s.s) ? 1 : 0;
+        if (first_bad_row) *first_bad_row = bad;
     });
 }
 

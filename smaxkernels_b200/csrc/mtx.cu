@@ -17,7 +17,7 @@
 //     row pointer by counting.
 // The text is parsed on the host by one thread per slice of the file (each
 // slice starts at a line boundary; the slices' entries are concatenated in
-// file order), numbers converted with strtol/strtod as fscanf's %d / %lg do.
+// file order); integers are read as %d reads them, values with strtod (%lg).
 // The sort, the gathers and the row pointer run on the GPU: a stable device
 // radix sort of (row, position) pairs.
 #include <cub/device/device_radix_sort.cuh>
@@ -201,45 +201,50 @@ Header parse_header(const std::string &s) {
     return h;
 }
 
-// Parses whitespace-separated entries of [b, e) (b at a line start); appends
-// per entry i-1, j-1 and the value.  Returns false on a malformed token.
+// Parses whitespace-separated entries of [p, end) (p at a line start, the
+// text NUL-terminated after its last byte); appends per entry i-1, j-1 and
+// the value.  Integers are read by hand (optional sign, decimal digits, as
+// %d); values by strtod in place (what %lg does).  Returns false on a
+// malformed token.
 bool parse_slice(const char *p, const char *end, bool pattern, std::vector<int> &I, std::vector<int> &J,
                  std::vector<double> &V) {
+    auto space = [](char c) { return c == ' ' || c == '\n' || c == '\t' || c == '\r' || c == '\v' || c == '\f'; };
     auto skip = [&] {
-        while (p < end && std::isspace((unsigned char)*p)) ++p;
+        while (p < end && space(*p)) ++p;
     };
-    std::string buf;
-    auto token = [&](const char *&t0, size_t &len) {
+    auto integer = [&](long long &out) {
         skip();
-        t0 = p;
-        while (p < end && !std::isspace((unsigned char)*p)) ++p;
-        len = (size_t)(p - t0);
-        if (len) buf.assign(t0, len);
-        return len > 0;
+        if (p >= end) return false;
+        bool neg = false;
+        if (*p == '+' || *p == '-') neg = *p++ == '-';
+        const char *d0 = p;
+        long long v = 0;
+        while (p < end && *p >= '0' && *p <= '9') {
+            v = v * 10 + (*p - '0');
+            if (v > (1ll << 40)) return false;
+            ++p;
+        }
+        if (p == d0 || (p < end && !space(*p))) return false;
+        out = neg ? -v : v;
+        return true;
     };
     while (true) {
-        const char *t;
-        size_t len;
-        if (!token(t, len)) return true;
-        long long vals[2];
-        for (int k = 0; k < 2; ++k) {
-            if (k == 1 && !token(t, len)) return false;
-            char *q = nullptr;
-            errno = 0;
-            vals[k] = std::strtoll(buf.c_str(), &q, 10);
-            if (q != buf.c_str() + len || errno) return false;
-        }
+        skip();
+        if (p >= end) return true;
+        long long r = 0, c = 0;
+        if (!integer(r) || !integer(c)) return false;
         double v = 0.01;
         if (!pattern) {
-            if (!token(t, len)) return false;
+            skip();
+            if (p >= end) return false;
             char *q = nullptr;
-            v = std::strtod(buf.c_str(), &q);
-            if (q != buf.c_str() + len) return false;
+            v = std::strtod(p, &q);
+            if (q == p || (q < end && !space(*q)) || q > end) return false;
+            p = q;
         }
-        if (vals[0] < -(1ll << 31) + 2 || vals[0] > (1ll << 31) || vals[1] < -(1ll << 31) + 2 || vals[1] > (1ll << 31))
-            return false;
-        I.push_back((int)(vals[0] - 1));
-        J.push_back((int)(vals[1] - 1));
+        if (r < -(1ll << 31) + 2 || r > (1ll << 31) || c < -(1ll << 31) + 2 || c > (1ll << 31)) return false;
+        I.push_back((int)(r - 1));
+        J.push_back((int)(c - 1));
         V.push_back(v);
     }
 }

@@ -21,9 +21,12 @@
 //    maximum and one atomicMax on the bit pattern (non-negative doubles order
 //    like their bits); a one-thread kernel records it, advances the iteration
 //    count and decides whether the loop goes on.
-// A row group is G lanes (a power of two >= the mean row length, at most 32)
-// that stride over the row's entries and add their partial sums with
-// shuffles inside the group's lane mask.
+// A row group is G lanes (1, 2, ..., 32) that stride over the row's entries
+// and add their partial sums with shuffles inside the group's lane mask.  G
+// is chosen per matrix when the solver is created: the residual kernel (the
+// same row loop) is timed for every G on the matrix itself and the fastest
+// kept; matrices below 2^20 entries take the smallest power of two >= half
+// the mean row length.
 #include <cub/device/device_scan.cuh>
 
 #include <cmath>
@@ -54,10 +57,10 @@ unsigned row_grid(int64_t n, int G) {
     return (unsigned)(g < 1 ? 1 : (g > cap ? cap : g));
 }
 
-int group_for(const DevCRS &m) {
+int group_guess(const DevCRS &m) {
     const double mean = m.n_rows ? (double)m.nnz / (double)m.n_rows : 1.0;
     int g = 1;
-    while (g < 32 && g < mean) g <<= 1;
+    while (g < 32 && 2 * g < mean) g <<= 1;
     return g;
 }
 
@@ -73,6 +76,7 @@ __device__ __forceinline__ VT row_dot(const int *__restrict__ rp, const int *__r
                                       unsigned mask) {
     VT s = VT(0);
     const int e = rp[r + 1];
+#pragma unroll 4
     for (int j = rp[r] + lane; j < e; j += G) s += val[j] * __ldg(x + ci[j]);
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(mask, s, o);
@@ -375,6 +379,55 @@ struct smax_solver_s {
         decide(tol, cl, limit, h, set, st);
     }
 
+    // the fastest row-group width for the row loop over m (the residual
+    // kernel, or with rhs the tmp = b - U x kernel), timed on m itself
+    template <typename VT> int tune_group(const DevCRS &m, bool rhs, cudaStream_t st) {
+        const int guess = group_guess(m);
+        if (m.nnz < (1 << 20)) return guess;
+        const int64_t nn = m.n_rows;
+        auto launch = [&](int g_) {
+            with_group(g_, [&](auto g) {
+                constexpr int G = decltype(g)::value;
+                if (rhs)
+                    rhs_kernel<VT, G><<<row_grid(nn, G), kRowThreads, 0, st>>>(m.rp(), m.ci(), m.val.as<VT>(),
+                                                                               x0.as<VT>(), b.as<VT>(), tmp.as<VT>(),
+                                                                               nn);
+                else
+                    residual_kernel<VT, G><<<row_grid(nn, G), kRowThreads, 0, st>>>(m.rp(), m.ci(), m.val.as<VT>(),
+                                                                                    x0.as<VT>(), b.as<VT>(), nn,
+                                                                                    dstate());
+            });
+            SMAX_CUDA(cudaGetLastError());
+        };
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        SMAX_CUDA(cudaEventCreate(&e0));
+        SMAX_CUDA(cudaEventCreate(&e1));
+        int best = guess;
+        float best_ms = 3.4e38f;
+        try {
+            for (int G = 1; G <= 32; G <<= 1) {
+                launch(G);
+                SMAX_CUDA(cudaEventRecord(e0, st));
+                for (int r = 0; r < 3; ++r) launch(G);
+                SMAX_CUDA(cudaEventRecord(e1, st));
+                SMAX_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                SMAX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = G;
+                }
+            }
+        } catch (...) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return best;
+    }
+
     void read_state(cudaStream_t st) {
         SMAX_CUDA(cudaMemcpyAsync(h_state, state.p, sizeof(SolverState), cudaMemcpyDeviceToHost, st));
         SMAX_CUDA(cudaStreamSynchronize(st));
@@ -539,7 +592,7 @@ template <typename VT> void build_jacobi(smax_solver_s *s, const RegCRS &r, cuda
                                                             s->D.as<VT>(), status.as<DevStatus>());
     SMAX_CUDA(cudaGetLastError());
     check_status(status, st, "Jacobi needs a non-zero diagonal entry in every row");
-    s->gA = group_for(s->A);
+    s->gA = s->tune_group<VT>(s->A, false, st);
 }
 
 template <typename VT> void build_gauss_seidel(smax_solver_s *s, const RegCRS &r, int float_type, cudaStream_t st) {
@@ -570,8 +623,8 @@ template <typename VT> void build_gauss_seidel(smax_solver_s *s, const RegCRS &r
                                                         s->U.val.as<VT>());
     SMAX_CUDA(cudaGetLastError());
     SMAX_CUDA(cudaStreamSynchronize(st));
-    s->gA = group_for(s->A);
-    s->gU = group_for(s->U);
+    s->gA = s->tune_group<VT>(s->A, false, st);
+    s->gU = s->tune_group<VT>(s->U, true, st);
     // the D+L solve: a SpTRSV kernel object of this platform on device arrays
     // (initialize copies them and peels the diagonal), launched without its
     // own graphs so that its launches join the solver's

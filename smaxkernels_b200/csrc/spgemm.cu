@@ -29,10 +29,13 @@ namespace smax {
 
 namespace {
 
-constexpr int kWarpP = 256, kWarpTS = 512;     // warp path: products, table slots
+constexpr int kSmallP = 64, kSmallTS = 128;    // small-row warp path: products, table slots
+constexpr int kSmallWarps = 8;                 // warps per CTA of the small-row path (2.3 KB each)
+constexpr int kWarpP = 256, kWarpTS = 512;     // warp path
 constexpr int kCtaP = 4096, kCtaTS = 8192;     // CTA path
 constexpr int kCtaThreads = 512;
 constexpr int kWarpsPerCta = 4;
+constexpr int kBins = 4;
 
 __device__ __forceinline__ unsigned hash_col(int c) { return (unsigned)c * 0x9E3779B1u; }
 
@@ -52,17 +55,17 @@ __global__ void row_products(const int *__restrict__ arp, const int *__restrict_
     if (lane == 0) P[i] = s;
 }
 
-// rows into three lists by product count (warp, CTA, global paths); the
-// order inside a list is irrelevant (rows are independent)
+// rows into four lists by product count (small-row warp, warp, CTA and global
+// paths); the order inside a list is irrelevant (rows are independent)
 __global__ void bin_rows(const long long *__restrict__ P, int64_t n, int *__restrict__ lists, int *counts) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < n;
     const long long p = valid ? P[i] : 0;
-    const int bin = p <= kWarpP ? 0 : (p <= kCtaP ? 1 : 2);
+    const int bin = p <= kSmallP ? 0 : (p <= kWarpP ? 1 : (p <= kCtaP ? 2 : 3));
     const unsigned active = __ballot_sync(0xffffffffu, valid);
     const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int b = 0; b < 3; ++b) {
+    for (int b = 0; b < kBins; ++b) {
         const unsigned mask = __ballot_sync(0xffffffffu, valid && bin == b) & active;
         if (!mask) continue;
         const int leader = __ffs(mask) - 1;
@@ -154,22 +157,24 @@ struct CtaSync {
     __device__ void operator()() const { __syncthreads(); }
 };
 
-template <typename VT>
-__global__ void __launch_bounds__(kWarpsPerCta * 32) gustavson_warp(
+// One warp per row of at most WP products, with a WTS-slot table (load at
+// most 1/2); WARPS warps per CTA.
+template <typename VT, int WP, int WTS, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) gustavson_warp(
     const int *__restrict__ rows, int n_rows_bin, const long long *__restrict__ P, const long long *__restrict__ Poff,
     const int *__restrict__ arp, const int *__restrict__ acol, const VT *__restrict__ aval,
     const int *__restrict__ brp, const int *__restrict__ bcol, const VT *__restrict__ bval, int *__restrict__ pcol,
     VT *__restrict__ pval, int *__restrict__ count) {
-    __shared__ int keys[kWarpsPerCta][kWarpTS];
-    __shared__ int first[kWarpsPerCta][kWarpTS];
-    __shared__ VT vals[kWarpsPerCta][kWarpTS];
-    __shared__ int posmap[kWarpsPerCta][kWarpP];
+    __shared__ int keys[WARPS][WTS];
+    __shared__ int first[WARPS][WTS];
+    __shared__ VT vals[WARPS][WTS];
+    __shared__ int posmap[WARPS][WP];
     const int w = threadIdx.x >> 5;
-    const int64_t r = (int64_t)blockIdx.x * kWarpsPerCta + w;
+    const int64_t r = (int64_t)blockIdx.x * WARPS + w;
     if (r >= n_rows_bin) return;  // uniform per warp; the warp path never touches CTA barriers
     const int i = rows[r];
     gustavson_row<VT>(i, threadIdx.x & 31, 32, arp, acol, aval, brp, bcol, bval, keys[w], first[w], vals[w],
-                      posmap[w], kWarpTS, P[i], Poff[i], pcol, pval, count, WarpSync());
+                      posmap[w], WTS, P[i], Poff[i], pcol, pval, count, WarpSync());
 }
 
 template <typename VT>
@@ -258,7 +263,7 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     // --- setup: product counts, their offsets, row bins
     w.P.ensure(sizeof(long long) * (n ? n : 1));
     w.Poff.ensure(sizeof(long long) * (n + 1));
-    w.lists.ensure(sizeof(int) * 3 * (n ? n : 1));
+    w.lists.ensure(sizeof(int) * kBins * (n ? n : 1));
     w.counts.ensure(sizeof(int) * 4);
     w.count.ensure(sizeof(int) * (n ? n : 1));
     long long *P = w.P.as<long long>(), *Poff = w.Poff.as<long long>();
@@ -277,16 +282,19 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     SMAX_CUDA(cudaMemcpyAsync(h.counts, w.counts.p, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
     SMAX_CUDA(cudaStreamSynchronize(st));
     const long long total_p = h.total_p;
-    const int nw = h.counts[0], nc = h.counts[1], ng = h.counts[2];
-    const int *rw = w.lists.as<int>(), *rc = rw + n, *rg = rw + 2 * n;
+    const int ns = h.counts[0], nw = h.counts[1], nc = h.counts[2], ng = h.counts[3];
+    const int *rs = w.lists.as<int>(), *rw = rs + n, *rc = rs + 2 * n, *rg = rs + 3 * n;
     SMAX_CUDA(cudaEventRecord(ev[1], st));
     // --- fused Gustavson pass into product-offset (padded) buffers
     w.pcol.ensure(sizeof(int) * (total_p ? total_p : 1));
     w.pval.ensure(sizeof(VT) * (total_p ? total_p : 1));
     int *pcol = w.pcol.as<int>(), *count = w.count.as<int>();
     VT *pval = w.pval.as<VT>();
+    if (ns > 0)
+        gustavson_warp<VT, kSmallP, kSmallTS, kSmallWarps><<<ceil_div_u(ns, kSmallWarps), kSmallWarps * 32, 0, st>>>(
+            rs, ns, P, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), pcol, pval, count);
     if (nw > 0)
-        gustavson_warp<VT><<<ceil_div_u(nw, kWarpsPerCta), kWarpsPerCta * 32, 0, st>>>(
+        gustavson_warp<VT, kWarpP, kWarpTS, kWarpsPerCta><<<ceil_div_u(nw, kWarpsPerCta), kWarpsPerCta * 32, 0, st>>>(
             rw, nw, P, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), pcol, pval, count);
     if (nc > 0) {
         const size_t sm = (size_t)kCtaTS * (sizeof(VT) + 2 * sizeof(int)) + sizeof(int) * kCtaP;

@@ -503,6 +503,14 @@ class Utils:
         check(lib.smax_utils_generate_perm(self._iface._ctx, int(IntType.INT32), int(n_rows), _ptr(row_ptr),
                                            _ptr(col), _ptr(perm), _ptr(inv_perm), type_.encode()))
 
+    def sanity_check_perm(self, n_rows, row_ptr, col, colors) -> bool:
+        """Utils::sanity_check_perm: no row shares a non-zero colour with a
+        lower neighbour."""
+        valid, bad = C.c_int(0), C.c_int64(-1)
+        check(lib.smax_utils_sanity_check_perm(int(IntType.INT32), int(n_rows), _ptr(_i32(row_ptr)), _ptr(_i32(col)),
+                                               _ptr(_i32(colors)), C.byref(valid), C.byref(bad)))
+        return bool(valid.value)
+
     def apply_mat_perm(self, n_rows, row_ptr, col, val, perm_row_ptr, perm_col, perm_val, perm, inv_perm):
         row_ptr, col, perm, inv_perm = _i32(row_ptr), _i32(col), _i32(perm), _i32(inv_perm)
         val = np.ascontiguousarray(val)
