@@ -730,7 +730,8 @@ def wl_solvers(b: Bench):
             return prp, pcol, pval, np.ones(n), (np.ones(n) if kind == "jacobi" else np.zeros(n))
         return rp, col, val, np.ones(n), np.zeros(n)
 
-    for kind in ("jacobi", "gauss_seidel"):
+    program_kinds = ("jacobi", "gauss_seidel") if b.args.solver_cases in ("all", "program") else ()
+    for kind in program_kinds:
         rp, col, val, rhs, x0 = problem(kind, 10)
         n = len(rp) - 1
         bd, x0d = b.dev(rhs), b.dev(x0)
@@ -763,7 +764,9 @@ def wl_solvers(b: Bench):
                graph_blocks_ms=round(res["graph_blocks"][0] * 1e3, 4), plain_ms=round(res["plain"][0] * 1e3, 4))
 
     side = b.args.solver_side
-    for kind in ("jacobi", "gauss_seidel", "gauss_seidel_pc"):
+    large_kinds = {"all": ("jacobi", "gauss_seidel", "gauss_seidel_pc"), "large": ("jacobi", "gauss_seidel",
+                   "gauss_seidel_pc"), "large_jacobi": ("jacobi",)}.get(b.args.solver_cases, ())
+    for kind in large_kinds:
         iters = b.args.solver_iters if kind != "gauss_seidel" else max(2, b.args.solver_iters // 20)
         if kind == "gauss_seidel_pc":
             # multicolour Gauss-Seidel: the matrix in PC colour order, so the
@@ -791,7 +794,8 @@ def wl_solvers(b: Bench):
         with Solver(skind, rp, col, val) as s:
             def run():
                 xd.copy_(x0d)
-                s.solve(bd, xd, tol=0.0, max_iters=iters, check_length=cl, stream=st_ptr)
+                s.solve(bd, xd, tol=0.0, max_iters=iters, check_length=cl, stream=st_ptr,
+                        mode=b.args.solver_mode)
             with b.clocks() as clk:
                 t, reps = b.time(run, budget_s=3.0, max_reps=20)
         t_it = t / iters
@@ -807,7 +811,7 @@ def wl_solvers(b: Bench):
         kern = "jacobi_kernel" if kind == "jacobi" else "rhs_kernel + level-pack SpTRSV (sweep_kernel)"
         b.emit(f"solver_{kind}_poisson2d_{side}", "solver iteration GB/s (algorithmic bytes)", nbytes / t_it / 1e9,
                "GB/s", t_it, reps, "f64", {"n_rows": n, "nnz": nnz, "iterations": iters, "check_length": cl,
-                                          "driver": "device_loop", "inputs": "larger than L2"},
+                                          "driver": b.args.solver_mode, "inputs": "larger than L2"},
                clk.summary(), b.hbm(nbytes, t_it, kern), cpu, ms_per_iteration=round(t_it * 1e3, 5))
         torch.cuda.empty_cache()
 
@@ -1062,6 +1066,11 @@ def main():
                     help="scs_spmv / spmm workloads: value types to run")
     ap.add_argument("--spmm-k", default="16,64", help="spmm workload: vector counts")
     ap.add_argument("--solver-side", type=int, default=2048, help="solvers workload: grid side of the large case")
+    ap.add_argument("--solver-cases", default="all", choices=("all", "program", "large", "large_jacobi"),
+                    help="solvers workload: the programs' 10x10 problem, the large grid (or only its Jacobi case), "
+                         "or both")
+    ap.add_argument("--solver-mode", default="device_loop", choices=("device_loop", "graph_blocks", "plain"),
+                    help="solvers workload: driver of the large-grid case")
     ap.add_argument("--solver-iters", type=int, default=200,
                     help="solvers workload: Jacobi iterations of the large case (Gauss-Seidel: 1/20 of it)")
     args = ap.parse_args()

@@ -425,7 +425,9 @@ smax_status smax_spmv_crs_noalloc(int float_type, uint64_t n_rows, uint64_t n_co
  *                             device kernel ends the loop; the host waits once
  *   SMAX_SOLVER_GRAPH_BLOCKS  one graph launch per check_length iterations and
  *                             residual; the host reads each residual
- *   SMAX_SOLVER_PLAIN         the same launches one by one, no graphs */
+ *   SMAX_SOLVER_PLAIN         the same launches one by one, no graphs
+ * Systems of at most 4096 rows run the whole loop in one launch of one CTA
+ * (x, b and D in shared memory) whatever the driver. */
 typedef struct smax_solver_s *smax_solver;
 #define SMAX_SOLVER_JACOBI 0
 #define SMAX_SOLVER_GAUSS_SEIDEL 1

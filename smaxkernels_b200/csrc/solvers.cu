@@ -21,6 +21,8 @@
 //    maximum and one atomicMax on the bit pattern (non-negative doubles order
 //    like their bits); a one-thread kernel records it, advances the iteration
 //    count and decides whether the loop goes on.
+// Systems of at most kSmallRows rows skip all of this: one CTA runs the whole
+// loop in one launch (small_jacobi, small_gauss_seidel).
 // A row group is G lanes (1, 2, ..., 32) that stride over the row's entries
 // and add their partial sums with shuffles inside the group's lane mask.  G
 // is chosen per matrix when the solver is created: the residual kernel (the
@@ -243,6 +245,158 @@ __global__ void split_fill_kernel(const int *__restrict__ rp, const int *__restr
     }
 }
 
+// ---- small systems: the whole loop in one CTA -----------------------------
+// Up to kSmallRows rows the loop runs in one launch of one CTA, exactly the
+// applications' loop (the check every check_length iterations, the stop test
+// before every iteration, iterations past the last full block unchecked),
+// with x, b and D in shared memory and __syncthreads between the steps.  The
+// loop ends after at most max_iters iterations.
+constexpr int kSmallRows = 4096;
+constexpr int kSmallThreads = 1024;
+
+// block-wide maximum of non-negative doubles (NaNs never win); every thread
+// returns it
+__device__ double block_max(double v, double *red) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const double w = __shfl_xor_sync(0xffffffffu, v, o);
+        if (w > v) v = w;
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+            if (red[w] > m) m = red[w];
+        red[32] = m;
+    }
+    __syncthreads();
+    const double m = red[32];
+    __syncthreads();
+    return m;
+}
+
+// max_r |b_r - (A x)_r| with one thread per row, rows summed in entry order
+template <typename VT>
+__device__ double small_residual(const int *__restrict__ rp, const int *__restrict__ ci, const VT *__restrict__ val,
+                                 const VT *x, const VT *b, int n, double *red) {
+    double mx = 0.0;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        VT s = VT(0);
+        for (int j = rp[r]; j < rp[r + 1]; ++j) s += val[j] * x[ci[j]];
+        const double a = fabs((double)(b[r] - s));
+        if (a > mx) mx = a;
+    }
+    return block_max(mx, red);
+}
+
+__device__ void small_record(SolverState *st, double *hist, int hist_cap, int &checks, double norm) {
+    if (threadIdx.x == 0 && checks < hist_cap) hist[checks] = norm;
+    ++checks;
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(kSmallThreads)
+    small_jacobi(const int *__restrict__ rp, const int *__restrict__ ci, const VT *__restrict__ val,
+                 const VT *__restrict__ Dg, const VT *__restrict__ bg, VT *x0g, VT *x1g, int n, double tol,
+                 int max_iters, int cl, double *hist, int hist_cap, SolverState *st) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    __shared__ double red[33];
+    VT *x0 = reinterpret_cast<VT *>(sm_raw), *x1 = x0 + n, *b = x1 + n, *D = b + n;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        x0[r] = x0g[r];
+        x1[r] = x1g[r];
+        b[r] = bg[r];
+        D[r] = Dg[r];
+    }
+    __syncthreads();
+    int checks = 0, it = 0;
+    double norm = small_residual<VT>(rp, ci, val, x1, b, n, red);  // x1: the first x_new buffer
+    small_record(st, hist, hist_cap, checks, norm);
+    while (norm > tol && it < max_iters) {
+        const bool odd = ((it + 1) & 1) != 0;
+        const VT *xo = odd ? x0 : x1;
+        VT *xn = odd ? x1 : x0;
+        for (int r = threadIdx.x; r < n; r += blockDim.x) {
+            VT s = VT(0);
+            for (int j = rp[r]; j < rp[r + 1]; ++j) s += val[j] * xo[ci[j]];
+            const VT diag_contrib = D[r] * xo[r];
+            const VT offdiag_sum = s - diag_contrib;
+            xn[r] = (b[r] - offdiag_sum) / D[r];
+        }
+        __syncthreads();
+        ++it;
+        if (it % cl == 0) {
+            norm = small_residual<VT>(rp, ci, val, x1, b, n, red);
+            small_record(st, hist, hist_cap, checks, norm);
+        }
+    }
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        x0g[r] = x0[r];
+        x1g[r] = x1[r];
+    }
+    if (threadIdx.x == 0) {
+        st->norm_bits = 0ull;
+        st->norm = norm;
+        st->n_iters = it;
+        st->n_checks = checks;
+        st->active = 0;
+    }
+}
+
+// (D+L) has its diagonal as the last entry of every row (the SpTRSV kernel's
+// peeled copy) and is solved level by level over `order`
+template <typename VT>
+__global__ void __launch_bounds__(kSmallThreads)
+    small_gauss_seidel(const int *__restrict__ arp, const int *__restrict__ aci, const VT *__restrict__ aval,
+                       const int *__restrict__ urp, const int *__restrict__ uci, const VT *__restrict__ uval,
+                       const int *__restrict__ lrp, const int *__restrict__ lci, const VT *__restrict__ lval,
+                       const VT *__restrict__ Dg, const int *__restrict__ order, const int *__restrict__ lvl_ptr,
+                       int n_levels, const VT *__restrict__ bg, VT *xg, int n, double tol, int max_iters, int cl,
+                       double *hist, int hist_cap, SolverState *st) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    __shared__ double red[33];
+    VT *x = reinterpret_cast<VT *>(sm_raw), *tmp = x + n, *b = tmp + n, *D = b + n;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) {
+        x[r] = xg[r];
+        b[r] = bg[r];
+        D[r] = Dg[r];
+    }
+    __syncthreads();
+    int checks = 0, it = 0;
+    double norm = small_residual<VT>(arp, aci, aval, x, b, n, red);
+    small_record(st, hist, hist_cap, checks, norm);
+    while (norm > tol && it < max_iters) {
+        for (int r = threadIdx.x; r < n; r += blockDim.x) {
+            VT s = VT(0);
+            for (int j = urp[r]; j < urp[r + 1]; ++j) s += uval[j] * x[uci[j]];
+            tmp[r] = b[r] - s;
+        }
+        __syncthreads();
+        for (int l = 0; l < n_levels; ++l) {
+            for (int i = lvl_ptr[l] + threadIdx.x; i < lvl_ptr[l + 1]; i += blockDim.x) {
+                const int r = order[i];
+                VT s = VT(0);
+                for (int j = lrp[r]; j < lrp[r + 1] - 1; ++j) s += lval[j] * x[lci[j]];
+                x[r] = (tmp[r] - s) / D[r];
+            }
+            __syncthreads();
+        }
+        ++it;
+        if (it % cl == 0) {
+            norm = small_residual<VT>(arp, aci, aval, x, b, n, red);
+            small_record(st, hist, hist_cap, checks, norm);
+        }
+    }
+    for (int r = threadIdx.x; r < n; r += blockDim.x) xg[r] = x[r];
+    if (threadIdx.x == 0) {
+        st->norm_bits = 0ull;
+        st->norm = norm;
+        st->n_iters = it;
+        st->n_checks = checks;
+        st->active = 0;
+    }
+}
+
 unsigned flat_grid(int64_t n) {
     const int64_t cap = (int64_t)sm_count() * 8;
     int64_t g = (n + 255) / 256;
@@ -300,6 +454,7 @@ struct smax_solver_s {
     DevBuf x0, x1, b, tmp;  // iterate buffers, right-hand side, Gauss-Seidel's rhs of the solve
     DevBuf state, hist;
     int hist_cap = 0;
+    DevBuf small_lvl;  // Gauss-Seidel, small systems: the D+L level pointer on the device
     SolverState *h_state = nullptr;  // pinned copy of the state
     smax_kernel tri = nullptr;       // Gauss-Seidel: SpTRSV on D+L
     // cached graphs and what they were built for
@@ -531,6 +686,40 @@ struct smax_solver_s {
         SMAX_CUDA(cudaMemcpyAsync(b.p, b_in, vb, cudaMemcpyDefault, st));
         SMAX_CUDA(cudaMemcpyAsync(x0.p, x_inout, vb, cudaMemcpyDefault, st));
         if (kind == SMAX_SOLVER_JACOBI) SMAX_CUDA(cudaMemcpyAsync(x1.p, x_inout, vb, cudaMemcpyDefault, st));
+        if (n <= kSmallRows) {
+            // every driver: the whole loop in one CTA, one launch
+            const size_t shm = (size_t)4 * vbytes * n;
+            if (kind == SMAX_SOLVER_JACOBI) {
+                SMAX_CUDA(cudaFuncSetAttribute(small_jacobi<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)shm));
+                small_jacobi<VT><<<1, kSmallThreads, shm, st>>>(A.rp(), A.ci(), A.val.as<VT>(), D.as<VT>(),
+                                                                b.as<VT>(), x0.as<VT>(), x1.as<VT>(), (int)n, o.tol,
+                                                                o.max_iters, cl, hist.as<double>(), hist_cap,
+                                                                dstate());
+            } else {
+                smax_kernel_s *t = K(tri);
+                SMAX_CUDA(cudaFuncSetAttribute(small_gauss_seidel<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)shm));
+                small_gauss_seidel<VT><<<1, kSmallThreads, shm, st>>>(
+                    A.rp(), A.ci(), A.val.as<VT>(), U.rp(), U.ci(), U.val.as<VT>(), t->dA.rp(), t->dA.ci(),
+                    t->dA.val.as<VT>(), t->D.as<VT>(), t->tri.order.as<int>(), small_lvl.as<int>(),
+                    t->tri.n_levels(), b.as<VT>(), x0.as<VT>(), (int)n, o.tol, o.max_iters, cl, hist.as<double>(),
+                    hist_cap, dstate());
+            }
+            SMAX_CUDA(cudaGetLastError());
+            read_state(st);
+            const int n_iters = h_state->n_iters;
+            const void *latest = (kind == SMAX_SOLVER_JACOBI && (n_iters & 1)) ? x1.p : x0.p;
+            SMAX_CUDA(cudaMemcpyAsync(x_inout, latest, vb, cudaMemcpyDefault, st));
+            SMAX_CUDA(cudaStreamSynchronize(st));
+            stats.n_iters = n_iters;
+            stats.residual_norm = h_state->norm;
+            stats.converged = h_state->norm < o.tol;
+            stats.n_checks = h_state->n_checks;
+            stats.host_waits = 1;
+            last_checks = h_state->n_checks;
+            return;
+        }
         const bool graphs = o.mode != SMAX_SOLVER_PLAIN;
         if (graphs && (g_tol != o.tol || g_limit != limit || g_cl != cl || g_hist != hist.p)) {
             release_graphs();
@@ -642,6 +831,14 @@ template <typename VT> void build_gauss_seidel(smax_solver_s *s, const RegCRS &r
     t->stream = st;
     apply_core(t, 0, 0);
     read_status(t);
+    if (n > 0 && n <= kSmallRows) {
+        // the one-CTA loop walks the SpTRSV plan's levels itself
+        if (!t->tri.has_order) fail(SMAX_ERR_STATE, "the D+L plan has no level order");
+        const std::vector<int> &lp = t->tri.lvl_ptr;
+        s->small_lvl.alloc(sizeof(int) * lp.size());
+        SMAX_CUDA(cudaMemcpyAsync(s->small_lvl.p, lp.data(), sizeof(int) * lp.size(), cudaMemcpyHostToDevice, st));
+        SMAX_CUDA(cudaStreamSynchronize(st));
+    }
 }
 
 }  // namespace

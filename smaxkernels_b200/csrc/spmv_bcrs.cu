@@ -48,7 +48,7 @@ __device__ __forceinline__ void load16(const VT *p, VT *o) {
 
 constexpr int kMaxBs = 128;  // largest block size of the stream path
 
-template <typename VT>
+template <typename VT, bool UNROLL>
 __global__ void __launch_bounds__(256) bcrs_stream_kernel(const int *__restrict__ row_ptr,
                                                           const int *__restrict__ col, const VT *__restrict__ val,
                                                           int64_t n_brows, int bh, int bw, int hpad, int wpad,
@@ -75,7 +75,33 @@ __global__ void __launch_bounds__(256) bcrs_stream_kernel(const int *__restrict_
     for (int i = 0; i < VEC; ++i) acc[i] = VT(0);
     const int64_t b0 = row_ptr[br], b1 = row_ptr[br + 1];
     const int64_t end = b1 * bs;
-    for (int64_t f = b0 * bs + lane * VEC; f < end; f += 32 * VEC) {
+    constexpr int64_t STEP = 32 * VEC;
+    int64_t f = b0 * bs + lane * VEC;
+    // four steps' value and column loads first, then their x gathers, then
+    // the products in step order (the same sums as the one-step loop); for
+    // short block rows the registers this takes cost more occupancy than the
+    // overlap gains, so it is compiled out (UNROLL false)
+    if constexpr (UNROLL)
+    for (; f + 3 * STEP < end; f += 4 * STEP) {
+        VT v[4][VEC];
+        int64_t c[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            load16<VT, VEC>(val + f + u * STEP, v[u]);
+            c[u] = (int64_t)col[(f + u * STEP) / bs] * wpad;
+        }
+        VT xv[4][VEC];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int i = 0; i < VEC; ++i) xv[u][i] = ok[i] ? ld_keep(x + c[u] + jx[i]) : VT(0);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int i = 0; i < VEC; ++i)
+                if (ok[i]) acc[i] += v[u][i] * xv[u][i];
+    }
+    for (; f < end; f += STEP) {
         const int64_t c = (int64_t)col[f / bs] * wpad;
         VT v[VEC];
         load16<VT, VEC>(val + f, v);
@@ -186,11 +212,19 @@ bool bcrs_stream_path(int64_t hpad, int64_t wpad, int vbytes) {
 template <typename VT>
 void bcrs_spmv(const DevBCRS &m, const VT *x, VT *y, cudaStream_t st) {
     if (m.n_rows == 0) return;
-    if (bcrs_stream_path(m.hpad, m.wpad, sizeof(VT)))
-        bcrs_stream_kernel<VT><<<ceil_div_u(m.n_rows, 8), 256, 0, st>>>(
-            m.row_ptr.as<int>(), m.col.as<int>(), m.val.as<VT>(), m.n_rows, (int)m.bh, (int)m.bw, (int)m.hpad,
-            (int)m.wpad, m.col_major ? 1 : 0, x, y);
-    else
+    if (bcrs_stream_path(m.hpad, m.wpad, sizeof(VT))) {
+        // the four-step loop pays off from a mean of about three steps per block row
+        const double steps = (double)m.n_blocks * (double)(m.hpad * m.wpad) /
+                             ((double)m.n_rows * 32.0 * (16.0 / sizeof(VT)));
+        if (steps >= 3.0)
+            bcrs_stream_kernel<VT, true><<<ceil_div_u(m.n_rows, 8), 256, 0, st>>>(
+                m.row_ptr.as<int>(), m.col.as<int>(), m.val.as<VT>(), m.n_rows, (int)m.bh, (int)m.bw, (int)m.hpad,
+                (int)m.wpad, m.col_major ? 1 : 0, x, y);
+        else
+            bcrs_stream_kernel<VT, false><<<ceil_div_u(m.n_rows, 8), 256, 0, st>>>(
+                m.row_ptr.as<int>(), m.col.as<int>(), m.val.as<VT>(), m.n_rows, (int)m.bh, (int)m.bw, (int)m.hpad,
+                (int)m.wpad, m.col_major ? 1 : 0, x, y);
+    } else
         bcrs_thread_kernel<VT><<<ceil_div_u(m.n_rows, 128), 128, 0, st>>>(
             m.row_ptr.as<int>(), m.col.as<int>(), m.val.as<VT>(), m.n_rows, (int)m.bh, (int)m.bw, (int)m.hpad,
             (int)m.wpad, m.col_major ? 1 : 0, x, y);

@@ -85,10 +85,14 @@ def test_the_programs_problem(kind, mode):
 @pytest.mark.parametrize("kind", ["jacobi", "gauss_seidel"])
 @pytest.mark.parametrize("nx,max_iters,check_length,tol", [(24, 1000, 5, 1e-8), (17, 37, 5, 1e-8),
                                                           (12, 60, 1, 0.0), (9, 300, 7, 1e-6),
-                                                          (16, 4, 5, 1e-8), (8, 0, 5, 1e-8)])
+                                                          (16, 4, 5, 1e-8), (8, 0, 5, 1e-8),
+                                                          (72, 37, 5, 1e-8), (72, 30, 1, 0.0),
+                                                          (66, 400, 7, 1e-3), (72, 3, 5, 1e-8)])
 def test_loop_shapes_against_the_oracle(kind, nx, max_iters, check_length, tol):
     """Runs that converge, run out of iterations, end inside a block (a tail
-    without a residual check), check every iteration, or do nothing."""
+    without a residual check), check every iteration, or do nothing -- on
+    systems small enough for the one-CTA loop and (nx >= 66, more than 4096
+    rows) on the multi-launch drivers with their graphs."""
     rp, col, val, _, _, _ = app_problem(kind, nx, gpu_perm=False)
     n = len(rp) - 1
     b = M.uniform_vector(n, 4)
