@@ -331,8 +331,74 @@ class Utils {
                         "apply_vec_perm");
     }
 
+    // Utils::sanity_check_perm (src/utils/permutations.hpp:794-818)
+    template <typename IT> bool sanity_check_perm(int A_n_rows, const IT *A_row_ptr, const IT *A_col, const int *colors) {
+        int valid = 0;
+        detail::require(smax_utils_sanity_check_perm(SMAX_INT32, (uint64_t)A_n_rows, A_row_ptr, A_col, colors, &valid,
+                                                     nullptr),
+                        "sanity_check_perm");
+        return valid != 0;
+    }
+
+    // The examples' Matrix Market reader + convert_coo_to_crs
+    // (examples/matrix_structs.hpp:52-180, 338-387): CRS arrays allocated with
+    // new[] (release with smax_free_host)
+    template <typename VT>
+    int read_mtx(const std::string &path, uint64_t &n_rows, uint64_t &n_cols, uint64_t &nnz, int *&row_ptr, int *&col,
+                 VT *&val) {
+        void *rp = nullptr, *cl = nullptr, *vl = nullptr;
+        const int rc = detail::check(smax_utils_read_mtx(path.c_str(), detail::float_code<VT>(), &n_rows, &n_cols, &nnz,
+                                                         &rp, &cl, &vl),
+                                     "read_mtx");
+        if (rc) return rc;
+        row_ptr = static_cast<int *>(rp);
+        col = static_cast<int *>(cl);
+        val = static_cast<VT *>(vl);
+        return 0;
+    }
+
   private:
     smax_ctx ctx_;
+};
+
+// The reference's solver programs (examples/applications/jacobi,
+// gauss_seidel) on device-resident operators: smax_solver_* with RAII.
+class Solver {
+  public:
+    enum Kind { JACOBI = SMAX_SOLVER_JACOBI, GAUSS_SEIDEL = SMAX_SOLVER_GAUSS_SEIDEL };
+    template <typename VT>
+    Solver(Kind kind, uint64_t n_rows, uint64_t nnz, const int *row_ptr, const int *col, const VT *val)
+        : vbytes_(sizeof(VT)) {
+        detail::require(smax_solver_create(&s_, kind, detail::float_code<VT>(), n_rows, nnz, row_ptr, col, val),
+                        "Solver");
+    }
+    ~Solver() {
+        if (s_) smax_solver_destroy(s_);
+    }
+    Solver(const Solver &) = delete;
+    Solver &operator=(const Solver &) = delete;
+
+    // the applications' loop from the initial guess in x; the solution is left in x
+    template <typename VT>
+    smax_solver_stats solve(const VT *b, VT *x, double tol = 1e-8, int max_iters = 1000, int check_length = 5,
+                            int mode = SMAX_SOLVER_DEVICE_LOOP, void *stream = nullptr) {
+        if (sizeof(VT) != vbytes_) throw std::runtime_error("Solver::solve: value type differs from the matrix");
+        smax_solver_opts o{tol, max_iters, check_length, mode};
+        smax_solver_stats st{};
+        detail::require(smax_solver_solve(s_, b, x, &o, &st, stream), "Solver::solve");
+        return st;
+    }
+    std::vector<double> history() const {
+        int count = 0;
+        detail::require(smax_solver_get_history(s_, nullptr, 0, &count), "Solver::history");
+        std::vector<double> h(count);
+        if (count) detail::require(smax_solver_get_history(s_, h.data(), count, &count), "Solver::history");
+        return h;
+    }
+
+  private:
+    smax_solver s_ = nullptr;
+    size_t vbytes_;
 };
 
 class Interface {

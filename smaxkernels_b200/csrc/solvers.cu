@@ -282,7 +282,9 @@ __device__ double small_residual(const int *__restrict__ rp, const int *__restri
     double mx = 0.0;
     for (int r = threadIdx.x; r < n; r += blockDim.x) {
         VT s = VT(0);
-        for (int j = rp[r]; j < rp[r + 1]; ++j) s += val[j] * x[ci[j]];
+        const int e = rp[r + 1];
+#pragma unroll 4
+        for (int j = rp[r]; j < e; ++j) s += val[j] * x[ci[j]];
         const double a = fabs((double)(b[r] - s));
         if (a > mx) mx = a;
     }
@@ -318,7 +320,9 @@ __global__ void __launch_bounds__(kSmallThreads)
         VT *xn = odd ? x1 : x0;
         for (int r = threadIdx.x; r < n; r += blockDim.x) {
             VT s = VT(0);
-            for (int j = rp[r]; j < rp[r + 1]; ++j) s += val[j] * xo[ci[j]];
+            const int e = rp[r + 1];
+#pragma unroll 4
+            for (int j = rp[r]; j < e; ++j) s += val[j] * xo[ci[j]];
             const VT diag_contrib = D[r] * xo[r];
             const VT offdiag_sum = s - diag_contrib;
             xn[r] = (b[r] - offdiag_sum) / D[r];
@@ -368,7 +372,9 @@ __global__ void __launch_bounds__(kSmallThreads)
     while (norm > tol && it < max_iters) {
         for (int r = threadIdx.x; r < n; r += blockDim.x) {
             VT s = VT(0);
-            for (int j = urp[r]; j < urp[r + 1]; ++j) s += uval[j] * x[uci[j]];
+            const int e = urp[r + 1];
+#pragma unroll 4
+            for (int j = urp[r]; j < e; ++j) s += uval[j] * x[uci[j]];
             tmp[r] = b[r] - s;
         }
         __syncthreads();
@@ -376,7 +382,9 @@ __global__ void __launch_bounds__(kSmallThreads)
             for (int i = lvl_ptr[l] + threadIdx.x; i < lvl_ptr[l + 1]; i += blockDim.x) {
                 const int r = order[i];
                 VT s = VT(0);
-                for (int j = lrp[r]; j < lrp[r + 1] - 1; ++j) s += lval[j] * x[lci[j]];
+                const int e = lrp[r + 1] - 1;
+#pragma unroll 4
+                for (int j = lrp[r]; j < e; ++j) s += lval[j] * x[lci[j]];
                 x[r] = (tmp[r] - s) / D[r];
             }
             __syncthreads();
@@ -689,10 +697,12 @@ struct smax_solver_s {
         if (n <= kSmallRows) {
             // every driver: the whole loop in one CTA, one launch
             const size_t shm = (size_t)4 * vbytes * n;
+            // one thread per row up to kSmallThreads: idle warps only add to every barrier
+            const int threads = (int)std::min<int64_t>(kSmallThreads, std::max<int64_t>(32, (n + 31) / 32 * 32));
             if (kind == SMAX_SOLVER_JACOBI) {
                 SMAX_CUDA(cudaFuncSetAttribute(small_jacobi<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)shm));
-                small_jacobi<VT><<<1, kSmallThreads, shm, st>>>(A.rp(), A.ci(), A.val.as<VT>(), D.as<VT>(),
+                small_jacobi<VT><<<1, threads, shm, st>>>(A.rp(), A.ci(), A.val.as<VT>(), D.as<VT>(),
                                                                 b.as<VT>(), x0.as<VT>(), x1.as<VT>(), (int)n, o.tol,
                                                                 o.max_iters, cl, hist.as<double>(), hist_cap,
                                                                 dstate());
@@ -700,7 +710,7 @@ struct smax_solver_s {
                 smax_kernel_s *t = K(tri);
                 SMAX_CUDA(cudaFuncSetAttribute(small_gauss_seidel<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                (int)shm));
-                small_gauss_seidel<VT><<<1, kSmallThreads, shm, st>>>(
+                small_gauss_seidel<VT><<<1, threads, shm, st>>>(
                     A.rp(), A.ci(), A.val.as<VT>(), U.rp(), U.ci(), U.val.as<VT>(), t->dA.rp(), t->dA.ci(),
                     t->dA.val.as<VT>(), t->D.as<VT>(), t->tri.order.as<int>(), small_lvl.as<int>(),
                     t->tri.n_levels(), b.as<VT>(), x0.as<VT>(), (int)n, o.tol, o.max_iters, cl, hist.as<double>(),

@@ -251,5 +251,40 @@ int main(int argc, char **argv) {
         const int cpu = smax.register_kernel("cpu", KernelType::SPMV, PlatformType::CPU);
         report("error_conventions", threw && bad_count && cpu == 1, 0.0);
     }
+
+    // -- Jacobi solver on the Laplacian: the iteration count and solution of a
+    //    host loop with the applications' rules (residual before the loop and
+    //    every 5 iterations, measured on the first x_new buffer)
+    {
+        const Crs P = laplace(12);
+        const int m = P.n;
+        std::vector<double> b(m), D(m);
+        for (int i = 0; i < m; ++i) b[i] = std::cos(0.21 * i);
+        for (int r = 0; r < m; ++r)
+            for (int j = P.rp[r]; j < P.rp[r + 1]; ++j)
+                if (P.col[j] == r) D[r] = P.val[j];
+        std::vector<double> x_old(m, 0.0), x_new(m, 0.0);
+        std::vector<double> *xo = &x_old, *xn = &x_new, *first = &x_new;
+        auto resid = [&]() {
+            const std::vector<double> t = host_spmv(P, *first);
+            double mx = 0.0;
+            for (int i = 0; i < m; ++i) mx = std::fmax(mx, std::fabs(b[i] - t[i]));
+            return mx;
+        };
+        double norm = resid();
+        int it = 0;
+        while (norm > 1e-8 && it < 1000) {
+            const std::vector<double> s = host_spmv(P, *xo);
+            for (int i = 0; i < m; ++i) (*xn)[i] = (b[i] - (s[i] - D[i] * (*xo)[i])) / D[i];
+            std::swap(xo, xn);
+            ++it;
+            if (it % 5 == 0) norm = resid();
+        }
+        std::vector<double> x(m, 0.0);
+        Solver s(Solver::JACOBI, (uint64_t)m, (uint64_t)P.col.size(), P.rp.data(), P.col.data(), P.val.data());
+        const smax_solver_stats st = s.solve(b.data(), x.data());
+        const double err = rel_err(x, *xo);
+        report("jacobi_solver", st.n_iters == it && err < 1e-12 && (int)s.history().size() == st.n_checks, err);
+    }
     return failures ? 1 : 0;
 }
