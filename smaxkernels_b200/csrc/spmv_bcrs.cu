@@ -14,7 +14,10 @@
 // sees the same VEC in-block positions, so it keeps VEC register accumulators
 // for fixed (ix, jx).  Lanes holding the same positions combine with
 // shuffles; the bs partial sums are then folded into the bh outputs through
-// a per-warp shared-memory tile (fixed order, deterministic).  Other block
+// a per-warp shared-memory tile (fixed order, deterministic).  Long block
+// rows (three or more warp steps on average) use a four-step loop with more
+// loads in flight; short ones (under two steps: e.g. a stencil in 4x4 blocks)
+// give each block row a group of bs/VEC lanes instead of a warp.  Other block
 // shapes: one thread per block row in the reference's loop order.
 //
 // Conversion: per block row, the sorted distinct block columns of its bh rows
@@ -124,6 +127,78 @@ __global__ void __launch_bounds__(256) bcrs_stream_kernel(const int *__restrict_
     }
 }
 
+// Short block rows: a group of G = bs / VEC lanes per block row (8 lanes for
+// 4x4 FP64), one block per step, two blocks' loads in flight.  Every lane
+// keeps the same VEC in-block positions for the whole row, so the bs sums
+// are complete without shuffles and are folded into the bh outputs through
+// the group's shared-memory tile (fixed order).
+template <typename VT>
+__global__ void __launch_bounds__(256) bcrs_group_kernel(const int *__restrict__ row_ptr,
+                                                         const int *__restrict__ col, const VT *__restrict__ val,
+                                                         int64_t n_brows, int bh, int bw, int hpad, int wpad,
+                                                         int col_major, const VT *__restrict__ x,
+                                                         VT *__restrict__ y) {
+    constexpr int VEC = V16<VT>::N;
+    __shared__ VT tile[256 * VEC];  // 256 / G groups x bs values = 256 * VEC
+    const int bs = hpad * wpad;
+    const int G = bs / VEC;
+    const int g_in_cta = threadIdx.x / G, lg = threadIdx.x % G;
+    const int64_t br = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const int o = lg * VEC;
+    int jx[VEC];
+    bool ok[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) {
+        const int q = o + i;
+        const int ix = col_major ? q % hpad : q / wpad;
+        jx[i] = col_major ? q / hpad : q % wpad;
+        ok[i] = ix < bh && jx[i] < bw;
+    }
+    VT acc[VEC];
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) acc[i] = VT(0);
+    if (br < n_brows) {
+        const int b1 = row_ptr[br + 1];
+        int j = row_ptr[br];
+        for (; j + 1 < b1; j += 2) {
+            VT v0[VEC], v1[VEC];
+            load16<VT, VEC>(val + (int64_t)j * bs + o, v0);
+            load16<VT, VEC>(val + (int64_t)(j + 1) * bs + o, v1);
+            const int64_t c0 = (int64_t)col[j] * wpad, c1 = (int64_t)col[j + 1] * wpad;
+            VT x0[VEC], x1[VEC];
+#pragma unroll
+            for (int i = 0; i < VEC; ++i) {
+                x0[i] = ok[i] ? ld_keep(x + c0 + jx[i]) : VT(0);
+                x1[i] = ok[i] ? ld_keep(x + c1 + jx[i]) : VT(0);
+            }
+#pragma unroll
+            for (int i = 0; i < VEC; ++i)
+                if (ok[i]) {
+                    acc[i] += v0[i] * x0[i];
+                    acc[i] += v1[i] * x1[i];
+                }
+        }
+        if (j < b1) {
+            VT v[VEC];
+            load16<VT, VEC>(val + (int64_t)j * bs + o, v);
+            const int64_t c = (int64_t)col[j] * wpad;
+#pragma unroll
+            for (int i = 0; i < VEC; ++i)
+                if (ok[i]) acc[i] += v[i] * ld_keep(x + c + jx[i]);
+        }
+    }
+    VT *t = tile + g_in_cta * bs;
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) t[o + i] = acc[i];
+    __syncthreads();
+    if (br < n_brows)
+        for (int ix = lg; ix < bh; ix += G) {
+            VT s = VT(0);
+            for (int q = 0; q < bw; ++q) s += t[col_major ? q * hpad + ix : ix * wpad + q];
+            st_stream(y + br * hpad + ix, s);
+        }
+}
+
 // generic block shapes: one thread per block row, the reference's loop order
 template <typename VT>
 __global__ void bcrs_thread_kernel(const int *__restrict__ row_ptr, const int *__restrict__ col,
@@ -213,10 +288,16 @@ template <typename VT>
 void bcrs_spmv(const DevBCRS &m, const VT *x, VT *y, cudaStream_t st) {
     if (m.n_rows == 0) return;
     if (bcrs_stream_path(m.hpad, m.wpad, sizeof(VT))) {
-        // the four-step loop pays off from a mean of about three steps per block row
+        // mean warp steps per block row: below two a lane group per block row
+        // wastes fewer lanes; the four-step loop pays off from about three
         const double steps = (double)m.n_blocks * (double)(m.hpad * m.wpad) /
                              ((double)m.n_rows * 32.0 * (16.0 / sizeof(VT)));
-        if (steps >= 3.0)
+        const int64_t group = m.hpad * m.wpad / (16 / (int64_t)sizeof(VT));
+        if (steps < 2.0)
+            bcrs_group_kernel<VT><<<ceil_div_u((uint64_t)m.n_rows * group, 256), 256, 0, st>>>(
+                m.row_ptr.as<int>(), m.col.as<int>(), m.val.as<VT>(), m.n_rows, (int)m.bh, (int)m.bw, (int)m.hpad,
+                (int)m.wpad, m.col_major ? 1 : 0, x, y);
+        else if (steps >= 3.0)
             bcrs_stream_kernel<VT, true><<<ceil_div_u(m.n_rows, 8), 256, 0, st>>>(
                 m.row_ptr.as<int>(), m.col.as<int>(), m.val.as<VT>(), m.n_rows, (int)m.bh, (int)m.bw, (int)m.hpad,
                 (int)m.wpad, m.col_major ? 1 : 0, x, y);

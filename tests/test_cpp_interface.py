@@ -39,4 +39,4 @@ def test_cpp_interface_on_gpu(program):
     r = subprocess.run([program], capture_output=True, text=True, timeout=600)
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.count("PASS") == 8 and "FAIL" not in r.stdout
+    assert r.stdout.count("PASS") == 9 and "FAIL" not in r.stdout
