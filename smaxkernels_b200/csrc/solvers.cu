@@ -253,6 +253,7 @@ __global__ void split_fill_kernel(const int *__restrict__ rp, const int *__restr
 // loop ends after at most max_iters iterations.
 constexpr int kSmallRows = 4096;
 constexpr int kSmallThreads = 1024;
+constexpr int kSmallStageBytes = 200 * 1024;  // dynamic shared memory of the one-CTA loop, at most
 
 // block-wide maximum of non-negative doubles (NaNs never win); every thread
 // returns it
@@ -354,9 +355,9 @@ __global__ void __launch_bounds__(kSmallThreads)
     small_gauss_seidel(const int *__restrict__ arp, const int *__restrict__ aci, const VT *__restrict__ aval,
                        const int *__restrict__ urp, const int *__restrict__ uci, const VT *__restrict__ uval,
                        const int *__restrict__ lrp, const int *__restrict__ lci, const VT *__restrict__ lval,
-                       const VT *__restrict__ Dg, const int *__restrict__ order, const int *__restrict__ lvl_ptr,
+                       const VT *__restrict__ Dg, const int *__restrict__ order_g, const int *__restrict__ lvl_g,
                        int n_levels, const VT *__restrict__ bg, VT *xg, int n, double tol, int max_iters, int cl,
-                       double *hist, int hist_cap, SolverState *st) {
+                       double *hist, int hist_cap, SolverState *st, int stage) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
     __shared__ double red[33];
     VT *x = reinterpret_cast<VT *>(sm_raw), *tmp = x + n, *b = tmp + n, *D = b + n;
@@ -364,6 +365,28 @@ __global__ void __launch_bounds__(kSmallThreads)
         x[r] = xg[r];
         b[r] = bg[r];
         D[r] = Dg[r];
+    }
+    // with stage, the level sweep's arrays follow the vectors in shared memory:
+    // its chain of dependent loads per level then never leaves the SM
+    const int *order = order_g, *lvl_ptr = lvl_g, *lrp_s = lrp, *lci_s = lci;
+    const VT *lval_s = lval;
+    if (stage) {
+        const int nl = lrp[n];
+        VT *sv = D + n;
+        int *si = reinterpret_cast<int *>(sv + nl);
+        int *so = si, *sp = so + n, *sl = sp + n + 1, *sc = sl + n_levels + 1;
+        for (int j = threadIdx.x; j < nl; j += blockDim.x) {
+            sv[j] = lval[j];
+            sc[j] = lci[j];
+        }
+        for (int r = threadIdx.x; r < n; r += blockDim.x) so[r] = order_g[r];
+        for (int r = threadIdx.x; r <= n; r += blockDim.x) sp[r] = lrp[r];
+        for (int l = threadIdx.x; l <= n_levels; l += blockDim.x) sl[l] = lvl_g[l];
+        order = so;
+        lvl_ptr = sl;
+        lrp_s = sp;
+        lci_s = sc;
+        lval_s = sv;
     }
     __syncthreads();
     int checks = 0, it = 0;
@@ -382,9 +405,9 @@ __global__ void __launch_bounds__(kSmallThreads)
             for (int i = lvl_ptr[l] + threadIdx.x; i < lvl_ptr[l + 1]; i += blockDim.x) {
                 const int r = order[i];
                 VT s = VT(0);
-                const int e = lrp[r + 1] - 1;
+                const int e = lrp_s[r + 1] - 1;
 #pragma unroll 4
-                for (int j = lrp[r]; j < e; ++j) s += lval[j] * x[lci[j]];
+                for (int j = lrp_s[r]; j < e; ++j) s += lval_s[j] * x[lci_s[j]];
                 x[r] = (tmp[r] - s) / D[r];
             }
             __syncthreads();
@@ -708,13 +731,18 @@ struct smax_solver_s {
                                                                 dstate());
             } else {
                 smax_kernel_s *t = K(tri);
+                // the level sweep's arrays in shared memory too, when they fit
+                const int64_t nl = t->dA.nnz, L = t->tri.n_levels();
+                const size_t staged = shm + (size_t)vbytes * nl + sizeof(int) * (size_t)(n + (n + 1) + (L + 1) + nl);
+                const int stage = staged <= (size_t)kSmallStageBytes ? 1 : 0;
+                const size_t bytes = stage ? staged : shm;
                 SMAX_CUDA(cudaFuncSetAttribute(small_gauss_seidel<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)shm));
-                small_gauss_seidel<VT><<<1, threads, shm, st>>>(
+                                               (int)bytes));
+                small_gauss_seidel<VT><<<1, threads, bytes, st>>>(
                     A.rp(), A.ci(), A.val.as<VT>(), U.rp(), U.ci(), U.val.as<VT>(), t->dA.rp(), t->dA.ci(),
-                    t->dA.val.as<VT>(), t->D.as<VT>(), t->tri.order.as<int>(), small_lvl.as<int>(),
-                    t->tri.n_levels(), b.as<VT>(), x0.as<VT>(), (int)n, o.tol, o.max_iters, cl, hist.as<double>(),
-                    hist_cap, dstate());
+                    t->dA.val.as<VT>(), t->D.as<VT>(), t->tri.order.as<int>(), small_lvl.as<int>(), (int)L,
+                    b.as<VT>(), x0.as<VT>(), (int)n, o.tol, o.max_iters, cl, hist.as<double>(), hist_cap, dstate(),
+                    stage);
             }
             SMAX_CUDA(cudaGetLastError());
             read_state(st);
