@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(kSmallThreads)
     for (int r = threadIdx.x; r < n; r += blockDim.x) {
         x[r] = xg[r];
         b[r] = bg[r];
-        D[r] = Dg[r];
+        D[r] = VT(1) / Dg[r];  // the sweep multiplies by 1/D, as the level-pack SpTRSV does
     }
     // with stage, the level sweep's arrays follow the vectors in shared memory:
     // its chain of dependent loads per level then never leaves the SM
@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(kSmallThreads)
                 const int e = lrp_s[r + 1] - 1;
 #pragma unroll 4
                 for (int j = lrp_s[r]; j < e; ++j) s += lval_s[j] * x[lci_s[j]];
-                x[r] = (tmp[r] - s) / D[r];
+                x[r] = (tmp[r] - s) * D[r];
             }
             __syncthreads();
         }

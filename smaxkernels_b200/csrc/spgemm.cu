@@ -29,8 +29,9 @@ namespace smax {
 
 namespace {
 
-constexpr int kSmallP = 64, kSmallTS = 128;    // small-row warp path: products, table slots
-constexpr int kSmallWarps = 8;                 // warps per CTA of the small-row path (2.3 KB each)
+constexpr int kSmallP = 64, kSmallTS = 128;    // small-row path: products, table slots
+constexpr int kSmallTeam = 8;                  // lanes per row of the small-row path
+constexpr int kSmallWarps = 4;                 // warps per CTA: 16 rows, 2.3 KB of tables each
 constexpr int kWarpP = 256, kWarpTS = 512;     // warp path
 constexpr int kCtaP = 4096, kCtaTS = 8192;     // CTA path
 constexpr int kCtaThreads = 512;
@@ -125,9 +126,12 @@ __device__ __forceinline__ void gustavson_row(int i, int t, int tsize, const int
         const long long q = q0 + t;
         const int h = q < P ? posmap[q] : -1;
         const int take = h >= 0;
-        // team-wide exclusive scan of `take` (warp ballots, then warps in order)
-        const unsigned bal = __ballot_sync(0xffffffffu, take);
-        const int lane = t & 31, warp = t >> 5;
+        // team-wide exclusive scan of `take` (warp ballots, then warps in
+        // order); a team smaller than a warp uses only its own lanes' bits
+        const int lane = (int)(threadIdx.x & 31), warp = t >> 5;
+        const unsigned tmask =
+            tsize >= 32 ? 0xffffffffu : (((1u << tsize) - 1u) << ((unsigned)lane & ~(unsigned)(tsize - 1)));
+        const unsigned bal = __ballot_sync(tmask, take) & tmask;
         const int before_in_warp = __popc(bal & ((1u << lane) - 1u));
         int before = before_in_warp, total = __popc(bal);
         if (tsize > 32) {
@@ -150,31 +154,37 @@ __device__ __forceinline__ void gustavson_row(int i, int t, int tsize, const int
     if (t == 0) count[i] = written;
 }
 
-struct WarpSync {
-    __device__ void operator()() const { __syncwarp(); }
+// the lanes of one team inside a warp (the whole warp for a team of 32)
+struct GroupSync {
+    unsigned mask;
+    __device__ void operator()() const { __syncwarp(mask); }
 };
 struct CtaSync {
     __device__ void operator()() const { __syncthreads(); }
 };
 
-// One warp per row of at most WP products, with a WTS-slot table (load at
-// most 1/2); WARPS warps per CTA.
-template <typename VT, int WP, int WTS, int WARPS>
+// A team of G lanes (G <= 32, a power of two) per row of at most WP products,
+// with a WTS-slot table (load at most 1/2); WARPS warps per CTA, 32 / G rows
+// per warp.  Small teams suit rows whose B rows are short: a team covers one
+// B row per step of the product loop.
+template <typename VT, int WP, int WTS, int WARPS, int G>
 __global__ void __launch_bounds__(WARPS * 32) gustavson_warp(
     const int *__restrict__ rows, int n_rows_bin, const long long *__restrict__ P, const long long *__restrict__ Poff,
     const int *__restrict__ arp, const int *__restrict__ acol, const VT *__restrict__ aval,
     const int *__restrict__ brp, const int *__restrict__ bcol, const VT *__restrict__ bval, int *__restrict__ pcol,
     VT *__restrict__ pval, int *__restrict__ count) {
-    __shared__ int keys[WARPS][WTS];
-    __shared__ int first[WARPS][WTS];
-    __shared__ VT vals[WARPS][WTS];
-    __shared__ int posmap[WARPS][WP];
-    const int w = threadIdx.x >> 5;
-    const int64_t r = (int64_t)blockIdx.x * WARPS + w;
-    if (r >= n_rows_bin) return;  // uniform per warp; the warp path never touches CTA barriers
+    constexpr int TEAMS = WARPS * 32 / G;
+    __shared__ int keys[TEAMS][WTS];
+    __shared__ int first[TEAMS][WTS];
+    __shared__ VT vals[TEAMS][WTS];
+    __shared__ int posmap[TEAMS][WP];
+    const int g = threadIdx.x / G;
+    const int64_t r = (int64_t)blockIdx.x * TEAMS + g;
+    if (r >= n_rows_bin) return;  // uniform per team; teams never touch CTA barriers
     const int i = rows[r];
-    gustavson_row<VT>(i, threadIdx.x & 31, 32, arp, acol, aval, brp, bcol, bval, keys[w], first[w], vals[w],
-                      posmap[w], WTS, P[i], Poff[i], pcol, pval, count, WarpSync());
+    const unsigned mask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(unsigned)(G - 1)));
+    gustavson_row<VT>(i, (int)(threadIdx.x % G), G, arp, acol, aval, brp, bcol, bval, keys[g], first[g], vals[g],
+                      posmap[g], WTS, P[i], Poff[i], pcol, pval, count, GroupSync{mask});
 }
 
 template <typename VT>
@@ -291,10 +301,11 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     int *pcol = w.pcol.as<int>(), *count = w.count.as<int>();
     VT *pval = w.pval.as<VT>();
     if (ns > 0)
-        gustavson_warp<VT, kSmallP, kSmallTS, kSmallWarps><<<ceil_div_u(ns, kSmallWarps), kSmallWarps * 32, 0, st>>>(
-            rs, ns, P, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), pcol, pval, count);
+        gustavson_warp<VT, kSmallP, kSmallTS, kSmallWarps, kSmallTeam>
+            <<<ceil_div_u(ns, kSmallWarps * 32 / kSmallTeam), kSmallWarps * 32, 0, st>>>(
+                rs, ns, P, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), pcol, pval, count);
     if (nw > 0)
-        gustavson_warp<VT, kWarpP, kWarpTS, kWarpsPerCta><<<ceil_div_u(nw, kWarpsPerCta), kWarpsPerCta * 32, 0, st>>>(
+        gustavson_warp<VT, kWarpP, kWarpTS, kWarpsPerCta, 32><<<ceil_div_u(nw, kWarpsPerCta), kWarpsPerCta * 32, 0, st>>>(
             rw, nw, P, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), pcol, pval, count);
     if (nc > 0) {
         const size_t sm = (size_t)kCtaTS * (sizeof(VT) + 2 * sizeof(int)) + sizeof(int) * kCtaP;
