@@ -145,8 +145,10 @@ def make_matrix(rank: int, world: int, vt):
     return rp, col, val
 
 
-def cpu_reference_time(rp, col, val, x, max_s=20.0, reps=None):
-    """Seconds per apply of the reference's OpenMP CRS SpMV on all host threads."""
+def cpu_reference_time(rp, col, val, x, max_s=20.0, reps=None, warm=1):
+    """Seconds per apply of the reference's OpenMP CRS SpMV on all host threads
+    (reps applies after warm warm-up applies; reps chosen to fill about max_s
+    when not given)."""
     from oracle.oracle import Oracle, Reference, reference_available
     ncores = os.cpu_count() or 1
     if reference_available():
@@ -154,7 +156,7 @@ def cpu_reference_time(rp, col, val, x, max_s=20.0, reps=None):
         threads = R.set_threads(ncores)
         t1, _ = R.time_spmv_crs(rp, col, val, x, warm=1, reps=1)
         n = reps or max(2, min(50, int(max_s / max(t1, 1e-6))))
-        t, _ = R.time_spmv_crs(rp, col, val, x, warm=1, reps=n)
+        t, _ = R.time_spmv_crs(rp, col, val, x, warm=warm, reps=n)
         return t, threads, "reference", n
     O = Oracle()
     t0 = time.perf_counter()
@@ -177,16 +179,22 @@ def run_reference(args):
     x = np.random.default_rng(100).uniform(-1, 1, N_ROWS).astype(vt)
     from smaxkernels_b200.matrices import crs_bytes
     nbytes = crs_bytes(N_ROWS, len(col), N_ROWS, vbytes)
-    budget = max(10.0, min(120.0, 0.5 * max(args.steps, 1)))
-    t, threads, kind, n = cpu_reference_time(rp, col, val, x, max_s=budget)
+    # one step = one full apply of the reference's OpenMP kernel (~16 ms on 16
+    # host threads): exactly --steps applies after --warmup warm-up applies,
+    # unless that would take longer than 4 minutes (the single-thread port)
+    from oracle.oracle import reference_available
+    steps, warm = max(args.steps, 1), max(args.warmup, 0)
+    if not reference_available():
+        steps = min(steps, 20)
+    t, threads, kind, n = cpu_reference_time(rp, col, val, x, reps=steps, warm=warm)
     gbs = nbytes / t / 1e9
     line = {"impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": UNIT, "n_gpus": 0,
-            "steps": n, "warmup": 1, "ms_per_step": round(t * 1e3, 4), "higher_is_better": True,
+            "steps": n, "warmup": warm, "ms_per_step": round(t * 1e3, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": args.dtype,
             "data": "synthetic (seeded lognormal CRS matrix)",
             "config": config_dict(len(col), vbytes, 1),
             "cpu_baseline": {"value": round(gbs, 3), "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"{n} full applies of the workload after 1 warm-up"},
+                             "sample": f"{n} full applies of the workload after {warm} warm-up applies"},
             "e2e": {"value": round(gbs, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
