@@ -403,7 +403,7 @@ def wl_bcrs_spmv(b: Bench):
     from smaxkernels_b200 import matrices as M
     from smaxkernels_b200.matrices import crs_bytes
     vt, vb = np.float64, 8
-    rp, col, val = M.lognormal_random(1 << 22, seed=1, dtype=vt)
+    rp, col, val = M.lognormal_random(b.args.bcrs_rows, seed=1, dtype=vt)
     n, nnz = len(rp) - 1, len(col)
     x = M.uniform_vector(n, 100, vt)
     smax, k = b.kernel(KernelType.SPMV, vt, lambda k: k.set_mat_bcrs(True))
@@ -421,7 +421,7 @@ def wl_bcrs_spmv(b: Bench):
         t, reps = b.time(k.apply, budget_s=3.0)
     cpu = b.cpu(lambda: b.ref.time_spmv_bcrs(bc, x, False, warm=1, reps=5), nbytes,
                 "5 applies after 1 warm-up (reference OpenMP BCRS kernel)")
-    b.emit("bcrs4x4_spmv_f64_lognormal_4194304", "BCRS SpMV GB/s (stored bytes)", nbytes / t / 1e9, "GB/s", t,
+    b.emit(f"bcrs4x4_spmv_f64_lognormal_{n}", "BCRS SpMV GB/s (stored bytes)", nbytes / t / 1e9, "GB/s", t,
            reps, "f64", {"block": "4x4", "n_blocks": nb, "nnz": nnz, "l2": "inputs larger than L2 (no flush)"},
            clk.summary(), b.hbm(nbytes, t, "bcrs_stream_kernel"), cpu, launches=reps,
            crs_equivalent_gbs=round(crs_bytes(n, nnz, n, vb) / t / 1e9, 3), gflops=round(2 * nnz / t / 1e9, 3))
@@ -1073,6 +1073,7 @@ def main():
     ap.add_argument("--extra-dtype", default="both", choices=("both", "f64", "f32"),
                     help="scs_spmv / spmm workloads: value types to run")
     ap.add_argument("--spmm-k", default="16,64", help="spmm workload: vector counts")
+    ap.add_argument("--bcrs-rows", type=int, default=1 << 22, help="bcrs_spmv workload: rows of the matrix")
     ap.add_argument("--solver-side", type=int, default=2048, help="solvers workload: grid side of the large case")
     ap.add_argument("--solver-cases", default="all", choices=("all", "program", "large", "large_jacobi"),
                     help="solvers workload: the programs' 10x10 problem, the large grid (or only its Jacobi case), "
