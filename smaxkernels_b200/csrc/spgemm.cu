@@ -8,6 +8,8 @@
 // order.  C_n_rows = A_n_rows, C_n_cols = B_n_cols.
 //
 // Design.  One fused pass per row of A, binned by its product count P_i:
+//   * P_i <= 64:    a team of 8 lanes, hash table in shared memory (128 slots),
+//                   persistent teams that reset only the slots a row used;
 //   * P_i <= 256:   one warp, hash table in shared memory (512 slots);
 //   * P_i <= 4096:  one CTA, hash table in shared memory (8192 slots);
 //   * larger:       one CTA, hash table in a global workspace (2*P_i slots).
@@ -25,13 +27,15 @@
 
 #include <cub/device/device_scan.cuh>
 
+#include <algorithm>
+
 namespace smax {
 
 namespace {
 
 constexpr int kSmallP = 64, kSmallTS = 128;    // small-row path: products, table slots
 constexpr int kSmallTeam = 8;                  // lanes per row of the small-row path
-constexpr int kSmallWarps = 4;                 // warps per CTA: 16 rows, 2.3 KB of tables each
+constexpr int kSmallWarps = 4;                 // warps per CTA: 16 teams, 1.8 KB of tables each
 constexpr int kWarpP = 256, kWarpTS = 512;     // warp path
 constexpr int kCtaP = 4096, kCtaTS = 8192;     // CTA path
 constexpr int kCtaThreads = 512;
@@ -187,6 +191,102 @@ __global__ void __launch_bounds__(WARPS * 32) gustavson_warp(
                       posmap[g], WTS, P[i], Poff[i], pcol, pval, count, GroupSync{mask});
 }
 
+// The small-row path as persistent teams of G lanes: a team keeps its WTS-slot
+// table across the rows it takes (rows r, r + teams in the grid, ...), clears
+// it once, records the slots a row inserts, builds the first-touch map from
+// that list and resets only those slots afterwards -- a row of ~25 distinct
+// columns touches ~25 slots instead of clearing and scanning all WTS.  The
+// steps, the first-touch bookkeeping and the summation order are those of
+// gustavson_row.  Product indices (< WP <= 255) and slots (< WTS <= 128) are
+// stored in bytes.
+template <typename VT, int WP, int WTS, int WARPS, int G>
+__global__ void __launch_bounds__(WARPS * 32) gustavson_small(
+    const int *__restrict__ rows, int n_rows_bin, const long long *__restrict__ P, const long long *__restrict__ Poff,
+    const int *__restrict__ arp, const int *__restrict__ acol, const VT *__restrict__ aval,
+    const int *__restrict__ brp, const int *__restrict__ bcol, const VT *__restrict__ bval, int *__restrict__ pcol,
+    VT *__restrict__ pval, int *__restrict__ count) {
+    static_assert(WP <= 255 && WTS <= 128 && (WTS & (WTS - 1)) == 0, "byte-sized product indices and slots");
+    constexpr int TEAMS = WARPS * 32 / G;
+    __shared__ int keys[TEAMS][WTS];
+    __shared__ VT vals[TEAMS][WTS];
+    __shared__ unsigned char first[TEAMS][WTS];
+    __shared__ signed char posmap[TEAMS][WP];
+    __shared__ unsigned char used[TEAMS][WP];
+    __shared__ int nused[TEAMS];
+    const int g = threadIdx.x / G, t = (int)(threadIdx.x % G);
+    const int lane = (int)(threadIdx.x & 31);
+    const unsigned mask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((unsigned)lane & ~(unsigned)(G - 1)));
+    for (int h = t; h < WTS; h += G) {
+        keys[g][h] = -1;
+        vals[g][h] = VT(0);
+    }
+    if (t == 0) nused[g] = 0;
+    __syncwarp(mask);
+    const int64_t stride = (int64_t)gridDim.x * TEAMS;
+    for (int64_t r = (int64_t)blockIdx.x * TEAMS + g; r < n_rows_bin; r += stride) {  // uniform per team
+        const int i = rows[r];
+        const int Pi = (int)P[i];
+        const long long out_off = Poff[i];
+        for (int q = t; q < Pi; q += G) posmap[g][q] = -1;
+        __syncwarp(mask);
+        int base = 0;
+        for (int j = arp[i]; j < arp[i + 1]; ++j) {
+            const int c = acol[j];
+            const VT av = aval[j];
+            const int bs = brp[c], be = brp[c + 1];
+            for (int k = bs + t; k < be; k += G) {
+                const int col = bcol[k];
+                const VT prod = av * bval[k];
+                unsigned h = hash_col(col) & (WTS - 1);
+                while (true) {
+                    const int old = atomicCAS(&keys[g][h], -1, col);
+                    if (old == -1) {
+                        first[g][h] = (unsigned char)(base + (k - bs));
+                        used[g][atomicAdd(&nused[g], 1)] = (unsigned char)h;
+                        break;
+                    }
+                    if (old == col) break;
+                    h = (h + 1) & (WTS - 1);
+                }
+                vals[g][h] += prod;  // one product per slot per step: the (j, k) order
+            }
+            base += be - bs;
+            __syncwarp(mask);
+        }
+        const int nu = nused[g];
+        for (int u = t; u < nu; u += G) {
+            const int h = used[g][u];
+            posmap[g][first[g][h]] = (signed char)h;
+        }
+        __syncwarp(mask);
+        // ordered compaction of posmap: entries in first-touch order
+        int written = 0;
+        for (int q0 = 0; q0 < Pi; q0 += G) {
+            const int q = q0 + t;
+            const int h = q < Pi ? posmap[g][q] : -1;
+            const int take = h >= 0;
+            const unsigned bal = __ballot_sync(mask, take) & mask;
+            const int before = __popc(bal & ((1u << lane) - 1u));
+            if (take) {
+                pcol[out_off + written + before] = keys[g][h];
+                pval[out_off + written + before] = vals[g][h];
+            }
+            written += __popc(bal);
+        }
+        __syncwarp(mask);
+        for (int u = t; u < nu; u += G) {
+            const int h = used[g][u];
+            keys[g][h] = -1;
+            vals[g][h] = VT(0);
+        }
+        if (t == 0) {
+            count[i] = written;
+            nused[g] = 0;
+        }
+        __syncwarp(mask);
+    }
+}
+
 template <typename VT>
 __global__ void __launch_bounds__(kCtaThreads) gustavson_cta(
     const int *__restrict__ rows, int n_rows_bin, const long long *__restrict__ P, const long long *__restrict__ Poff,
@@ -300,10 +400,21 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     w.pval.ensure(sizeof(VT) * (total_p ? total_p : 1));
     int *pcol = w.pcol.as<int>(), *count = w.count.as<int>();
     VT *pval = w.pval.as<VT>();
-    if (ns > 0)
-        gustavson_warp<VT, kSmallP, kSmallTS, kSmallWarps, kSmallTeam>
-            <<<ceil_div_u(ns, kSmallWarps * 32 / kSmallTeam), kSmallWarps * 32, 0, st>>>(
-                rs, ns, P, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), pcol, pval, count);
+    if (ns > 0) {
+        // persistent teams: as many CTAs as are resident at once, or fewer
+        auto kern = gustavson_small<VT, kSmallP, kSmallTS, kSmallWarps, kSmallTeam>;
+        static int per_sm[2] = {0, 0};
+        int &ps = per_sm[sizeof(VT) == 8 ? 1 : 0];
+        if (ps == 0) {
+            SMAX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, kern, kSmallWarps * 32, 0));
+            if (ps < 1) ps = 1;
+        }
+        const int64_t teams_per_cta = kSmallWarps * 32 / kSmallTeam;
+        const int64_t need = (ns + teams_per_cta - 1) / teams_per_cta;
+        const unsigned grid = (unsigned)std::min<int64_t>(need, (int64_t)ps * sm_count());
+        kern<<<grid, kSmallWarps * 32, 0, st>>>(rs, ns, P, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(),
+                                                B.val.as<VT>(), pcol, pval, count);
+    }
     if (nw > 0)
         gustavson_warp<VT, kWarpP, kWarpTS, kWarpsPerCta, 32><<<ceil_div_u(nw, kWarpsPerCta), kWarpsPerCta * 32, 0, st>>>(
             rw, nw, P, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), pcol, pval, count);
