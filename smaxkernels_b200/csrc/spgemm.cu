@@ -44,20 +44,22 @@ constexpr int kBins = 4;
 
 __device__ __forceinline__ unsigned hash_col(int c) { return (unsigned)c * 0x9E3779B1u; }
 
-// product count of every row of A
+constexpr int kRowGroup = 8;  // lanes per row of the per-row helper passes (short rows)
+
+// product count of every row of A (kRowGroup lanes per row)
 __global__ void row_products(const int *__restrict__ arp, const int *__restrict__ acol, const int *__restrict__ brp,
                              int64_t n, long long *__restrict__ P) {
-    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (i >= n) return;
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kRowGroup;
+    const int lane = threadIdx.x % kRowGroup;
     long long s = 0;
-    for (int j = arp[i] + lane; j < arp[i + 1]; j += 32) {
-        const int c = acol[j];
-        s += brp[c + 1] - brp[c];
-    }
+    if (i < n)
+        for (int j = arp[i] + lane; j < arp[i + 1]; j += kRowGroup) {
+            const int c = acol[j];
+            s += brp[c + 1] - brp[c];
+        }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) P[i] = s;
+    for (int o = kRowGroup / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (i < n && lane == 0) P[i] = s;
 }
 
 // rows into four lists by product count (small-row warp, warp, CTA and global
@@ -332,12 +334,12 @@ template <typename VT>
 __global__ void compact_kernel(const int *__restrict__ crp, const long long *__restrict__ Poff, int64_t n,
                                const int *__restrict__ pcol, const VT *__restrict__ pval, int *__restrict__ ccol,
                                VT *__restrict__ cval) {
-    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kRowGroup;
+    const int lane = threadIdx.x % kRowGroup;
     if (i >= n) return;
     const int s = crp[i], len = crp[i + 1] - s;
     const long long o = Poff[i];
-    for (int t = lane; t < len; t += 32) {
+    for (int t = lane; t < len; t += kRowGroup) {
         ccol[s + t] = pcol[o + t];
         cval[s + t] = pval[o + t];
     }
@@ -379,7 +381,7 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     long long *P = w.P.as<long long>(), *Poff = w.Poff.as<long long>();
     SMAX_CUDA(cudaMemsetAsync(w.counts.p, 0, sizeof(int) * 4, st));
     if (n > 0) {
-        row_products<<<ceil_div_u((uint64_t)n * 32, 256), 256, 0, st>>>(A.rp(), A.ci(), B.rp(), n, P);
+        row_products<<<ceil_div_u((uint64_t)n * kRowGroup, 256), 256, 0, st>>>(A.rp(), A.ci(), B.rp(), n, P);
         bin_rows<<<ceil_div_u(n, 256), 256, 0, st>>>(P, n, w.lists.as<int>(), w.counts.as<int>());
         SMAX_CUDA(cudaGetLastError());
     }
@@ -455,7 +457,7 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     C.val.ensure(sizeof(VT) * (nnz ? nnz : 1));
     SMAX_CUDA(cudaEventRecord(ev[3], st));
     if (n > 0) {
-        compact_kernel<VT><<<ceil_div_u((uint64_t)n * 32, 256), 256, 0, st>>>(C.rp(), Poff, n, pcol, pval,
+        compact_kernel<VT><<<ceil_div_u((uint64_t)n * kRowGroup, 256), 256, 0, st>>>(C.rp(), Poff, n, pcol, pval,
                                                                               C.col.as<int>(), C.val.as<VT>());
         SMAX_CUDA(cudaGetLastError());
     }

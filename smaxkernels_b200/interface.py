@@ -463,6 +463,24 @@ class Utils:
 
 
     # -- level sets and permutations (src/utils/permutations.hpp) --------------
+    def print_timers(self, file=None):
+        """Utils::print_timers (src/utils.hpp:24): every registered kernel's
+        initialize / apply / finalize stopwatches and their total (SpGEMM also
+        its phases), in seconds."""
+        import sys
+        out = file or sys.stdout
+        for name, k in self._iface._kernels.items():
+            parts = ["initialize", "apply", "finalize"]
+            t = {p: k.timer(p) for p in parts}
+            print(f"+{'-' * 19} SMAX Timer {'-' * 19}+", file=out)
+            print(f"Total time in '{name}': {sum(t.values()):.3e} [s]", file=out)
+            for p_ in parts:
+                print(f"| {p_.capitalize()} time: {t[p_]:.3e} [s]", file=out)
+            if k.kernel_type == KernelType.SPGEMM:
+                for p_ in ("Symbolic_Setup", "Fused_Gustavson", "Alloc_C", "Compress"):
+                    print(f"|   {p_}: {k.timer(p_):.3e} [s]", file=out)
+            print(f"+{'-' * 50}+", file=out)
+
     def read_mtx(self, path: str, dtype=np.float64):
         """A Matrix Market file as CRS (n_rows, n_cols, nnz, row_ptr, col, val),
         read as the reference's examples read it (smax_utils_read_mtx)."""

@@ -82,6 +82,11 @@ def test_offsets_and_repeated_runs():
     assert normwise(Y[:n], O.spmv_crs(rp, col, val, X[n:])) <= 1e-12
     assert normwise(Y[n:], O.spmv_crs(rp, col, val, X[:n])) <= 1e-12
     assert k.timer("apply") > 0
+    import io
+    buf = io.StringIO()
+    smax.utils.print_timers(file=buf)
+    text = buf.getvalue()
+    assert "Total time in 'k'" in text and "Apply time" in text
     smax.close()
 
 
