@@ -454,8 +454,9 @@ smax_status smax_solver_create(smax_solver *out, int kind, int float_type, uint6
                                const void *row_ptr, const void *col, const void *val);
 smax_status smax_solver_solve(smax_solver s, const void *b, void *x, const smax_solver_opts *opts,
                               smax_solver_stats *stats, void *stream);
-/* The residuals of the last solve in the order they were measured: writes
- * min(cap, n_checks) of them to out (host array) and n_checks to *count. */
+/* The residuals of the last solve in the order they were measured (the first
+ * 2^20 of them): writes min(cap, n_checks, 2^20) values to out (host array)
+ * and n_checks to *count. */
 smax_status smax_solver_get_history(smax_solver s, double *out, int cap, int *count);
 smax_status smax_solver_destroy(smax_solver s);
 

@@ -43,6 +43,7 @@ namespace smax {
 namespace {
 
 constexpr int kRowThreads = 256;
+constexpr int64_t kMaxHistory = 1 << 20;  // residuals recorded per solve, at most
 
 struct SolverState {
     unsigned long long norm_bits;  // running maximum of the residual being measured
@@ -710,9 +711,12 @@ struct smax_solver_s {
             last_checks = 0;
             return;
         }
-        if (n_full + 1 > hist_cap) {
-            hist.alloc(sizeof(double) * (n_full + 1));
-            hist_cap = n_full + 1;
+        // the residual history keeps at most kMaxHistory entries (the count
+        // of checks is still exact)
+        const int want = (int)std::min<int64_t>((int64_t)n_full + 1, kMaxHistory);
+        if (want > hist_cap) {
+            hist.alloc(sizeof(double) * want);
+            hist_cap = want;
         }
         SMAX_CUDA(cudaMemcpyAsync(b.p, b_in, vb, cudaMemcpyDefault, st));
         SMAX_CUDA(cudaMemcpyAsync(x0.p, x_inout, vb, cudaMemcpyDefault, st));

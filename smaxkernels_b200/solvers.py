@@ -77,9 +77,9 @@ class Solver:
         """The residuals of the last solve, in the order they were measured."""
         count = C.c_int(0)
         check(lib.smax_solver_get_history(self._h, None, 0, C.byref(count)))
-        out = np.zeros(count.value, dtype=np.float64)
-        if count.value:
-            check(lib.smax_solver_get_history(self._h, out.ctypes.data_as(C.c_void_p), count.value,
+        out = np.zeros(min(count.value, 1 << 20), dtype=np.float64)  # the first 2^20 are kept
+        if len(out):
+            check(lib.smax_solver_get_history(self._h, out.ctypes.data_as(C.c_void_p), len(out),
                                               C.byref(count)))
         return out
 
