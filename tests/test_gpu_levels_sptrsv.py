@@ -142,12 +142,9 @@ def test_perm_laplace2d(typ):
         np.testing.assert_array_equal(perm, operm)
 
 
-def test_perm_colourings_unsupported_and_unknown_type():
-    from smaxkernels_b200 import SmaxError, _lib
+def test_perm_unknown_type():
+    from smaxkernels_b200 import SmaxError
     rp, col, val = rand_crs(50, 4, 1)
-    with pytest.raises(SmaxError) as e:
-        gpu_perm(rp, col, "PC")
-    assert e.value.code == _lib.ERR_UNSUPPORTED
     with pytest.raises(SmaxError, match="does not exist"):
         gpu_perm(rp, col, "XYZ")
 
