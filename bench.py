@@ -436,13 +436,14 @@ def wl_spmm(b: Bench):
     dts = (np.float64, np.float32) if b.args.extra_dtype == "both" else \
         ((np.float64,) if b.args.extra_dtype == "f64" else (np.float32,))
     ks = [int(v) for v in b.args.spmm_k.split(",")]
+    variants = [int(v) for v in b.args.spmm_variants.split(",")]
     for vt in dts:
         vb = np.dtype(vt).itemsize
         rp, col, val = M.stencil27(128, dtype=vt)
         n, nnz = len(rp) - 1, len(col)
-        for kv in ks:
+        for kv, var in [(kv, var) for kv in ks for var in variants]:
             X = np.random.default_rng(2).uniform(-1, 1, n * kv).astype(vt)
-            smax, k = b.kernel(KernelType.SPMM, vt, lambda k: k.set_vec_row_major(True))
+            smax, k = b.kernel(KernelType.SPMM, vt, lambda k: (k.set_vec_row_major(True), k.set_spmv_variant(var)))
             Xd, Yd = b.dev(X), b.zeros(n * kv, vt)
             k.register_A(n, n, nnz, col, rp, val)
             k.register_B(n, kv, Xd)
@@ -453,11 +454,14 @@ def wl_spmm(b: Bench):
             with b.clocks() as clk:
                 t, reps = b.time(k.apply)
             cpu = b.cpu(lambda: b.ref.time_spmm(rp, col, val, X, kv, True, warm=1, reps=5), nbytes,
-                        "5 applies after 1 warm-up (reference OpenMP row-major SpMM)")
-            b.emit(f"spmm_rowmajor_k{kv}_{_dt(vt)}_stencil27_128", "SpMM GB/s", nbytes / t / 1e9, "GB/s", t, reps,
-                   _dt(vt), {"n_rows": n, "nnz": nnz, "k": kv, "layout": "row-major X, Y",
-                             "l2": "inputs larger than L2 (no flush)"},
-                   clk.summary(), b.hbm(nbytes, t, "spmm_row_major_kernel"), cpu, launches=reps,
+                        "5 applies after 1 warm-up (reference OpenMP row-major SpMM)") if var == variants[0] else None
+            vname = {0: "", 1: "_grid", 2: "_walk"}[var]
+            b.emit(f"spmm_rowmajor_k{kv}_{_dt(vt)}_stencil27_128{vname}", "SpMM GB/s", nbytes / t / 1e9, "GB/s", t,
+                   reps, _dt(vt), {"n_rows": n, "nnz": nnz, "k": kv, "layout": "row-major X, Y",
+                                   "l2": "inputs larger than L2 (no flush)",
+                                   "kernel": "spmm_row_major_kernel" if var == 1 else "spmm_walk_kernel"},
+                   clk.summary(), b.hbm(nbytes, t, "spmm_row_major_kernel" if var == 1 else "spmm_walk_kernel"),
+                   cpu, launches=reps,
                    gflops=round(2 * nnz * kv / t / 1e9, 3))
             smax.close()
             del Xd, Yd
@@ -514,10 +518,10 @@ def wl_sptrsv(b: Bench):
     n, nnz = len(rp) - 1, len(col)
     n_lv = 2 * side - 1
     rhs = M.uniform_vector(n, 3)
-    names = {1: "per_level", 2: "merged", 3: "graph", 4: "persistent"}
-    results = {}
+    names = {1: "per_level", 2: "merged", 3: "graph", 4: "persistent", 5: "syncfree"}
+    results, xs = {}, {}
     modes = [int(m) for m in b.args.tri_modes.split(",")]
-    for mode in [m for m in (1, 2, 3, 4) if m in modes]:
+    for mode in [m for m in (1, 2, 3, 4, 5) if m in modes]:
         smax, k = b.kernel(KernelType.SPTRSV, vt, lambda k: k.set_solve_mode(mode))
         xd, bd = b.zeros(n, vt), b.dev(rhs)
         k.register_A(n, n, nnz, col.copy(), rp, val.copy())
@@ -529,6 +533,8 @@ def wl_sptrsv(b: Bench):
         with b.clocks() as clk:
             t, reps = b.time(k.apply, budget_s=2.0, max_reps=100)
         results[mode] = t
+        xs[mode] = xd.clone()
+        same = bool(b.torch.equal(xs[mode], xs[3])) if 3 in xs else None
         cpu = None
         if mode == 3:
             cpu = b.cpu(lambda: b.ref.time_sptrsv(rp, col, val, rhs, warm=1, reps=3)[0], nbytes,
@@ -537,7 +543,7 @@ def wl_sptrsv(b: Bench):
                reps, "f64", {"n_rows": n, "nnz": nnz, "levels": n_lv, "scheme": names[mode]}, clk.summary(),
                b.hbm(nbytes, t, "level_kernel/segment_kernel"), cpu,
                launches=n_lv * reps if mode == 1 else (reps if mode == 4 else None),
-               us_per_level=round(t * 1e6 / n_lv, 4))
+               us_per_level=round(t * 1e6 / n_lv, 4), bitwise_equal_to_graph=same)
         smax.close()
     if b.args.tri_natural_only:
         return
@@ -554,7 +560,8 @@ def wl_sptrsv(b: Bench):
     lrp, lcol, lval = M.lower_triangle(prp, pcol, pval)
     lvl = np.array([smax.get_level_ptr_at(i) for i in range(smax.get_n_levels() + 1)], np.int32)
     nl = len(lvl) - 1
-    for mode in (3, 4):
+    xs = {}
+    for mode in (3, 4, 5):
         smax.register_kernel(f"p{mode}", KernelType.SPTRSV, *b_types(vt))
         k = smax.kernel(f"p{mode}")
         k.set_mat_perm(True)
@@ -568,6 +575,8 @@ def wl_sptrsv(b: Bench):
         nbytes = _tri_bytes(n, len(lcol), vb)
         with b.clocks() as clk:
             t, reps = b.time(k.apply, budget_s=2.0, max_reps=200)
+        xs[mode] = xd.clone()
+        same = bool(b.torch.equal(xs[mode], xs[3])) if 3 in xs else None
         cpu = None
         if mode == 3:
             cpu = b.cpu(lambda: b.ref.time_sptrsv(lrp, lcol, lval, rhs, levels=lvl, warm=1, reps=5)[0], nbytes,
@@ -576,7 +585,8 @@ def wl_sptrsv(b: Bench):
                reps, "f64", {"n_rows": n, "nnz": len(lcol), "levels": nl, "scheme": names[mode],
                              "ordering": "random symmetric permutation (seed 3), RS level order"},
                clk.summary(), b.hbm(nbytes, t, "level_kernel/segment_kernel"), cpu,
-               launches=reps if mode == 4 else None, us_per_level=round(t * 1e6 / max(nl, 1), 4))
+               launches=reps if mode == 4 else None, us_per_level=round(t * 1e6 / max(nl, 1), 4),
+               bitwise_equal_to_graph=same)
     smax.close()
     # SpTRSM, k = 32 right-hand sides, row-major
     kv = 32
@@ -1068,11 +1078,13 @@ def main():
     ap.add_argument("--workload", default="crs_spmv", choices=("crs_spmv", "all") + EXTRA_WORKLOADS,
                     help="crs_spmv (the headline line) or another workload of the hot path (1 GPU)")
     ap.add_argument("--tri-side", type=int, default=2048, help="sptrsv workload: grid side of the Laplacian")
-    ap.add_argument("--tri-modes", default="1,2,3,4", help="sptrsv workload: solve modes of the natural case")
+    ap.add_argument("--tri-modes", default="1,2,3,4,5", help="sptrsv workload: solve modes of the natural case")
     ap.add_argument("--tri-natural-only", action="store_true", help="sptrsv workload: natural order only")
     ap.add_argument("--extra-dtype", default="both", choices=("both", "f64", "f32"),
                     help="scs_spmv / spmm workloads: value types to run")
     ap.add_argument("--spmm-k", default="16,64", help="spmm workload: vector counts")
+    ap.add_argument("--spmm-variants", default="0",
+                    help="spmm workload: row-major kernels (0 default, 1 all-rows grid, 2 per-SM row walks)")
     ap.add_argument("--bcrs-rows", type=int, default=1 << 22, help="bcrs_spmv workload: rows of the matrix")
     ap.add_argument("--solver-side", type=int, default=2048, help="solvers workload: grid side of the large case")
     ap.add_argument("--solver-cases", default="all", choices=("all", "program", "large", "large_jacobi"),

@@ -89,7 +89,8 @@ typedef int smax_status;
 #define SMAX_FLAG_KERNEL_IMPL 7        /* set_kernel_implementation(SpMVType) */
 #define SMAX_FLAG_DEVICE_POINTERS 8    /* B and C registered as device pointers */
 #define SMAX_FLAG_A_DIRTY 9            /* re-upload A at the next initialize */
-#define SMAX_FLAG_SPMV_VARIANT 10      /* CRS SpMV kernel: 0 auto, 1 warp-stream, 2 row-tile */
+#define SMAX_FLAG_SPMV_VARIANT 10      /* CRS SpMV kernel: 0 auto, 1 warp-stream, 2 row-tile; row-major SpMM:
+                                          0 auto (= 1), 1 a grid of all rows, 2 one CTA per SM walking a row range */
 #define SMAX_FLAG_SOLVE_MODE 11        /* SpTRSV/SpTRSM launch scheme, one of SMAX_SOLVE_* */
 #define SMAX_FLAG_LEVEL_MERGE 12       /* levels with <= this many rows*rhs run merged in one CTA (0: never) */
 #define SMAX_FLAG_SPIN_LIMIT 13        /* polls (x 1000) before a persistent solve's grid barrier times out */
@@ -105,6 +106,8 @@ typedef int smax_status;
 #define SMAX_SOLVE_MERGED 2      /* narrow levels merged into single-CTA runs, no graph */
 #define SMAX_SOLVE_GRAPH 3       /* the merged launch sequence captured into a CUDA graph */
 #define SMAX_SOLVE_PERSISTENT 4  /* one cooperative launch, bounded grid barrier per level (SpTRSV, k = 1) */
+#define SMAX_SOLVE_SYNCFREE 5    /* one launch, no level barriers: each row waits (bounded) on the rows it reads
+                                    (SpTRSV, k = 1; falls back to SMAX_SOLVE_MERGED where it does not apply) */
 
 typedef struct smax_ctx_s *smax_ctx;
 typedef struct smax_kernel_s *smax_kernel;
@@ -240,7 +243,7 @@ smax_status smax_kernel_get_refine_stats(smax_kernel k, int *steps, double *last
  * a hash of the pattern); a later kernel with the same matrix takes them from
  * the cache.  Overwrites the output operand (C for SpMV, B for solves). */
 typedef struct smax_tuning {
-    int spmv_variant; /* SMAX_FLAG_SPMV_VARIANT chosen (SpMV) */
+    int spmv_variant; /* SMAX_FLAG_SPMV_VARIANT chosen (SpMV, row-major SpMM) */
     int solve_mode;   /* SMAX_SOLVE_* chosen (SpTRSV / SpTRSM) */
     int level_merge;  /* SMAX_FLAG_LEVEL_MERGE chosen (SpTRSV / SpTRSM) */
     int sweep_cluster; /* SMAX_FLAG_SWEEP_CLUSTER chosen (SpTRSV) */

@@ -173,7 +173,7 @@ void spmm_upload(smax_kernel_s *k) {
 template <typename VT> void spmm_apply_t(smax_kernel_s *k, const VT *X, VT *Y) {
     const int64_t kk = (int64_t)(k->B.n_cols ? k->B.n_cols : 1);
     if (k->f_row_major) {
-        crs_spmm_row_major<VT>(k->dA, kk, X, Y, k->stream);
+        crs_spmm_row_major<VT>(k->dA, kk, X, Y, k->stream, &k->spmm_plan, k->spmv_variant);
     } else {
         // column-major: the reference uses A's n_rows as the leading dimension
         // of both X and Y (src/kernels/spmm/spmm_cpu/spmm_cpu_crs_impl.hpp:29,44)
@@ -227,6 +227,13 @@ template <typename VT> void tri_apply_t(smax_kernel_s *k, const VT *Bv, VT *Xv) 
         tri_solve_persistent<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, dstatus(k), k->persist_scratch,
                                  k->force_timeout, k->spin_limit, k->stream);
         return;
+    }
+    if (k->solve_mode == SMAX_SOLVE_SYNCFREE) {
+        require(kk == 1, SMAX_ERR_UNSUPPORTED, "the sync-free solve handles one right-hand side");
+        if (tri_solve_syncfree<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, k->vals_version, k->sf_ctl, k->spin_limit,
+                                   k->force_timeout, dstatus(k), k->stream))
+            return;
+        // not applicable to this matrix or these operands: the merged solve
     }
     if (k->solve_mode == SMAX_SOLVE_AUTO || k->solve_mode == SMAX_SOLVE_GRAPH)
         tri_solve_graph<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, kk, rm, ld, merge, k->vals_version, k->stream);
@@ -661,7 +668,7 @@ smax_status smax_kernel_set_flag(smax_kernel k, int flag, int value) {
             break;
         case SMAX_FLAG_TEST_FORCE_TIMEOUT: kk->force_timeout = v; break;
         case SMAX_FLAG_SOLVE_MODE:
-            require(value >= SMAX_SOLVE_AUTO && value <= SMAX_SOLVE_PERSISTENT, SMAX_ERR_BAD_ARG,
+            require(value >= SMAX_SOLVE_AUTO && value <= SMAX_SOLVE_SYNCFREE, SMAX_ERR_BAD_ARG,
                     "unknown solve mode");
             kk->solve_mode = value;
             break;

@@ -98,6 +98,15 @@ void tune_kernel(smax_kernel_s *k, smax_tuning &r) {
             if (t < best) { best = t; r.spmv_variant = v; }
         }
         k->spmv_variant = r.spmv_variant;
+    } else if (k->ktype == SMAX_KERNEL_SPMM && k->f_row_major) {
+        // row-major SpMM: all-rows grid (1) or per-SM row walks (2)
+        for (int v : {1, 2}) {
+            k->spmv_variant = v;
+            const double t = time_apply(k);
+            ++r.n_candidates;
+            if (t < best) { best = t; r.spmv_variant = v; }
+        }
+        k->spmv_variant = r.spmv_variant;
     } else if (is_tri(k)) {
         struct Cand { int mode, merge; bool cluster; };
         std::vector<Cand> cands;
@@ -107,8 +116,10 @@ void tune_kernel(smax_kernel_s *k, smax_tuning &r) {
             cands.push_back({SMAX_SOLVE_GRAPH, 4096, true});
             cands.push_back({SMAX_SOLVE_GRAPH, 16384, true});
         }
-        if (k->ktype == SMAX_KERNEL_SPTRSV && one_rhs && k->refine_steps == 0)
+        if (k->ktype == SMAX_KERNEL_SPTRSV && one_rhs && k->refine_steps == 0) {
             cands.push_back({SMAX_SOLVE_PERSISTENT, 0, false});
+            cands.push_back({SMAX_SOLVE_SYNCFREE, 0, false});
+        }
         for (const Cand &c : cands) {
             k->solve_mode = c.mode;
             k->level_merge = c.merge;
@@ -117,7 +128,7 @@ void tune_kernel(smax_kernel_s *k, smax_tuning &r) {
             try {
                 t = time_apply(k);
             } catch (const Error &e) {
-                // a persistent solve whose grid barrier timed out is not a candidate
+                // a persistent or sync-free solve whose wait timed out is not a candidate
                 if (e.code != SMAX_ERR_TIMEOUT) throw;
                 continue;
             }
@@ -137,6 +148,8 @@ void tune_kernel(smax_kernel_s *k, smax_tuning &r) {
 void apply_choice(smax_kernel_s *k, const smax_tuning &t) {
     if (k->ktype == SMAX_KERNEL_SPMV && !k->f_scs && !k->f_bcrs) {
         if (t.spmv_variant != k->spmv_variant) build_crs_plans(k);
+        k->spmv_variant = t.spmv_variant;
+    } else if (k->ktype == SMAX_KERNEL_SPMM && k->f_row_major) {
         k->spmv_variant = t.spmv_variant;
     } else if (is_tri(k)) {
         k->solve_mode = t.solve_mode;

@@ -111,6 +111,7 @@ struct smax_kernel_s {
     smax::DevBuf dB, dC;
     smax::CrsTilePlan crs_plan;
     smax::CrsStreamPlan crs_stream;
+    smax::SpmmPlan spmm_plan;  // row ranges of the row-major SpMM walk
     int spmv_variant = 0;  // 0 auto, 1 warp-stream, 2 row-tile
     smax::DevBuf status;   // smax::DevStatus
 
@@ -131,6 +132,7 @@ struct smax_kernel_s {
     bool force_timeout = false;     // test knob of the persistent solve's grid barrier
     long long spin_limit = 20000000; // polls before a grid barrier gives up
     smax::DevBuf persist_scratch;
+    smax::DevBuf sf_ctl;  // task counter, abort flag of the sync-free solve
 
     // versions of the device copy of A: pattern + values (each upload), values
     // alone (each upload or value update)

@@ -84,7 +84,7 @@ __global__ void fill_kernel(const int *__restrict__ rp, const int *__restrict__ 
                             const int *__restrict__ plev, const int *__restrict__ pos_of_row,
                             const Level *__restrict__ lv, const int *__restrict__ seg_pos,
                             const int2 *__restrict__ geo, int *__restrict__ psrc, VT *__restrict__ pval,
-                            VT *__restrict__ pinv, int *needs_init) {
+                            VT *__restrict__ pinv, int *needs_init, bool row_src) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
         const int s = plev[p];
@@ -109,7 +109,7 @@ __global__ void fill_kernel(const int *__restrict__ rp, const int *__restrict__ 
                     const int owner = (tq % G) / g2.y;
                     code = -((owner << kRingShift) | (q & (kRing - 1))) - 1;
                 }
-                psrc[idx] = code;
+                psrc[idx] = row_src ? ci[j0 + i] : code;
                 pval[idx] = val[j0 + i];
             } else {
                 psrc[idx] = kPad;
@@ -339,6 +339,138 @@ __global__ void __launch_bounds__(T, 1)
     }
 }
 
+// ------------------------------------------------------------ sync-free --
+constexpr int kSfThreads = 256;
+constexpr int kSfChunk = 32;  // warp tasks a CTA claims at once
+constexpr int kSfEnts = 4;    // entries of a row loaded before its first wait
+
+// "not solved yet": signalling-NaN patterns; arithmetic never returns a
+// signalling NaN, so a computed solution is never mistaken for one
+template <typename VT> struct Pending;
+template <> struct Pending<double> {
+    static constexpr unsigned long long bits = 0x7FF5A5A5A5A5A5A5ull;
+    __device__ static bool is(double v) { return (unsigned long long)__double_as_longlong(v) == bits; }
+    __device__ static double value() { return __longlong_as_double((long long)bits); }
+};
+template <> struct Pending<float> {
+    static constexpr unsigned bits = 0x7FA5A5A5u;
+    __device__ static bool is(float v) { return (unsigned)__float_as_uint(v) == bits; }
+    __device__ static float value() { return __uint_as_float(bits); }
+};
+
+__device__ __forceinline__ double ld_relaxed(const double *p) {
+    double v;
+    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float ld_relaxed(const float *p) {
+    float v;
+    asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(double *p, double v) {
+    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(float *p, float v) {
+    asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+
+// The value at p once it is no longer pending.  Bounded: after `limit` polls
+// the wait records SMAX_ERR_TIMEOUT and raises the abort flag; once the flag
+// is up every wait returns NaN (checked every 64 polls).
+template <typename VT>
+__device__ __noinline__ VT wait_solved(const VT *p, long long limit, int *abort_flag, DevStatus *st) {
+    for (long long it = 1;; ++it) {
+        __nanosleep(64);
+        const VT v = ld_relaxed(p);
+        if (!Pending<VT>::is(v)) return v;
+        if ((it & 63) == 0 && *(volatile int *)abort_flag) return VT(NAN);
+        if (it >= limit) {
+            report(st, SMAX_ERR_TIMEOUT, it);
+            atomicExch(abort_flag, 1);
+            return VT(NAN);
+        }
+    }
+}
+
+template <typename VT>
+__device__ __forceinline__ VT solved(const VT *p, long long limit, int *abort_flag, DevStatus *st) {
+    const VT v = ld_relaxed(p);
+    return Pending<VT>::is(v) ? wait_solved(p, limit, abort_flag, st) : v;
+}
+
+// X := pending; ctl[0] (task counter) = ctl[1] (abort flag) = 0; ctl[4..] pending
+template <typename VT>
+__global__ void sf_reset_kernel(VT *__restrict__ X, int64_t n, int *__restrict__ ctl) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i0 == 0) {
+        ctl[0] = 0;
+        ctl[1] = 0;
+        *reinterpret_cast<VT *>(ctl + 4) = Pending<VT>::value();
+    }
+    for (int64_t i = i0; i < n; i += stride) X[i] = Pending<VT>::value();
+}
+
+// ctl: [0] task counter, [1] abort flag, [4..] a word that stays pending
+// (waited on by the first row when `never` is set: the test knob)
+template <typename VT>
+__global__ void __launch_bounds__(kSfThreads)
+    syncfree_kernel(const Level *__restrict__ lv, const int2 *__restrict__ tasks, int n_tasks,
+                    const int *__restrict__ prow, const int *__restrict__ psrc, const VT *__restrict__ pval,
+                    const VT *__restrict__ pinv, const VT *__restrict__ B, VT *X, int *ctl, long long limit,
+                    bool never, DevStatus *st) {
+    __shared__ int chunk_sh;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int *abort_flag = ctl + 1;
+    while (true) {
+        if (threadIdx.x == 0) chunk_sh = atomicAdd(ctl, kSfChunk);
+        __syncthreads();
+        const int c0 = chunk_sh;
+        __syncthreads();  // chunk_sh is rewritten on the next turn
+        if (c0 >= n_tasks) return;
+        const int c1 = min(c0 + kSfChunk, n_tasks);
+        for (int ti = c0 + warp; ti < c1; ti += kSfThreads / 32) {
+            const int2 tk = tasks[ti];
+            const Level L = load_level(lv, tk.x);
+            const int t = tk.y + lane;
+            if (t >= L.m) continue;
+            // every load that does not wait goes out first
+            int src[kSfEnts];
+            VT v[kSfEnts];
+#pragma unroll
+            for (int i = 0; i < kSfEnts; ++i) {
+                src[i] = kPad;
+                if (i < L.w) {
+                    const long long idx = L.base + (long long)i * L.m + t;
+                    src[i] = psrc[idx];
+                    v[i] = pval[idx];
+                }
+            }
+            const int p = L.pos + t;
+            const int r = prow[p];
+            const VT bi = B[r], inv = pinv[p];
+            VT sum = VT(0);
+            if (never && ti == 0 && lane == 0)
+                sum += VT(0) * solved(reinterpret_cast<const VT *>(ctl + 4), limit, abort_flag, st);
+            bool more = true;
+#pragma unroll
+            for (int i = 0; i < kSfEnts; ++i) {
+                if (src[i] == kPad) { more = false; break; }
+                sum += v[i] * solved(X + src[i], limit, abort_flag, st);
+            }
+            if (more)
+                for (int i = kSfEnts; i < L.w; ++i) {
+                    const long long idx = L.base + (long long)i * L.m + t;
+                    const int sc = psrc[idx];
+                    if (sc == kPad) break;
+                    sum += pval[idx] * solved(X + sc, limit, abort_flag, st);
+                }
+            st_relaxed(X + r, (bi - sum) * inv);
+        }
+    }
+}
+
 template <typename VT, int T> void set_smem_attr_t() {
     SMAX_CUDA(cudaFuncSetAttribute(sweep_kernel<VT, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(kRing * sizeof(VT))));
@@ -427,7 +559,7 @@ void launch_run(const LevelPack &pk, int s0, int s1, const int *psrc, const VT *
 
 bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *val, const void *D, int vbytes,
                       int64_t n, const int *order, const std::vector<int> &src_begin, const std::vector<int> &count,
-                      const std::vector<int> &seg_begin, bool allow_cluster, cudaStream_t st) {
+                      const std::vector<int> &seg_begin, bool allow_cluster, cudaStream_t st, bool row_sources) {
     const int L = (int)count.size();
     if ((int)src_begin.size() != L || (int)seg_begin.size() != L) fail(SMAX_ERR_STATE, "inconsistent sweep steps");
     pk = LevelPack();
@@ -442,8 +574,11 @@ bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *v
     const size_t nb = sizeof(int) * (n > 0 ? n : 1);
     pk.prow.alloc(nb);
     pk.pinv.alloc((size_t)vbytes * (n > 0 ? n : 1));
-    pk.bp.alloc((size_t)vbytes * (n > 0 ? n : 1));
-    pk.xp.alloc((size_t)vbytes * (n > 0 ? n : 1));
+    pk.row_sources = row_sources;
+    // a sync-free solve reads B and writes X in the caller's numbering
+    const int64_t nv = row_sources ? 1 : (n > 0 ? n : 1);
+    pk.bp.alloc((size_t)vbytes * nv);
+    pk.xp.alloc((size_t)vbytes * nv);
     if (n == 0 || L == 0) {
         pk.lv.alloc(sizeof(Level));
         pk.psrc.alloc(sizeof(int));
@@ -488,6 +623,16 @@ bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *v
         seg_pos[s] = pos_begin[seg_begin[s]];
     }
     pk.ents = base;
+    if (row_sources) {
+        std::vector<int2> tk;
+        tk.reserve((size_t)(n / 32 + L));
+        for (int s = 0; s < L; ++s)
+            for (int t0 = 0; t0 < count[s]; t0 += 32) tk.push_back(make_int2(s, t0));
+        pk.n_tasks = (int)tk.size();
+        pk.tasks.alloc(sizeof(int2) * (tk.empty() ? 1 : tk.size()));
+        if (!tk.empty())
+            SMAX_CUDA(cudaMemcpyAsync(pk.tasks.p, tk.data(), sizeof(int2) * tk.size(), cudaMemcpyHostToDevice, st));
+    }
     // launch geometry per run (steps sharing a run start), from its widest level
     pk.h_geo.assign(L, make_int2(1, 256));
     for (int s = 0; s < L;) {
@@ -510,12 +655,12 @@ bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *v
         fill_kernel<double><<<grid_for(n), 256, 0, st>>>(
             rp, ci, static_cast<const double *>(val), static_cast<const double *>(D), n, pk.prow.as<int>(),
             plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(), d_geo.as<int2>(),
-            pk.psrc.as<int>(), pk.pval.as<double>(), pk.pinv.as<double>(), flag.as<int>());
+            pk.psrc.as<int>(), pk.pval.as<double>(), pk.pinv.as<double>(), flag.as<int>(), row_sources);
     else
         fill_kernel<float><<<grid_for(n), 256, 0, st>>>(
             rp, ci, static_cast<const float *>(val), static_cast<const float *>(D), n, pk.prow.as<int>(),
             plev.as<int>(), pos_of_row.as<int>(), pk.lv.as<Level>(), d_seg.as<int>(), d_geo.as<int2>(),
-            pk.psrc.as<int>(), pk.pval.as<float>(), pk.pinv.as<float>(), flag.as<int>());
+            pk.psrc.as<int>(), pk.pval.as<float>(), pk.pinv.as<float>(), flag.as<int>(), row_sources);
     SMAX_CUDA(cudaGetLastError());
     int h_flag = 0;
     SMAX_CUDA(cudaMemcpyAsync(&h_flag, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -579,6 +724,38 @@ void pack_solve_batch(const LevelPack &pk, const int *mat_steps, const int *queu
     SMAX_CUDA(cudaGetLastError());
 }
 
+template <typename VT>
+void pack_solve_syncfree(const LevelPack &pk, const VT *B, VT *X, void *ctl, long long limit, bool force_timeout,
+                         DevStatus *st, cudaStream_t s) {
+    if (pk.n == 0) return;
+    if (!pk.row_sources) fail(SMAX_ERR_STATE, "the sync-free solve needs a row-sourced pack");
+    int *c = static_cast<int *>(ctl);
+    sf_reset_kernel<VT><<<grid_for(pk.n), 256, 0, s>>>(X, pk.n, c);
+    static int per_sm_cache[64] = {};
+    int dev = 0;
+    SMAX_CUDA(cudaGetDevice(&dev));
+    int per_sm = dev >= 0 && dev < 64 ? per_sm_cache[dev] : 0;
+    if (per_sm == 0) {
+        SMAX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, syncfree_kernel<VT>, kSfThreads, 0));
+        if (per_sm < 1) per_sm = 1;
+        if (dev >= 0 && dev < 64) per_sm_cache[dev] = per_sm;
+    }
+    const int chunks = (pk.n_tasks + kSfChunk - 1) / kSfChunk;
+    // deep, narrow schedules: about four levels' rows in flight, so waiting
+    // warps do not flood L2 with polls
+    const int64_t avg = pk.n / std::max(1, pk.n_levels());
+    const int64_t cap = std::max<int64_t>(8, (4 * avg + kSfThreads - 1) / kSfThreads);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)chunks, (int64_t)per_sm * sm_count(), cap}));
+    syncfree_kernel<VT><<<grid, kSfThreads, 0, s>>>(pk.lv.as<Level>(), pk.tasks.as<int2>(), pk.n_tasks,
+                                                    pk.prow.as<int>(), pk.psrc.as<int>(), pk.pval.as<VT>(),
+                                                    pk.pinv.as<VT>(), B, X, c, limit, force_timeout, st);
+    SMAX_CUDA(cudaGetLastError());
+}
+
+template void pack_solve_syncfree<double>(const LevelPack &, const double *, double *, void *, long long, bool,
+                                          DevStatus *, cudaStream_t);
+template void pack_solve_syncfree<float>(const LevelPack &, const float *, float *, void *, long long, bool,
+                                         DevStatus *, cudaStream_t);
 template void pack_solve<double>(const LevelPack &, const std::vector<PackStep> &, const double *, double *,
                                  cudaStream_t);
 template void pack_solve<float>(const LevelPack &, const std::vector<PackStep> &, const float *, float *,

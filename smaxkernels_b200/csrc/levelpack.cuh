@@ -42,6 +42,13 @@ struct LevelPack {
     DevBuf pinv;    // VT[n]: 1 / diagonal
     DevBuf bp, xp;  // VT[n]: right-hand side and solution in position order
     bool needs_x_init = false;  // some entry reads a solution not computed before it
+    // sync-free packs (row_sources): entries name the source ROW in the
+    // caller's numbering, never a ring slot, and `tasks` lists the warp tasks
+    // in sweep order: (level, first row of the level), 32 rows each, so a
+    // warp's rows never depend on one another
+    bool row_sources = false;
+    DevBuf tasks;  // int2[n_tasks]
+    int n_tasks = 0;
     int n_levels() const { return (int)h_lv.size(); }
 };
 
@@ -55,9 +62,12 @@ struct LevelPack {
 // pack more than about three times the off-diagonal entries.  allow_cluster:
 // runs with levels wider than one CTA covers may be solved by a thread-block
 // cluster (single matrices; the batch kernel is one CTA per matrix).
+// row_sources: build the sync-free form (every step its own level, entries
+// naming source rows, the task table).
 bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *val, const void *D, int vbytes,
                       int64_t n, const int *order, const std::vector<int> &src_begin, const std::vector<int> &count,
-                      const std::vector<int> &seg_begin, bool allow_cluster, cudaStream_t st);
+                      const std::vector<int> &seg_begin, bool allow_cluster, cudaStream_t st,
+                      bool row_sources = false);
 
 // Solves with the pack: gathers B into position order, runs each step --
 // wide levels as one grid launch each, runs of narrow levels as one
@@ -68,6 +78,20 @@ struct PackStep {
 };
 template <typename VT>
 void pack_solve(const LevelPack &pk, const std::vector<PackStep> &steps, const VT *B, VT *X, cudaStream_t st);
+
+// Sync-free solve on a row_sources pack: X is first filled with a pending
+// marker (a signalling-NaN pattern that no arithmetic result has), then one
+// launch of warps takes 32-row tasks in sweep order (a CTA claims a chunk of
+// tasks with one atomic) and each row waits on its sources' values in X,
+// with no barrier between levels.  A row's sources lie in earlier tasks, which
+// were claimed by running CTAs, so the earliest unfinished task can always
+// finish.  Each wait gives up after `limit` polls: SMAX_ERR_TIMEOUT in st, an
+// abort flag that ends the other waits, and NaN for the missing value.
+// B and X must not overlap.  ctl: device scratch of at least 64 bytes.
+// force_timeout (test only): the first row also waits on a word nothing writes.
+template <typename VT>
+void pack_solve_syncfree(const LevelPack &pk, const VT *B, VT *X, void *ctl, long long limit, bool force_timeout,
+                         DevStatus *st, cudaStream_t s);
 
 // One single-CTA sweep per matrix of a batch, matrices taken from a device
 // work queue: mat_steps[m] .. mat_steps[m+1] are matrix m's sweep steps.

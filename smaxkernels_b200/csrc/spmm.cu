@@ -21,18 +21,13 @@ template <typename VT> struct V16;
 template <> struct V16<double> { using T = double2; static constexpr int N = 2; };
 template <> struct V16<float> { using T = float4; static constexpr int N = 4; };
 
-// G lanes per row, NV vectors of VEC values per lane, k == G * NV * VEC (VEC
+// One row of Y from its group of G lanes (lane g of the group, gmask the
+// group's lanes): NV vectors of VEC values per lane, k == G * NV * VEC (VEC
 // == 1 is the scalar path for k not divisible by the vector width).
 template <typename VT, int G, int NV, int VEC>
-__global__ void __launch_bounds__(256) spmm_row_major_kernel(const int *__restrict__ row_ptr,
-                                                             const int *__restrict__ col,
-                                                             const VT *__restrict__ val, int64_t n_rows, int64_t k,
-                                                             const VT *__restrict__ X, VT *__restrict__ Y) {
-    const int lane = threadIdx.x & 31;
-    const int g = lane % G;
-    const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
-    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane - g));
-    if (row >= n_rows) return;  // whole groups leave together
+__device__ __forceinline__ void spmm_row(int64_t row, int g, unsigned gmask, const int *__restrict__ row_ptr,
+                                         const int *__restrict__ col, const VT *__restrict__ val, int64_t k,
+                                         const VT *__restrict__ X, VT *__restrict__ Y) {
     VT acc[NV][VEC];
 #pragma unroll
     for (int m = 0; m < NV; ++m)
@@ -84,12 +79,86 @@ __global__ void __launch_bounds__(256) spmm_row_major_kernel(const int *__restri
     }
 }
 
+template <int G> __device__ __forceinline__ unsigned group_mask(int lane) {
+    return (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (lane - lane % G));
+}
+
+// a grid of all rows, one group of G lanes per row
 template <typename VT, int G, int NV, int VEC>
-void launch_rm(const DevCRS &a, int64_t k, const VT *X, VT *Y, cudaStream_t st) {
+__global__ void __launch_bounds__(256) spmm_row_major_kernel(const int *__restrict__ row_ptr,
+                                                             const int *__restrict__ col,
+                                                             const VT *__restrict__ val, int64_t n_rows, int64_t k,
+                                                             const VT *__restrict__ X, VT *__restrict__ Y) {
+    const int lane = threadIdx.x & 31;
+    const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+    if (row >= n_rows) return;  // whole groups leave together
+    spmm_row<VT, G, NV, VEC>(row, lane % G, group_mask<G>(lane), row_ptr, col, val, k, X, Y);
+}
+
+// CTA b walks rows ranges[b] .. ranges[b+1] in order, kWalkThreads / G rows
+// at a time
+constexpr int kWalkThreads = 1024;
+template <typename VT, int G, int NV, int VEC>
+__global__ void __launch_bounds__(kWalkThreads, 1)
+    spmm_walk_kernel(const int *__restrict__ row_ptr, const int *__restrict__ col, const VT *__restrict__ val,
+                     const int64_t *__restrict__ ranges, int64_t k, const VT *__restrict__ X, VT *__restrict__ Y) {
+    const int lane = threadIdx.x & 31;
+    const int64_t r0 = ranges[blockIdx.x], r1 = ranges[blockIdx.x + 1];
+    for (int64_t row = r0 + threadIdx.x / G; row < r1; row += kWalkThreads / G)
+        spmm_row<VT, G, NV, VEC>(row, lane % G, group_mask<G>(lane), row_ptr, col, val, k, X, Y);
+}
+
+// ranges[b] = first row r with row_ptr[r] + r >= b * (nnz + n) / grid
+// (nonzeros and rows balanced: a row costs its entries plus its Y write)
+__global__ void walk_ranges_kernel(const int *__restrict__ row_ptr, int64_t n, int grid, int64_t *__restrict__ ranges) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > grid) return;
+    const int64_t total = (int64_t)row_ptr[n] + n;
+    const int64_t target = total * b / grid;
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if ((int64_t)row_ptr[mid] + mid < target) lo = mid + 1;
+        else hi = mid;
+    }
+    ranges[b] = b == grid ? n : lo;
+}
+
+template <typename VT, int G, int NV, int VEC>
+void launch_rm(const DevCRS &a, int64_t k, const VT *X, VT *Y, cudaStream_t st, const SpmmPlan *walk) {
+    if (walk) {
+        static bool carve[64] = {};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev >= 0 && dev < 64 && !carve[dev]) {
+            // no shared memory: the whole unified L1 holds X rows
+            SMAX_CUDA(cudaFuncSetAttribute(spmm_walk_kernel<VT, G, NV, VEC>,
+                                           cudaFuncAttributePreferredSharedMemoryCarveout, 0));
+            carve[dev] = true;
+        }
+        spmm_walk_kernel<VT, G, NV, VEC><<<walk->grid, kWalkThreads, 0, st>>>(
+            a.rp(), a.ci(), a.val.template as<VT>(), walk->ranges.as<int64_t>(), k, X, Y);
+        return;
+    }
     const uint64_t threads = (uint64_t)a.n_rows * G;
     spmm_row_major_kernel<VT, G, NV, VEC><<<ceil_div_u(threads, 256), 256, 0, st>>>(a.rp(), a.ci(),
                                                                                     a.val.template as<VT>(),
                                                                                     a.n_rows, k, X, Y);
+}
+
+const SpmmPlan *walk_plan(const DevCRS &a, SpmmPlan *plan, cudaStream_t st) {
+    if (!plan) return nullptr;
+    if (plan->key != a.row_ptr.p || plan->n != a.n_rows || plan->nnz != a.nnz) {
+        plan->grid = sm_count();
+        plan->ranges.ensure(sizeof(int64_t) * (plan->grid + 1));
+        walk_ranges_kernel<<<ceil_div_u((uint64_t)plan->grid + 1, 256), 256, 0, st>>>(a.rp(), a.n_rows, plan->grid,
+                                                                                      plan->ranges.as<int64_t>());
+        SMAX_CUDA(cudaGetLastError());
+        plan->key = a.row_ptr.p;
+        plan->n = a.n_rows;
+        plan->nnz = a.nnz;
+    }
+    return plan;
 }
 
 // scalar fallback for any k: one warp per row, lanes over the k columns
@@ -111,8 +180,10 @@ __global__ void spmm_row_major_generic(const int *__restrict__ row_ptr, const in
 }  // namespace
 
 template <typename VT>
-void crs_spmm_row_major(const DevCRS &a, int64_t k, const VT *X, VT *Y, cudaStream_t st) {
+void crs_spmm_row_major(const DevCRS &a, int64_t k, const VT *X, VT *Y, cudaStream_t st, SpmmPlan *plan,
+                        int variant) {
     if (a.n_rows == 0 || k == 0) return;
+    const SpmmPlan *w = variant == 2 ? walk_plan(a, plan, st) : nullptr;
     constexpr int VEC = V16<VT>::N;
     // vector path when k is a multiple of VEC: k/VEC vectors spread over G lanes
     // (and X, Y 16-byte aligned: offsets given to apply() may shift them)
@@ -120,24 +191,24 @@ void crs_spmm_row_major(const DevCRS &a, int64_t k, const VT *X, VT *Y, cudaStre
     const int64_t nvec = (aligned && k % VEC == 0) ? k / VEC : 0;
     bool done = true;
     switch (nvec) {
-    case 1: launch_rm<VT, 1, 1, VEC>(a, k, X, Y, st); break;
-    case 2: launch_rm<VT, 2, 1, VEC>(a, k, X, Y, st); break;
-    case 4: launch_rm<VT, 4, 1, VEC>(a, k, X, Y, st); break;
-    case 8: launch_rm<VT, 8, 1, VEC>(a, k, X, Y, st); break;
-    case 16: launch_rm<VT, 16, 1, VEC>(a, k, X, Y, st); break;
-    case 32: launch_rm<VT, 32, 1, VEC>(a, k, X, Y, st); break;
-    case 64: launch_rm<VT, 32, 2, VEC>(a, k, X, Y, st); break;
-    case 128: launch_rm<VT, 32, 4, VEC>(a, k, X, Y, st); break;
+    case 1: launch_rm<VT, 1, 1, VEC>(a, k, X, Y, st, w); break;
+    case 2: launch_rm<VT, 2, 1, VEC>(a, k, X, Y, st, w); break;
+    case 4: launch_rm<VT, 4, 1, VEC>(a, k, X, Y, st, w); break;
+    case 8: launch_rm<VT, 8, 1, VEC>(a, k, X, Y, st, w); break;
+    case 16: launch_rm<VT, 16, 1, VEC>(a, k, X, Y, st, w); break;
+    case 32: launch_rm<VT, 32, 1, VEC>(a, k, X, Y, st, w); break;
+    case 64: launch_rm<VT, 32, 2, VEC>(a, k, X, Y, st, w); break;
+    case 128: launch_rm<VT, 32, 4, VEC>(a, k, X, Y, st, w); break;
     default: done = false;
     }
     if (!done) {
         // k not a power-of-two number of vectors: small k -> scalar lanes per
         // element, otherwise one warp per row
-        if (k == 1) launch_rm<VT, 1, 1, 1>(a, k, X, Y, st);
-        else if (k == 2) launch_rm<VT, 2, 1, 1>(a, k, X, Y, st);
-        else if (k == 4) launch_rm<VT, 4, 1, 1>(a, k, X, Y, st);
-        else if (k == 8) launch_rm<VT, 8, 1, 1>(a, k, X, Y, st);
-        else if (k == 16) launch_rm<VT, 16, 1, 1>(a, k, X, Y, st);
+        if (k == 1) launch_rm<VT, 1, 1, 1>(a, k, X, Y, st, w);
+        else if (k == 2) launch_rm<VT, 2, 1, 1>(a, k, X, Y, st, w);
+        else if (k == 4) launch_rm<VT, 4, 1, 1>(a, k, X, Y, st, w);
+        else if (k == 8) launch_rm<VT, 8, 1, 1>(a, k, X, Y, st, w);
+        else if (k == 16) launch_rm<VT, 16, 1, 1>(a, k, X, Y, st, w);
         else
             spmm_row_major_generic<VT><<<ceil_div_u((uint64_t)a.n_rows * 32, 256), 256, 0, st>>>(
                 a.rp(), a.ci(), a.val.template as<VT>(), a.n_rows, k, X, Y);
@@ -145,7 +216,9 @@ void crs_spmm_row_major(const DevCRS &a, int64_t k, const VT *X, VT *Y, cudaStre
     SMAX_CUDA(cudaGetLastError());
 }
 
-template void crs_spmm_row_major<double>(const DevCRS &, int64_t, const double *, double *, cudaStream_t);
-template void crs_spmm_row_major<float>(const DevCRS &, int64_t, const float *, float *, cudaStream_t);
+template void crs_spmm_row_major<double>(const DevCRS &, int64_t, const double *, double *, cudaStream_t, SpmmPlan *,
+                                         int);
+template void crs_spmm_row_major<float>(const DevCRS &, int64_t, const float *, float *, cudaStream_t, SpmmPlan *,
+                                        int);
 
 }  // namespace smax

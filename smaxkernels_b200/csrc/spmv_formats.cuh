@@ -54,7 +54,20 @@ void crs_to_bcrs(const DevCRS &a, int vbytes, int64_t bh, int64_t bw, int64_t hp
 // Y = A X with k right-hand sides.  Row-major: X[col*k+v], Y[row*k+v].
 // Column-major: X[ldx*v+col], Y[row+ldy*v] (the reference uses A's n_rows as
 // the leading dimension of X and Y, src/kernels/spmm/spmm_cpu/spmm_cpu_crs_impl.hpp:29,44).
+// Row-major SpMM launch plan.  variant 1: one thread group per row over a
+// grid of all rows.  variant 2 ("walk"): one CTA per SM, each walking a
+// contiguous, nonzero-balanced range of rows in order, so the X rows that
+// neighbouring rows share can stay in that SM's L1 (an autotuner candidate:
+// on the 27-point stencil it loses to the grid's occupancy).  variant 0: the
+// grid.
+struct SpmmPlan {
+    DevBuf ranges;  // int64 row bounds of the walk CTAs, grid + 1 entries
+    int grid = 0;
+    const void *key = nullptr;
+    int64_t n = -1, nnz = -1;
+};
 template <typename VT>
-void crs_spmm_row_major(const DevCRS &a, int64_t k, const VT *X, VT *Y, cudaStream_t st);
+void crs_spmm_row_major(const DevCRS &a, int64_t k, const VT *X, VT *Y, cudaStream_t st, SpmmPlan *plan = nullptr,
+                        int variant = 0);
 
 }  // namespace smax

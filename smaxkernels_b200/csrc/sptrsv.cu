@@ -203,6 +203,9 @@ void TriPlan::finish(cudaStream_t) {
     pack_ok = false;
     pack_unfit = false;
     pack = LevelPack();
+    sf_ok = false;
+    sf_unfit = false;
+    sf_pack = LevelPack();
 }
 
 bool TriPlan::ensure_pack(const int *rp, const int *ci, const void *val, const void *D, int vbytes, int merge_rows,
@@ -239,6 +242,34 @@ bool TriPlan::ensure_pack(const int *rp, const int *ci, const void *val, const v
     pack_tag = tag;
     pack_merge = merge_rows;
     pack_vbytes = vbytes;
+    return true;
+}
+
+bool TriPlan::ensure_syncfree(const int *rp, const int *ci, const void *val, const void *D, int vbytes, uint64_t tag,
+                              cudaStream_t st) {
+    if (sf_ok && sf_key[0] == val && sf_key[1] == D && sf_tag == tag && sf_vbytes == vbytes) return true;
+    if (sf_unfit) return false;  // a property of the pattern and the level sets
+    const int L = n_levels();
+    std::vector<int> src_begin(L), count(L), seg_begin(L);
+    for (int sw = 0; sw < L; ++sw) {
+        const int lv = descending ? L - 1 - sw : sw;
+        src_begin[sw] = lvl_ptr[lv];
+        count[sw] = lvl_ptr[lv + 1] - lvl_ptr[lv];
+        seg_begin[sw] = sw;
+    }
+    sf_ok = false;
+    const bool ok = build_level_pack(sf_pack, rp, ci, val, D, vbytes, n_rows, has_order ? order.as<int>() : nullptr,
+                                     src_begin, count, seg_begin, false, st, true);
+    if (!ok || sf_pack.needs_x_init) {
+        sf_pack = LevelPack();
+        sf_unfit = true;
+        return false;
+    }
+    sf_ok = true;
+    sf_key[0] = val;
+    sf_key[1] = D;
+    sf_tag = tag;
+    sf_vbytes = vbytes;
     return true;
 }
 
@@ -398,6 +429,23 @@ void TriPlan::release_graph() {
 
 TriPlan::~TriPlan() { release_graph(); }
 
+template <typename VT>
+bool tri_solve_syncfree(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, uint64_t tag, DevBuf &ctl,
+                        long long limit, bool force_timeout, DevStatus *st, cudaStream_t s) {
+    if (p.n_rows == 0) return true;
+    const uintptr_t b0 = reinterpret_cast<uintptr_t>(B), x0 = reinterpret_cast<uintptr_t>(X);
+    const uintptr_t len = sizeof(VT) * (uintptr_t)p.n_rows;
+    if (b0 < x0 + len && x0 < b0 + len) return false;  // B is read while X fills
+    if (!p.ensure_syncfree(a.rp(), a.ci(), a.val.p, D, sizeof(VT), tag, s)) return false;
+    ctl.ensure(64);
+    pack_solve_syncfree<VT>(p.sf_pack, B, X, ctl.p, limit, force_timeout, st, s);
+    return true;
+}
+
+template bool tri_solve_syncfree<double>(TriPlan &, const DevCRS &, const double *, const double *, double *, uint64_t,
+                                         DevBuf &, long long, bool, DevStatus *, cudaStream_t);
+template bool tri_solve_syncfree<float>(TriPlan &, const DevCRS &, const float *, const float *, float *, uint64_t,
+                                        DevBuf &, long long, bool, DevStatus *, cudaStream_t);
 template void tri_solve<double>(TriPlan &, const DevCRS &, const double *, const double *, double *, int64_t, bool,
                                 int64_t, int, uint64_t, cudaStream_t);
 template void tri_solve<float>(TriPlan &, const DevCRS &, const float *, const float *, float *, int64_t, bool,

@@ -70,6 +70,17 @@ struct TriPlan {
     bool ensure_pack(const int *rp, const int *ci, const void *val, const void *D, int vbytes, int merge_rows,
                      uint64_t tag, cudaStream_t st);
 
+    // sync-free form of the pack (SMAX_SOLVE_SYNCFREE): every level its own
+    // step, entries naming source rows; unfit when padding is too large or an
+    // entry reads a row that is not solved before it
+    LevelPack sf_pack;
+    bool sf_ok = false, sf_unfit = false;
+    const void *sf_key[2] = {nullptr, nullptr};
+    uint64_t sf_tag = ~0ull;
+    int sf_vbytes = 0;
+    bool ensure_syncfree(const int *rp, const int *ci, const void *val, const void *D, int vbytes, uint64_t tag,
+                         cudaStream_t st);
+
     // dependency levels of the matrix itself (plain solve)
     void build_own(const DevCRS &a, bool upper, cudaStream_t st);
     // caller-given contiguous levels (permuted, level-scheduled solve)
@@ -101,6 +112,12 @@ void tri_solve(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int
 template <typename VT>
 void tri_solve_raw(TriPlan &p, const int *rp, const int *ci, const VT *val, const VT *D, const VT *B, VT *X,
                    int64_t k, bool row_major, int64_t ld, int merge_rows, uint64_t tag, cudaStream_t st);
+// The sync-free solve of one right-hand side (pack_solve_syncfree).  Returns
+// false, launching nothing, when it does not apply: the matrix does not pack,
+// an entry reads a row not solved before it, or B and X overlap.
+template <typename VT>
+bool tri_solve_syncfree(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, uint64_t tag, DevBuf &ctl,
+                        long long limit, bool force_timeout, DevStatus *st, cudaStream_t s);
 // The same launch sequence, captured once into a CUDA graph and replayed.
 template <typename VT>
 void tri_solve_graph(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int64_t k, bool row_major,

@@ -67,7 +67,7 @@ FLAG = dict(mat_perm=0, mat_upper_triang=1, mat_lower_triang=2, vec_row_major=3,
             spmv_variant=10, solve_mode=11, level_merge=12, spin_limit=13, test_force_timeout=14,
             refine=15, refine_tol=16, sweep_cluster=17, spmv_pipeline=18)
 
-SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED, SOLVE_GRAPH, SOLVE_PERSISTENT = 0, 1, 2, 3, 4
+SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED, SOLVE_GRAPH, SOLVE_PERSISTENT, SOLVE_SYNCFREE = 0, 1, 2, 3, 4, 5
 
 
 CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy: the legacy default stream as an explicit handle
@@ -230,7 +230,8 @@ class Kernel:
         return self._flag("spmv_variant", v)
 
     def set_solve_mode(self, mode: int):
-        """SpTRSV/SpTRSM launch scheme: SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED or SOLVE_GRAPH."""
+        """SpTRSV/SpTRSM launch scheme: SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED, SOLVE_GRAPH,
+        SOLVE_PERSISTENT or SOLVE_SYNCFREE."""
         return self._flag("solve_mode", mode)
 
     def set_spin_limit(self, kilo_polls: int):

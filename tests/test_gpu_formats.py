@@ -59,13 +59,15 @@ def gpu_bcrs_spmv(b, x, col_major):
     return y
 
 
-def gpu_spmm(rp, col, val, X, k_, row_major, n_cols=None):
+def gpu_spmm(rp, col, val, X, k_, row_major, n_cols=None, variant=0):
     from smaxkernels_b200 import IntType, KernelType, PlatformType
     n = len(rp) - 1
     Y = np.zeros(n * k_, dtype=val.dtype)
     smax = _iface()
     smax.register_kernel("k", KernelType.SPMM, PlatformType.CUDA, IntType.INT32, _ft(val.dtype))
     k = smax.kernel("k")
+    if variant:
+        k.set_spmv_variant(variant)
     k.register_A(n, n_cols or n, len(col), col, rp, val)
     k.register_B(n_cols or n, k_, np.ascontiguousarray(X, val.dtype))
     k.register_C(n, k_, Y)
@@ -234,6 +236,19 @@ def test_spmm_random_vs_oracle(vt, k_, row_major):
     assert normwise(Y, Y_ref) <= tol(vt)
     Y64 = O.spmm(rp, col, val.astype(np.float64), X.astype(np.float64), k_, row_major=row_major)
     assert normwise(Y, Y64) <= tol(vt)
+
+
+@pytest.mark.parametrize("vt", [np.float64, np.float32])
+@pytest.mark.parametrize("k_", [1, 3, 16, 64, 100])
+def test_spmm_row_major_kernels_agree(vt, k_):
+    """The all-rows grid and the per-SM row walks compute each row with the
+    same group and the same order of products: bit-identical results."""
+    rp, col, val = rand_crs(20000, 9, 61, vt=vt, empty_frac=0.05, long_rows=(3000,))
+    X = np.random.default_rng(62).uniform(-1, 1, 20000 * k_).astype(vt)
+    Y1 = gpu_spmm(rp, col.copy(), val.copy(), X, k_, True, variant=1)
+    Y2 = gpu_spmm(rp, col.copy(), val.copy(), X, k_, True, variant=2)
+    np.testing.assert_array_equal(Y1, Y2)
+    assert normwise(Y2, O.spmm(rp, col, val, X, k_, row_major=True)) <= tol(vt)
 
 
 @pytest.mark.slow
