@@ -534,15 +534,15 @@ def wl_sptrsv(b: Bench):
             t, reps = b.time(k.apply, budget_s=2.0, max_reps=100)
         results[mode] = t
         xs[mode] = xd.clone()
-        same = bool(b.torch.equal(xs[mode], xs[3])) if 3 in xs else None
+        same = bool(b.torch.equal(xd, xs[3])) if 3 in xs else None
         cpu = None
         if mode == 3:
             cpu = b.cpu(lambda: b.ref.time_sptrsv(rp, col, val, rhs, warm=1, reps=3)[0], nbytes,
                         "3 solves after 1 warm-up (reference naive_crs_sptrsv, serial)")
         b.emit(f"sptrsv_f64_laplace2d_{side}_natural_{names[mode]}", "SpTRSV GB/s", nbytes / t / 1e9, "GB/s", t,
                reps, "f64", {"n_rows": n, "nnz": nnz, "levels": n_lv, "scheme": names[mode]}, clk.summary(),
-               b.hbm(nbytes, t, "level_kernel/segment_kernel"), cpu,
-               launches=n_lv * reps if mode == 1 else (reps if mode == 4 else None),
+               b.hbm(nbytes, t, "syncfree_kernel" if mode == 5 else "wide_level_kernel/sweep_kernel"), cpu,
+               launches=n_lv * reps if mode == 1 else (reps if mode == 4 else (2 * reps if mode == 5 else None)),
                us_per_level=round(t * 1e6 / n_lv, 4), bitwise_equal_to_graph=same)
         smax.close()
     if b.args.tri_natural_only:
@@ -561,7 +561,8 @@ def wl_sptrsv(b: Bench):
     lvl = np.array([smax.get_level_ptr_at(i) for i in range(smax.get_n_levels() + 1)], np.int32)
     nl = len(lvl) - 1
     xs = {}
-    for mode in (3, 4, 5):
+    names[0] = "auto"
+    for mode in (3, 0, 4, 5):
         smax.register_kernel(f"p{mode}", KernelType.SPTRSV, *b_types(vt))
         k = smax.kernel(f"p{mode}")
         k.set_mat_perm(True)
@@ -584,9 +585,9 @@ def wl_sptrsv(b: Bench):
         b.emit(f"sptrsv_f64_laplace2d_{side}_permuted_{names[mode]}", "SpTRSV GB/s", nbytes / t / 1e9, "GB/s", t,
                reps, "f64", {"n_rows": n, "nnz": len(lcol), "levels": nl, "scheme": names[mode],
                              "ordering": "random symmetric permutation (seed 3), RS level order"},
-               clk.summary(), b.hbm(nbytes, t, "level_kernel/segment_kernel"), cpu,
-               launches=reps if mode == 4 else None, us_per_level=round(t * 1e6 / max(nl, 1), 4),
-               bitwise_equal_to_graph=same)
+               clk.summary(), b.hbm(nbytes, t, "syncfree_kernel" if mode in (0, 5) else "wide_level_kernel/sweep_kernel"),
+               cpu, launches=reps if mode == 4 else (2 * reps if mode in (0, 5) else None),
+               us_per_level=round(t * 1e6 / max(nl, 1), 4), bitwise_equal_to_graph=same)
     smax.close()
     # SpTRSM, k = 32 right-hand sides, row-major
     kv = 32

@@ -101,7 +101,9 @@ typedef int smax_status;
 #define SMAX_FLAG_SPMV_PIPELINE 18     /* CRS SpMV with host pointers: row blocks whose y is downloaded while later blocks compute (default 4; 0/1: off) */
 
 /* SpTRSV / SpTRSM launch schemes (SMAX_FLAG_SOLVE_MODE) */
-#define SMAX_SOLVE_AUTO 0        /* graph-captured, narrow levels merged (the default) */
+#define SMAX_SOLVE_AUTO 0        /* the default: SMAX_SOLVE_SYNCFREE for one right-hand side and few wide
+                                    levels (>= 2^17 rows, >= 32768 rows per level on average), else
+                                    SMAX_SOLVE_GRAPH */
 #define SMAX_SOLVE_PER_LEVEL 1   /* one kernel launch per level, no merging, no graph */
 #define SMAX_SOLVE_MERGED 2      /* narrow levels merged into single-CTA runs, no graph */
 #define SMAX_SOLVE_GRAPH 3       /* the merged launch sequence captured into a CUDA graph */

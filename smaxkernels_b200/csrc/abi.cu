@@ -228,8 +228,12 @@ template <typename VT> void tri_apply_t(smax_kernel_s *k, const VT *Bv, VT *Xv) 
                                  k->force_timeout, k->spin_limit, k->stream);
         return;
     }
-    if (k->solve_mode == SMAX_SOLVE_SYNCFREE) {
+    if (k->solve_mode == SMAX_SOLVE_SYNCFREE)
         require(kk == 1, SMAX_ERR_UNSUPPORTED, "the sync-free solve handles one right-hand side");
+    // the default runs a schedule of few, wide levels sync-free: no barrier
+    // (launch) between levels
+    if (k->solve_mode == SMAX_SOLVE_SYNCFREE ||
+        (k->solve_mode == SMAX_SOLVE_AUTO && kk == 1 && syncfree_suits(k->tri))) {
         if (tri_solve_syncfree<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, k->vals_version, k->sf_ctl, k->spin_limit,
                                    k->force_timeout, dstatus(k), k->stream))
             return;

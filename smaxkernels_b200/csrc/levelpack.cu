@@ -37,7 +37,7 @@ using Level = LevelPack::Level;
 constexpr int kPad = LevelPack::kPad;
 constexpr int kRing = LevelPack::kRing;
 constexpr int kRingShift = 13;     // kRing == 1 << kRingShift
-constexpr int kRowsPerThread = 2;  // rows of a level held in registers per thread
+constexpr int kRowsPerThread = 2;  // rows of a level held in registers per thread (default sweeps)
 constexpr int kEnts = 2;           // prefetched entries per row (the rest are loaded when used)
 constexpr int kClusterCTAs = 8;    // CTAs of a cluster run (portable cluster size)
 constexpr int kClusterThreads = 256;
@@ -138,21 +138,46 @@ __global__ void scatter_kernel(const int *__restrict__ prow, int64_t n, const VT
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) X[prow[p]] = xp[p];
 }
 
-// one wide level: thread per row
+constexpr int kWideEnts = 4;  // entries of a row whose loads are all issued before the first use
+
+// one wide level: thread per row.  The first kWideEnts entries and their
+// solutions are loaded before any is used, so a row costs one entry load and
+// one gather of latency instead of one pair per entry.
 template <typename VT>
 __global__ void wide_level_kernel(Level L, const int *__restrict__ psrc, const VT *__restrict__ pval,
                                   const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= L.m) return;
-    VT sum = VT(0);
-    for (int i = 0; i < L.w; ++i) {
-        const long long idx = L.base + (long long)i * L.m + t;
-        const int src = psrc[idx];
-        if (src == kPad) break;
-        sum += pval[idx] * xp[src];
+    int src[kWideEnts];
+    VT v[kWideEnts], xs[kWideEnts];
+#pragma unroll
+    for (int i = 0; i < kWideEnts; ++i) {
+        src[i] = kPad;
+        if (i < L.w) {
+            const long long idx = L.base + (long long)i * L.m + t;
+            src[i] = psrc[idx];
+            v[i] = pval[idx];
+        }
     }
+#pragma unroll
+    for (int i = 0; i < kWideEnts; ++i) xs[i] = src[i] != kPad ? xp[src[i]] : VT(0);
     const int p = L.pos + t;
-    xp[p] = (bp[p] - sum) * pinv[p];
+    const VT bi = bp[p], inv = pinv[p];
+    VT sum = VT(0);
+    bool more = true;
+#pragma unroll
+    for (int i = 0; i < kWideEnts; ++i) {
+        if (src[i] == kPad) { more = false; break; }
+        sum += v[i] * xs[i];
+    }
+    if (more)
+        for (int i = kWideEnts; i < L.w; ++i) {
+            const long long idx = L.base + (long long)i * L.m + t;
+            const int s = psrc[idx];
+            if (s == kPad) break;
+            sum += pval[idx] * xp[s];
+        }
+    xp[p] = (bi - sum) * inv;
 }
 
 template <typename VT> struct RowRegs {
@@ -167,12 +192,12 @@ __device__ __forceinline__ Level load_level(const Level *lv, int s) {
     return Level{v.x, v.y, v.z, v.w};
 }
 
-template <typename VT, int T, int CS>
+template <typename VT, int T, int CS, int NR>
 __device__ __forceinline__ void load_rows(const Level &L, int g, const int *__restrict__ psrc,
                                           const VT *__restrict__ pval, const VT *__restrict__ pinv,
-                                          const VT *__restrict__ bp, RowRegs<VT> (&R)[kRowsPerThread]) {
+                                          const VT *__restrict__ bp, RowRegs<VT> (&R)[NR]) {
 #pragma unroll
-    for (int k = 0; k < kRowsPerThread; ++k) {
+    for (int k = 0; k < NR; ++k) {
         const int t = g + k * T * CS;
 #pragma unroll
         for (int i = 0; i < kEnts; ++i) R[k].src[i] = kPad;
@@ -231,8 +256,9 @@ template <int CS> __device__ __forceinline__ void run_barrier() {
 }
 
 // Sweeps steps [s0, s1) of the pack with CS CTAs of T threads (one CTA or one
-// cluster); thread g of the run solves rows g, g + T*CS, ... of every level.
-template <typename VT, int T, int CS>
+// cluster); thread g of the run solves rows g, g + T*CS, ... of every level,
+// the first NR of them from registers loaded one level ahead.
+template <typename VT, int T, int CS, int NR = kRowsPerThread>
 __device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const int *__restrict__ psrc,
                           const VT *__restrict__ pval, const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp,
                           VT *ring) {
@@ -242,17 +268,17 @@ __device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const in
     if constexpr (CS > 1) rank = cooperative_groups::this_cluster().block_rank();
     const int g = (int)rank * T + (int)threadIdx.x;
     const int warp0 = g & ~31;
-    RowRegs<VT> cur[kRowsPerThread], nxt[kRowsPerThread];
+    RowRegs<VT> cur[NR], nxt[NR];
     Level Lc = load_level(lv, s0);
     Level Ln = load_level(lv, s0 + 1 < s1 ? s0 + 1 : s0);
-    load_rows<VT, T, CS>(Lc, g, psrc, pval, pinv, bp, cur);
+    load_rows<VT, T, CS, NR>(Lc, g, psrc, pval, pinv, bp, cur);
     for (int s = s0; s < s1; ++s) {
         const Level Lnn = load_level(lv, s + 2 < s1 ? s + 2 : s);
-        if (s + 1 < s1 && warp0 < Ln.m) load_rows<VT, T, CS>(Ln, g, psrc, pval, pinv, bp, nxt);
+        if (s + 1 < s1 && warp0 < Ln.m) load_rows<VT, T, CS, NR>(Ln, g, psrc, pval, pinv, bp, nxt);
         if (s + 2 < s1) prefetch_level_l2<VT>(Lnn, g, psrc, pval, pinv, bp);
         if (warp0 < Lc.m) {
 #pragma unroll
-            for (int k = 0; k < kRowsPerThread; ++k) {
+            for (int k = 0; k < NR; ++k) {
                 const int t = g + k * G;
                 if (t < Lc.m) {
                     VT sum = VT(0);
@@ -277,7 +303,7 @@ __device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const in
                 }
             }
             // rows beyond the register slots (levels wider than the slots cover)
-            for (int t = g + kRowsPerThread * G; t < Lc.m; t += G) {
+            for (int t = g + NR * G; t < Lc.m; t += G) {
                 VT sum = VT(0);
                 for (int i = 0; i < Lc.w; ++i) {
                     const int idx = Lc.base + i * Lc.m + t;
@@ -297,16 +323,16 @@ __device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const in
         Lc = Ln;
         Ln = Lnn;
 #pragma unroll
-        for (int k = 0; k < kRowsPerThread; ++k) cur[k] = nxt[k];
+        for (int k = 0; k < NR; ++k) cur[k] = nxt[k];
     }
 }
 
-template <typename VT, int T>
+template <typename VT, int T, int NR>
 __global__ void __launch_bounds__(T, 1)
     sweep_kernel(const Level *__restrict__ lv, int s0, int s1, const int *__restrict__ psrc,
                  const VT *__restrict__ pval, const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp) {
     extern __shared__ __align__(16) unsigned char smem[];
-    sweep_run<VT, T, 1>(lv, s0, s1, psrc, pval, pinv, bp, xp, reinterpret_cast<VT *>(smem));
+    sweep_run<VT, T, 1, NR>(lv, s0, s1, psrc, pval, pinv, bp, xp, reinterpret_cast<VT *>(smem));
 }
 
 // one run on a cluster of kClusterCTAs CTAs (launched with cluster dimensions)
@@ -413,13 +439,14 @@ __global__ void sf_reset_kernel(VT *__restrict__ X, int64_t n, int *__restrict__
 }
 
 // ctl: [0] task counter, [1] abort flag, [4..] a word that stays pending
-// (waited on by the first row when `never` is set: the test knob)
+// (waited on by the first row when `never` is set: the test knob).
+// A task is (first position, rows | width << 6, level rows = entry stride,
+// first entry).
 template <typename VT>
 __global__ void __launch_bounds__(kSfThreads)
-    syncfree_kernel(const Level *__restrict__ lv, const int2 *__restrict__ tasks, int n_tasks,
-                    const int *__restrict__ prow, const int *__restrict__ psrc, const VT *__restrict__ pval,
-                    const VT *__restrict__ pinv, const VT *__restrict__ B, VT *X, int *ctl, long long limit,
-                    bool never, DevStatus *st) {
+    syncfree_kernel(const int4 *__restrict__ tasks, int n_tasks, const int *__restrict__ prow,
+                    const int *__restrict__ psrc, const VT *__restrict__ pval, const VT *__restrict__ pinv,
+                    const VT *__restrict__ B, VT *X, int *ctl, long long limit, bool never, DevStatus *st) {
     __shared__ int chunk_sh;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int *abort_flag = ctl + 1;
@@ -431,23 +458,25 @@ __global__ void __launch_bounds__(kSfThreads)
         if (c0 >= n_tasks) return;
         const int c1 = min(c0 + kSfChunk, n_tasks);
         for (int ti = c0 + warp; ti < c1; ti += kSfThreads / 32) {
-            const int2 tk = tasks[ti];
-            const Level L = load_level(lv, tk.x);
-            const int t = tk.y + lane;
-            if (t >= L.m) continue;
-            // every load that does not wait goes out first
+            const int4 tk = tasks[ti];
+            const int w = tk.y >> 6;
+            if (lane >= (tk.y & 63)) continue;
+            // every load goes out before the first wait: entries, then the
+            // sources' values, right-hand side and 1/D
             int src[kSfEnts];
-            VT v[kSfEnts];
+            VT v[kSfEnts], xs[kSfEnts];
 #pragma unroll
             for (int i = 0; i < kSfEnts; ++i) {
                 src[i] = kPad;
-                if (i < L.w) {
-                    const long long idx = L.base + (long long)i * L.m + t;
+                if (i < w) {
+                    const long long idx = tk.w + (long long)i * tk.z + lane;
                     src[i] = psrc[idx];
                     v[i] = pval[idx];
                 }
             }
-            const int p = L.pos + t;
+#pragma unroll
+            for (int i = 0; i < kSfEnts; ++i) xs[i] = src[i] != kPad ? ld_relaxed(X + src[i]) : VT(0);
+            const int p = tk.x + lane;
             const int r = prow[p];
             const VT bi = B[r], inv = pinv[p];
             VT sum = VT(0);
@@ -457,11 +486,12 @@ __global__ void __launch_bounds__(kSfThreads)
 #pragma unroll
             for (int i = 0; i < kSfEnts; ++i) {
                 if (src[i] == kPad) { more = false; break; }
-                sum += v[i] * solved(X + src[i], limit, abort_flag, st);
+                const VT xv = Pending<VT>::is(xs[i]) ? wait_solved(X + src[i], limit, abort_flag, st) : xs[i];
+                sum += v[i] * xv;
             }
             if (more)
-                for (int i = kSfEnts; i < L.w; ++i) {
-                    const long long idx = L.base + (long long)i * L.m + t;
+                for (int i = kSfEnts; i < w; ++i) {
+                    const long long idx = tk.w + (long long)i * tk.z + lane;
                     const int sc = psrc[idx];
                     if (sc == kPad) break;
                     sum += pval[idx] * solved(X + sc, limit, abort_flag, st);
@@ -472,7 +502,7 @@ __global__ void __launch_bounds__(kSfThreads)
 }
 
 template <typename VT, int T> void set_smem_attr_t() {
-    SMAX_CUDA(cudaFuncSetAttribute(sweep_kernel<VT, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    SMAX_CUDA(cudaFuncSetAttribute(sweep_kernel<VT, T, kRowsPerThread>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(kRing * sizeof(VT))));
     SMAX_CUDA(cudaFuncSetAttribute(sweep_batch_kernel<VT, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(kRing * sizeof(VT))));
@@ -547,11 +577,13 @@ void launch_run(const LevelPack &pk, int s0, int s1, const int *psrc, const VT *
         cudaLaunchConfig_t cfg = cluster_config(attr, sm, st);
         SMAX_CUDA(cudaLaunchKernelEx(&cfg, sweep_cluster_kernel<VT>, lv, s0, s1, psrc, pval, pinv, bp, xp));
     } else if (geo.y == 256) {
-        sweep_kernel<VT, 256><<<1, 256, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
+        sweep_kernel<VT, 256, kRowsPerThread><<<1, 256, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
     } else if (geo.y == 512) {
-        sweep_kernel<VT, 512><<<1, 512, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
+        sweep_kernel<VT, 512, kRowsPerThread><<<1, 512, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
     } else {
-        sweep_kernel<VT, 1024><<<1, 1024, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
+        // 256 threads holding 8 rows each were measured 1.37x slower on the
+        // natural 2048^2 triangle: each thread's rows then solve one after another
+        sweep_kernel<VT, 1024, kRowsPerThread><<<1, 1024, sm, st>>>(lv, s0, s1, psrc, pval, pinv, bp, xp);
     }
 }
 
@@ -624,14 +656,23 @@ bool build_level_pack(LevelPack &pk, const int *rp, const int *ci, const void *v
     }
     pk.ents = base;
     if (row_sources) {
-        std::vector<int2> tk;
+        // warp tasks: (first position, rows | width << 6, entry stride, first entry)
+        std::vector<int4> tk;
         tk.reserve((size_t)(n / 32 + L));
-        for (int s = 0; s < L; ++s)
-            for (int t0 = 0; t0 < count[s]; t0 += 32) tk.push_back(make_int2(s, t0));
+        for (int s = 0; s < L; ++s) {
+            const Level &lv_s = pk.h_lv[s];
+            if (lv_s.w >= (1 << 25)) {  // does not fit the task encoding
+                pk = LevelPack();
+                return false;
+            }
+            for (int t0 = 0; t0 < lv_s.m; t0 += 32)
+                tk.push_back(make_int4(lv_s.pos + t0, std::min(32, lv_s.m - t0) | (lv_s.w << 6), lv_s.m,
+                                       lv_s.base + t0));
+        }
         pk.n_tasks = (int)tk.size();
-        pk.tasks.alloc(sizeof(int2) * (tk.empty() ? 1 : tk.size()));
+        pk.tasks.alloc(sizeof(int4) * (tk.empty() ? 1 : tk.size()));
         if (!tk.empty())
-            SMAX_CUDA(cudaMemcpyAsync(pk.tasks.p, tk.data(), sizeof(int2) * tk.size(), cudaMemcpyHostToDevice, st));
+            SMAX_CUDA(cudaMemcpyAsync(pk.tasks.p, tk.data(), sizeof(int4) * tk.size(), cudaMemcpyHostToDevice, st));
     }
     // launch geometry per run (steps sharing a run start), from its widest level
     pk.h_geo.assign(L, make_int2(1, 256));
@@ -746,9 +787,9 @@ void pack_solve_syncfree(const LevelPack &pk, const VT *B, VT *X, void *ctl, lon
     const int64_t avg = pk.n / std::max(1, pk.n_levels());
     const int64_t cap = std::max<int64_t>(8, (4 * avg + kSfThreads - 1) / kSfThreads);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)chunks, (int64_t)per_sm * sm_count(), cap}));
-    syncfree_kernel<VT><<<grid, kSfThreads, 0, s>>>(pk.lv.as<Level>(), pk.tasks.as<int2>(), pk.n_tasks,
-                                                    pk.prow.as<int>(), pk.psrc.as<int>(), pk.pval.as<VT>(),
-                                                    pk.pinv.as<VT>(), B, X, c, limit, force_timeout, st);
+    syncfree_kernel<VT><<<grid, kSfThreads, 0, s>>>(pk.tasks.as<int4>(), pk.n_tasks, pk.prow.as<int>(),
+                                                    pk.psrc.as<int>(), pk.pval.as<VT>(), pk.pinv.as<VT>(), B, X, c,
+                                                    limit, force_timeout, st);
     SMAX_CUDA(cudaGetLastError());
 }
 

@@ -44,10 +44,10 @@ struct LevelPack {
     bool needs_x_init = false;  // some entry reads a solution not computed before it
     // sync-free packs (row_sources): entries name the source ROW in the
     // caller's numbering, never a ring slot, and `tasks` lists the warp tasks
-    // in sweep order: (level, first row of the level), 32 rows each, so a
-    // warp's rows never depend on one another
+    // in sweep order, up to 32 rows of one level each, so a warp's rows never
+    // depend on one another
     bool row_sources = false;
-    DevBuf tasks;  // int2[n_tasks]
+    DevBuf tasks;  // int4[n_tasks]: first position, rows | width << 6, level rows, first entry
     int n_tasks = 0;
     int n_levels() const { return (int)h_lv.size(); }
 };

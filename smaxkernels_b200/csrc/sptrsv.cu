@@ -429,6 +429,11 @@ void TriPlan::release_graph() {
 
 TriPlan::~TriPlan() { release_graph(); }
 
+bool syncfree_suits(const TriPlan &p) {
+    const int64_t L = p.n_levels();
+    return p.n_rows >= (1 << 17) && L > 0 && p.n_rows >= L * 32768;
+}
+
 template <typename VT>
 bool tri_solve_syncfree(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, uint64_t tag, DevBuf &ctl,
                         long long limit, bool force_timeout, DevStatus *st, cudaStream_t s) {

@@ -115,6 +115,9 @@ void tri_solve_raw(TriPlan &p, const int *rp, const int *ci, const VT *val, cons
 // The sync-free solve of one right-hand side (pack_solve_syncfree).  Returns
 // false, launching nothing, when it does not apply: the matrix does not pack,
 // an entry reads a row not solved before it, or B and X overlap.
+// Whether the default scheme (SMAX_SOLVE_AUTO, one right-hand side) runs
+// sync-free: at least 2^17 rows in levels of 32768 rows on average.
+bool syncfree_suits(const TriPlan &p);
 template <typename VT>
 bool tri_solve_syncfree(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, uint64_t tag, DevBuf &ctl,
                         long long limit, bool force_timeout, DevStatus *st, cudaStream_t s);

@@ -105,3 +105,4 @@ def test_wide_levels_adjoint():
     assert normwise(lam, lam_ref) <= 1e-12
     assert normwise(dval, dval_ref) <= 1e-12
     smax.close()
+
