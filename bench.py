@@ -520,7 +520,8 @@ def wl_sptrsv(b: Bench):
     rhs = M.uniform_vector(n, 3)
     names = {1: "per_level", 2: "merged", 3: "graph", 4: "persistent", 5: "syncfree"}
     results, xs = {}, {}
-    modes = [int(m) for m in b.args.tri_modes.split(",")]
+    cases = b.args.tri_cases.split(",")
+    modes = [int(m) for m in b.args.tri_modes.split(",")] if "natural" in cases else []
     for mode in [m for m in (1, 2, 3, 4, 5) if m in modes]:
         smax, k = b.kernel(KernelType.SPTRSV, vt, lambda k: k.set_solve_mode(mode))
         xd, bd = b.zeros(n, vt), b.dev(rhs)
@@ -547,67 +548,69 @@ def wl_sptrsv(b: Bench):
         smax.close()
     if b.args.tri_natural_only:
         return
-    # permuted flow: random symmetric permutation (seed 3), RS levels, level order
-    Ar, Ac, Av, _ = M.random_symmetric_permutation(*A, seed=3)
-    smax, k = b.kernel(KernelType.SPTRSV, vt)
-    perm = np.zeros(n, np.int32)
-    inv = np.zeros(n, np.int32)
-    smax.utils.generate_perm(n, Ar, Ac, perm, inv, "RS")
-    prp = np.zeros(n + 1, np.int32)
-    pcol = np.zeros(len(Ac), np.int32)
-    pval = np.zeros(len(Ac))
-    smax.utils.apply_mat_perm(n, Ar, Ac, Av, prp, pcol, pval, perm, inv)
-    lrp, lcol, lval = M.lower_triangle(prp, pcol, pval)
-    lvl = np.array([smax.get_level_ptr_at(i) for i in range(smax.get_n_levels() + 1)], np.int32)
-    nl = len(lvl) - 1
-    xs = {}
-    names[0] = "auto"
-    for mode in (3, 0, 4, 5):
-        smax.register_kernel(f"p{mode}", KernelType.SPTRSV, *b_types(vt))
-        k = smax.kernel(f"p{mode}")
-        k.set_mat_perm(True)
-        k.set_solve_mode(mode)
-        xd, bd = b.zeros(n, vt), b.dev(rhs)
-        k.register_A(n, n, len(lcol), lcol.copy(), lrp, lval.copy())
-        k.register_B(n, xd)
-        k.register_C(n, bd)
+    if "permuted" in cases:
+        # permuted flow: random symmetric permutation (seed 3), RS levels, level order
+        Ar, Ac, Av, _ = M.random_symmetric_permutation(*A, seed=3)
+        smax, k = b.kernel(KernelType.SPTRSV, vt)
+        perm = np.zeros(n, np.int32)
+        inv = np.zeros(n, np.int32)
+        smax.utils.generate_perm(n, Ar, Ac, perm, inv, "RS")
+        prp = np.zeros(n + 1, np.int32)
+        pcol = np.zeros(len(Ac), np.int32)
+        pval = np.zeros(len(Ac))
+        smax.utils.apply_mat_perm(n, Ar, Ac, Av, prp, pcol, pval, perm, inv)
+        lrp, lcol, lval = M.lower_triangle(prp, pcol, pval)
+        lvl = np.array([smax.get_level_ptr_at(i) for i in range(smax.get_n_levels() + 1)], np.int32)
+        nl = len(lvl) - 1
+        xs = {}
+        names[0] = "auto"
+        for mode in [int(m) for m in b.args.tri_permuted_modes.split(",")]:
+            smax.register_kernel(f"p{mode}", KernelType.SPTRSV, *b_types(vt))
+            k = smax.kernel(f"p{mode}")
+            k.set_mat_perm(True)
+            k.set_solve_mode(mode)
+            xd, bd = b.zeros(n, vt), b.dev(rhs)
+            k.register_A(n, n, len(lcol), lcol.copy(), lrp, lval.copy())
+            k.register_B(n, xd)
+            k.register_C(n, bd)
+            k.set_stream(b.stream.cuda_stream)
+            k.initialize()
+            nbytes = _tri_bytes(n, len(lcol), vb)
+            with b.clocks() as clk:
+                t, reps = b.time(k.apply, budget_s=2.0, max_reps=200)
+            xs[mode] = xd.clone()
+            same = bool(b.torch.equal(xs[mode], xs[3])) if 3 in xs else None
+            cpu = None
+            if mode == 3:
+                cpu = b.cpu(lambda: b.ref.time_sptrsv(lrp, lcol, lval, rhs, levels=lvl, warm=1, reps=5)[0], nbytes,
+                            "5 solves after 1 warm-up (reference crs_sptrsv_lvl, OpenMP within levels)")
+            b.emit(f"sptrsv_f64_laplace2d_{side}_permuted_{names[mode]}", "SpTRSV GB/s", nbytes / t / 1e9, "GB/s", t,
+                   reps, "f64", {"n_rows": n, "nnz": len(lcol), "levels": nl, "scheme": names[mode],
+                                 "ordering": "random symmetric permutation (seed 3), RS level order"},
+                   clk.summary(), b.hbm(nbytes, t, "syncfree_kernel" if mode in (0, 5) else "wide_level_kernel/sweep_kernel"),
+                   cpu, launches=reps if mode == 4 else (2 * reps if mode in (0, 5) else None),
+                   us_per_level=round(t * 1e6 / max(nl, 1), 4), bitwise_equal_to_graph=same)
+        smax.close()
+    if "sptrsm" in cases:
+        # SpTRSM, k = 32 right-hand sides, row-major
+        kv = 32
+        B = np.random.default_rng(3).uniform(-1, 1, n * kv)
+        smax, k = b.kernel(KernelType.SPTRSM, vt, lambda k: k.set_vec_row_major(True))
+        Xd, Bd = b.zeros(n * kv, vt), b.dev(B)
+        k.register_A(n, n, nnz, col.copy(), rp, val.copy())
+        k.register_B(n, kv, Xd)
+        k.register_C(n, kv, Bd)
         k.set_stream(b.stream.cuda_stream)
         k.initialize()
-        nbytes = _tri_bytes(n, len(lcol), vb)
+        nbytes = _tri_bytes(n, nnz, vb, kv)
         with b.clocks() as clk:
-            t, reps = b.time(k.apply, budget_s=2.0, max_reps=200)
-        xs[mode] = xd.clone()
-        same = bool(b.torch.equal(xs[mode], xs[3])) if 3 in xs else None
-        cpu = None
-        if mode == 3:
-            cpu = b.cpu(lambda: b.ref.time_sptrsv(lrp, lcol, lval, rhs, levels=lvl, warm=1, reps=5)[0], nbytes,
-                        "5 solves after 1 warm-up (reference crs_sptrsv_lvl, OpenMP within levels)")
-        b.emit(f"sptrsv_f64_laplace2d_{side}_permuted_{names[mode]}", "SpTRSV GB/s", nbytes / t / 1e9, "GB/s", t,
-               reps, "f64", {"n_rows": n, "nnz": len(lcol), "levels": nl, "scheme": names[mode],
-                             "ordering": "random symmetric permutation (seed 3), RS level order"},
-               clk.summary(), b.hbm(nbytes, t, "syncfree_kernel" if mode in (0, 5) else "wide_level_kernel/sweep_kernel"),
-               cpu, launches=reps if mode == 4 else (2 * reps if mode in (0, 5) else None),
-               us_per_level=round(t * 1e6 / max(nl, 1), 4), bitwise_equal_to_graph=same)
-    smax.close()
-    # SpTRSM, k = 32 right-hand sides, row-major
-    kv = 32
-    B = np.random.default_rng(3).uniform(-1, 1, n * kv)
-    smax, k = b.kernel(KernelType.SPTRSM, vt, lambda k: k.set_vec_row_major(True))
-    Xd, Bd = b.zeros(n * kv, vt), b.dev(B)
-    k.register_A(n, n, nnz, col.copy(), rp, val.copy())
-    k.register_B(n, kv, Xd)
-    k.register_C(n, kv, Bd)
-    k.set_stream(b.stream.cuda_stream)
-    k.initialize()
-    nbytes = _tri_bytes(n, nnz, vb, kv)
-    with b.clocks() as clk:
-        t, reps = b.time(k.apply, budget_s=2.0, max_reps=50)
-    cpu = b.cpu(lambda: b.ref.time_sptrsm(rp, col, val, B, kv, True, warm=0, reps=1), nbytes,
-                "1 solve (reference naive row-major SpTRSM, serial)")
-    b.emit(f"sptrsm_k32_f64_laplace2d_{side}_natural_graph", "SpTRSM GB/s", nbytes / t / 1e9, "GB/s", t, reps,
-           "f64", {"n_rows": n, "nnz": nnz, "k": kv, "levels": n_lv, "layout": "row-major"}, clk.summary(),
-           b.hbm(nbytes, t, "level_kernel/segment_kernel"), cpu, us_per_level=round(t * 1e6 / n_lv, 4))
-    smax.close()
+            t, reps = b.time(k.apply, budget_s=2.0, max_reps=50)
+        cpu = b.cpu(lambda: b.ref.time_sptrsm(rp, col, val, B, kv, True, warm=0, reps=1), nbytes,
+                    "1 solve (reference naive row-major SpTRSM, serial)")
+        b.emit(f"sptrsm_k32_f64_laplace2d_{side}_natural_graph", "SpTRSM GB/s", nbytes / t / 1e9, "GB/s", t, reps,
+               "f64", {"n_rows": n, "nnz": nnz, "k": kv, "levels": n_lv, "layout": "row-major"}, clk.summary(),
+               b.hbm(nbytes, t, "level_kernel/segment_kernel"), cpu, us_per_level=round(t * 1e6 / n_lv, 4))
+        smax.close()
 
 
 def b_types(vt):
@@ -1081,6 +1084,10 @@ def main():
     ap.add_argument("--tri-side", type=int, default=2048, help="sptrsv workload: grid side of the Laplacian")
     ap.add_argument("--tri-modes", default="1,2,3,4,5", help="sptrsv workload: solve modes of the natural case")
     ap.add_argument("--tri-natural-only", action="store_true", help="sptrsv workload: natural order only")
+    ap.add_argument("--tri-cases", default="natural,permuted,sptrsm",
+                    help="sptrsv workload: cases to run (natural, permuted, sptrsm)")
+    ap.add_argument("--tri-permuted-modes", default="3,0,4,5",
+                    help="sptrsv workload: solve modes of the permuted case (0 = the default scheme)")
     ap.add_argument("--extra-dtype", default="both", choices=("both", "f64", "f32"),
                     help="scs_spmv / spmm workloads: value types to run")
     ap.add_argument("--spmm-k", default="16,64", help="spmm workload: vector counts")
