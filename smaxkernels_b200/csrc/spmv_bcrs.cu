@@ -84,15 +84,25 @@ __global__ void __launch_bounds__(256) bcrs_stream_kernel(const int *__restrict_
     // the products in step order (the same sums as the one-step loop); for
     // short block rows the registers this takes cost more occupancy than the
     // overlap gains, so it is compiled out (UNROLL false)
-    if constexpr (UNROLL)
+    // The column indices are loaded one iteration ahead, so an iteration's x
+    // gathers wait on no load of their own.
+    if constexpr (UNROLL) {
+    int cn[4] = {0, 0, 0, 0};
+    if (f + 3 * STEP < end)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) cn[u] = col[(f + u * STEP) / bs];
     for (; f + 3 * STEP < end; f += 4 * STEP) {
         VT v[4][VEC];
         int64_t c[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             load16<VT, VEC>(val + f + u * STEP, v[u]);
-            c[u] = (int64_t)col[(f + u * STEP) / bs] * wpad;
+            c[u] = (int64_t)cn[u] * wpad;
         }
+        const int64_t fn = f + 4 * STEP;
+        if (fn + 3 * STEP < end)
+#pragma unroll
+            for (int u = 0; u < 4; ++u) cn[u] = col[(fn + u * STEP) / bs];
         VT xv[4][VEC];
 #pragma unroll
         for (int u = 0; u < 4; ++u)
@@ -103,6 +113,7 @@ __global__ void __launch_bounds__(256) bcrs_stream_kernel(const int *__restrict_
 #pragma unroll
             for (int i = 0; i < VEC; ++i)
                 if (ok[i]) acc[i] += v[u][i] * xv[u][i];
+    }
     }
     for (; f < end; f += STEP) {
         const int64_t c = (int64_t)col[f / bs] * wpad;

@@ -206,6 +206,27 @@ def test_bcrs_random_vs_oracle(vt, shape, col_major):
     assert normwise(y[rows], y_ref[rows]) <= tol(vt)
 
 
+@pytest.mark.parametrize("vt", [np.float64, np.float32])
+@pytest.mark.parametrize("shape", [(4, 4, 4, 4), (2, 2, 2, 2), (8, 8, 8, 8), (3, 3, 4, 4)])
+@pytest.mark.parametrize("col_major", [False, True])
+def test_bcrs_long_block_rows_vs_oracle(vt, shape, col_major):
+    """Block rows of many blocks (the bulk-copy stream path): warp tasks of
+    several block rows, chunks that end inside a row, empty block rows and
+    one block row longer than a task."""
+    bh, bw, hp, wp = shape
+    n = 600 * bh
+    nc = 700 * bw
+    rp, col, val = rand_crs(n, 120, 43, vt=vt, n_cols=nc, empty_frac=0.15, long_rows=(2500,))
+    smax = _iface()
+    b = smax.utils.convert_crs_to_bcrs(n, nc, len(col), col, rp, val, bh, bw, hp, wp, col_major)
+    smax.close()
+    x = np.random.default_rng(44).uniform(-1, 1, (nc // bw) * wp).astype(vt)
+    y = gpu_bcrs_spmv(b, x, col_major)
+    y_ref = O.spmv_bcrs(b["n_rows"], bh, bw, hp, wp, b["row_ptr"], b["col"], b["val"], col_major, x)
+    rows = np.concatenate([np.arange(r * hp, r * hp + bh) for r in range(b["n_rows"])])
+    assert normwise(y[rows], y_ref[rows]) <= tol(vt)
+
+
 def test_bcrs_conversion_rejects_bad_blocks():
     from smaxkernels_b200 import SmaxError
     rp, col, val = rand_crs(10, 3, 1)
