@@ -34,10 +34,29 @@ __device__ __forceinline__ void spmm_row(int64_t row, int g, unsigned gmask, con
 #pragma unroll
         for (int i = 0; i < VEC; ++i) acc[m][i] = VT(0);
     const int s = row_ptr[row], e = row_ptr[row + 1];
+    // FP32: the group's next G (col, val) pairs are loaded while the current
+    // ones are used (k = 16 / 64 on the 27-point stencil: 7 % / 4 % faster);
+    // FP64: the extra registers cost more occupancy than the overlap gains
+    constexpr bool kAhead = sizeof(VT) == 4;
+    int nc = 0;
+    VT nv = VT(0);
+    if (kAhead && s + g < e) {
+        nc = ld_stream(col + s + g);
+        nv = ld_stream(val + s + g);
+    }
     for (int j0 = s; j0 < e; j0 += G) {
         const int jj = j0 + g;
-        const int myc = jj < e ? ld_stream(col + jj) : 0;
-        const VT myv = jj < e ? ld_stream(val + jj) : VT(0);
+        int myc;
+        VT myv;
+        if constexpr (kAhead) {
+            myc = nc;
+            myv = nv;
+            nc = jj + G < e ? ld_stream(col + jj + G) : 0;
+            nv = jj + G < e ? ld_stream(val + jj + G) : VT(0);
+        } else {
+            myc = jj < e ? ld_stream(col + jj) : 0;
+            myv = jj < e ? ld_stream(val + jj) : VT(0);
+        }
         const int cnt = min(G, e - j0);
         // unrolled so the X-row loads of consecutive entries overlap; holding
         // more rows in registers lowered occupancy and was measured slower
