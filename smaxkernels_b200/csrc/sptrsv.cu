@@ -27,6 +27,8 @@
 // replayed (tri_solve_graph).
 #include "sptrsv.cuh"
 
+#include <algorithm>
+
 namespace smax {
 
 namespace {
@@ -294,20 +296,66 @@ void TriPlan::schedule(int64_t k, int merge_rows) {
         const int lv = level_at(l);
         const int64_t m = lvl_ptr[lv + 1] - lvl_ptr[lv];
         if (merge_rows > 0 && m * k <= merge_rows) {
-            Step s;
-            s.kind = 1;
-            s.seg_first = (int)seg_ranges.size();
-            s.sweep_first = l;
+            const int l0 = l;
             while (l < L) {
                 const int lv2 = level_at(l);
                 const int64_t m2 = lvl_ptr[lv2 + 1] - lvl_ptr[lv2];
                 if (m2 * k > merge_rows) break;
-                seg_ranges.push_back({lvl_ptr[lv2], lvl_ptr[lv2 + 1]});
                 ++l;
             }
-            s.seg_count = (int)seg_ranges.size() - s.seg_first;
-            s.sweep_count = s.seg_count;
-            steps.push_back(s);
+            // One right-hand side: the run's single-CTA sweep is sized by its
+            // widest level (256 / 512 / 1024 threads for up to 512 / 1024 /
+            // more rows), and every warp of it passes every level.  Long
+            // stretches of narrower levels become runs of their own, on fewer
+            // threads; stretches shorter than kMinStretch levels stay with a
+            // neighbour (a run boundary costs a launch, and the first level of
+            // a run reads its sources from global memory instead of the ring).
+            std::vector<std::pair<int, int>> parts;  // (first sweep step, width class)
+            auto width_class = [&](int idx) {
+                const int lv2 = level_at(idx);
+                const int64_t m2 = lvl_ptr[lv2 + 1] - lvl_ptr[lv2];
+                return k == 1 ? (m2 <= 512 ? 0 : (m2 <= 1024 ? 1 : 2)) : 0;
+            };
+            for (int i = l0; i < l; ++i) {
+                const int c = width_class(i);
+                if (parts.empty() || parts.back().second != c) parts.push_back({i, c});
+            }
+            constexpr int kMinStretch = 64;
+            for (bool changed = true; changed && parts.size() > 1;) {
+                changed = false;
+                for (size_t i = 0; i < parts.size(); ++i) {
+                    const int end = i + 1 < parts.size() ? parts[i + 1].first : l;
+                    if (end - parts[i].first >= kMinStretch) continue;
+                    // merge the short stretch into its wider neighbour
+                    size_t j;
+                    if (i == 0) j = 1;
+                    else if (i + 1 == parts.size()) j = i - 1;
+                    else j = parts[i - 1].second >= parts[i + 1].second ? i - 1 : i + 1;
+                    const size_t lo = std::min(i, j);
+                    parts[lo].second = std::max(parts[i].second, parts[j].second);
+                    parts.erase(parts.begin() + (long)(lo + 1));
+                    // neighbours of equal class join
+                    if (lo + 1 < parts.size() && parts[lo + 1].second == parts[lo].second)
+                        parts.erase(parts.begin() + (long)(lo + 1));
+                    if (lo > 0 && parts[lo - 1].second == parts[lo].second) parts.erase(parts.begin() + (long)lo);
+                    changed = true;
+                    break;
+                }
+            }
+            for (size_t pi = 0; pi < parts.size(); ++pi) {
+                const int a = parts[pi].first, b = pi + 1 < parts.size() ? parts[pi + 1].first : l;
+                Step s;
+                s.kind = 1;
+                s.seg_first = (int)seg_ranges.size();
+                s.sweep_first = a;
+                for (int i = a; i < b; ++i) {
+                    const int lv2 = level_at(i);
+                    seg_ranges.push_back({lvl_ptr[lv2], lvl_ptr[lv2 + 1]});
+                }
+                s.seg_count = (int)seg_ranges.size() - s.seg_first;
+                s.sweep_count = s.seg_count;
+                steps.push_back(s);
+            }
         } else {
             Step s;
             s.kind = 0;
