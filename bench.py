@@ -188,7 +188,8 @@ def run_reference(args):
         steps = min(steps, 20)
     t, threads, kind, n = cpu_reference_time(rp, col, val, x, reps=steps, warm=warm)
     gbs = nbytes / t / 1e9
-    line = {"impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": UNIT, "n_gpus": 0,
+    # n_gpus: the launch's N (the reference runs on the host cores of rank 0)
+    line = {"impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": UNIT, "n_gpus": args.gpus,
             "steps": n, "warmup": warm, "ms_per_step": round(t * 1e3, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": args.dtype,
             "data": "synthetic (seeded lognormal CRS matrix)",
