@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(T, 1)
 
 // ------------------------------------------------------------ sync-free --
 constexpr int kSfThreads = 256;
-constexpr int kSfChunk = 32;  // warp tasks a CTA claims at once
+constexpr int kSfChunk = 8;   // warp tasks a CTA claims at once (one per warp)
 constexpr int kSfEnts = 4;    // entries of a row loaded before its first wait
 
 // "not solved yet": signalling-NaN patterns; arithmetic never returns a
