@@ -593,26 +593,34 @@ def wl_sptrsv(b: Bench):
                    us_per_level=round(t * 1e6 / max(nl, 1), 4), bitwise_equal_to_graph=same)
         smax.close()
     if "sptrsm" in cases:
-        # SpTRSM, k = 32 right-hand sides, row-major
+        # SpTRSM, k = 32 right-hand sides, row-major: graph-captured level
+        # launches, then the default (the sync-free row kernel for this schedule)
         kv = 32
         B = np.random.default_rng(3).uniform(-1, 1, n * kv)
-        smax, k = b.kernel(KernelType.SPTRSM, vt, lambda k: k.set_vec_row_major(True))
-        Xd, Bd = b.zeros(n * kv, vt), b.dev(B)
-        k.register_A(n, n, nnz, col.copy(), rp, val.copy())
-        k.register_B(n, kv, Xd)
-        k.register_C(n, kv, Bd)
-        k.set_stream(b.stream.cuda_stream)
-        k.initialize()
-        nbytes = _tri_bytes(n, nnz, vb, kv)
-        with b.clocks() as clk:
-            t, reps = b.time(k.apply, budget_s=2.0, max_reps=50)
-        cpu = b.cpu(lambda: b.ref.time_sptrsm(rp, col, val, B, kv, True, warm=0, reps=1), nbytes,
-                    "1 solve (reference naive row-major SpTRSM, serial)")
-        b.emit(f"sptrsm_k32_f64_laplace2d_{side}_natural_graph", "SpTRSM GB/s", nbytes / t / 1e9, "GB/s", t, reps,
-               "f64", {"n_rows": n, "nnz": nnz, "k": kv, "levels": n_lv, "layout": "row-major"}, clk.summary(),
-               b.hbm(nbytes, t, "level_kernel/segment_kernel"), cpu, us_per_level=round(t * 1e6 / n_lv, 4))
-        smax.close()
-
+        xs_m = {}
+        for mode in (3, 0):
+            smax, k = b.kernel(KernelType.SPTRSM, vt, lambda k: (k.set_vec_row_major(True), k.set_solve_mode(mode)))
+            Xd, Bd = b.zeros(n * kv, vt), b.dev(B)
+            k.register_A(n, n, nnz, col.copy(), rp, val.copy())
+            k.register_B(n, kv, Xd)
+            k.register_C(n, kv, Bd)
+            k.set_stream(b.stream.cuda_stream)
+            k.initialize()
+            nbytes = _tri_bytes(n, nnz, vb, kv)
+            with b.clocks() as clk:
+                t, reps = b.time(k.apply, budget_s=2.0, max_reps=50)
+            xs_m[mode] = Xd.clone()
+            same = bool(b.torch.equal(Xd, xs_m[3])) if mode != 3 else None
+            cpu = b.cpu(lambda: b.ref.time_sptrsm(rp, col, val, B, kv, True, warm=0, reps=1), nbytes,
+                        "1 solve (reference naive row-major SpTRSM, serial)") if mode == 3 else None
+            tag = "graph" if mode == 3 else "auto"
+            b.emit(f"sptrsm_k32_f64_laplace2d_{side}_natural_{tag}", "SpTRSM GB/s", nbytes / t / 1e9, "GB/s", t,
+                   reps, "f64", {"n_rows": n, "nnz": nnz, "k": kv, "levels": n_lv, "layout": "row-major",
+                                 "scheme": tag}, clk.summary(),
+                   b.hbm(nbytes, t, "level_kernel/segment_kernel" if mode == 3 else "syncfree_rows_kernel"), cpu,
+                   us_per_level=round(t * 1e6 / n_lv, 4), bitwise_equal_to_graph=same)
+            smax.close()
+            del Xd, Bd
 
 def b_types(vt):
     from smaxkernels_b200 import FloatType, IntType, PlatformType

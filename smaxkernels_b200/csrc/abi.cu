@@ -228,14 +228,13 @@ template <typename VT> void tri_apply_t(smax_kernel_s *k, const VT *Bv, VT *Xv) 
                                  k->force_timeout, k->spin_limit, k->stream);
         return;
     }
-    if (k->solve_mode == SMAX_SOLVE_SYNCFREE)
-        require(kk == 1, SMAX_ERR_UNSUPPORTED, "the sync-free solve handles one right-hand side");
-    // the default runs a schedule of few, wide levels sync-free: no barrier
-    // (launch) between levels
+    // the default runs sync-free (no barrier, no launch between levels) one
+    // right-hand side over few wide levels, and row-major blocks of k > 1 over
+    // many narrow ones
     if (k->solve_mode == SMAX_SOLVE_SYNCFREE ||
-        (k->solve_mode == SMAX_SOLVE_AUTO && kk == 1 && syncfree_suits(k->tri))) {
+        (k->solve_mode == SMAX_SOLVE_AUTO && (kk == 1 || rm) && syncfree_suits(k->tri, kk))) {
         if (tri_solve_syncfree<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, k->vals_version, k->sf_ctl, k->spin_limit,
-                                   k->force_timeout, dstatus(k), k->stream))
+                                   k->force_timeout, dstatus(k), k->stream, kk, rm))
             return;
         // not applicable to this matrix or these operands: the merged solve
     }

@@ -501,6 +501,50 @@ __global__ void __launch_bounds__(kSfThreads)
     }
 }
 
+// k > 1 right-hand sides, row-major (element (r, v) at r*k + v): a warp per
+// row with its lanes over the vectors, 32 at a time; a CTA claims 8
+// consecutive positions, one per warp, with one atomic.  Per row the plain
+// solves' arithmetic: x[r][v] = (b[r][v] - sum_j val[j] x[col[j]][v]) / D[r],
+// the off-diagonal entries in stored order (the diagonal is last in each row).
+template <typename VT>
+__global__ void __launch_bounds__(kSfThreads)
+    syncfree_rows_kernel(const int *__restrict__ prow, int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                         const VT *__restrict__ val, const VT *__restrict__ D, const VT *__restrict__ B, VT *X,
+                         int64_t k, int *ctl, long long limit, DevStatus *st) {
+    __shared__ int base_sh;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int *abort_flag = ctl + 1;
+    while (true) {
+        if (threadIdx.x == 0) base_sh = atomicAdd(ctl, kSfThreads / 32);
+        __syncthreads();
+        const int p0 = base_sh;
+        __syncthreads();  // base_sh is rewritten on the next turn
+        if (p0 >= n) return;
+        const int p = p0 + warp;
+        if (p >= n) continue;
+        const int r = prow[p];
+        const int s = rp[r], e = rp[r + 1] - 1;
+        const VT d = D[r];
+        for (int64_t v0 = 0; v0 < k; v0 += 32) {
+            const int64_t v = v0 + lane;
+            const bool act = v < k;
+            VT sum = VT(0);
+            for (int j0 = s; j0 < e; j0 += 32) {
+                const int jj = j0 + lane;
+                const int cj = jj < e ? ci[jj] : 0;
+                const VT aj = jj < e ? val[jj] : VT(0);
+                const int cnt = min(32, e - j0);
+                for (int t = 0; t < cnt; ++t) {
+                    const int c = __shfl_sync(0xffffffffu, cj, t);
+                    const VT a = __shfl_sync(0xffffffffu, aj, t);
+                    if (act) sum += a * solved(X + (int64_t)c * k + v, limit, abort_flag, st);
+                }
+            }
+            if (act) st_relaxed(X + (int64_t)r * k + v, (B[(int64_t)r * k + v] - sum) / d);
+        }
+    }
+}
+
 template <typename VT, int T> void set_smem_attr_t() {
     SMAX_CUDA(cudaFuncSetAttribute(sweep_kernel<VT, T, kRowsPerThread>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)(kRing * sizeof(VT))));
@@ -793,6 +837,39 @@ void pack_solve_syncfree(const LevelPack &pk, const VT *B, VT *X, void *ctl, lon
     SMAX_CUDA(cudaGetLastError());
 }
 
+template <typename VT>
+void solve_syncfree_rows(const LevelPack &pk, const int *rp, const int *ci, const VT *val, const VT *D, const VT *B,
+                         VT *X, int64_t k, void *ctl, long long limit, DevStatus *st, cudaStream_t s) {
+    if (pk.n == 0 || k == 0) return;
+    if (!pk.row_sources) fail(SMAX_ERR_STATE, "the sync-free solve needs a row-sourced pack");
+    int *c = static_cast<int *>(ctl);
+    sf_reset_kernel<VT><<<grid_for(pk.n * k), 256, 0, s>>>(X, pk.n * k, c);
+    static int per_sm_cache[64] = {};
+    int dev = 0;
+    SMAX_CUDA(cudaGetDevice(&dev));
+    int per_sm = dev >= 0 && dev < 64 ? per_sm_cache[dev] : 0;
+    if (per_sm == 0) {
+        SMAX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, syncfree_rows_kernel<VT>, kSfThreads, 0));
+        if (per_sm < 1) per_sm = 1;
+        if (dev >= 0 && dev < 64) per_sm_cache[dev] = per_sm;
+    }
+    constexpr int rows_per_claim = kSfThreads / 32;
+    const int64_t claims = (pk.n + rows_per_claim - 1) / rows_per_claim;
+    // about four levels' rows in flight, as for one right-hand side
+    const int64_t avg = pk.n / std::max(1, pk.n_levels());
+    const int64_t cap = std::max<int64_t>(8, (4 * avg + rows_per_claim - 1) / rows_per_claim);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>({claims, (int64_t)per_sm * sm_count(), cap}));
+    syncfree_rows_kernel<VT><<<grid, kSfThreads, 0, s>>>(pk.prow.as<int>(), (int)pk.n, rp, ci, val, D, B, X, k, c,
+                                                         limit, st);
+    SMAX_CUDA(cudaGetLastError());
+}
+
+template void solve_syncfree_rows<double>(const LevelPack &, const int *, const int *, const double *,
+                                          const double *, const double *, double *, int64_t, void *, long long,
+                                          DevStatus *, cudaStream_t);
+template void solve_syncfree_rows<float>(const LevelPack &, const int *, const int *, const float *, const float *,
+                                         const float *, float *, int64_t, void *, long long, DevStatus *,
+                                         cudaStream_t);
 template void pack_solve_syncfree<double>(const LevelPack &, const double *, double *, void *, long long, bool,
                                           DevStatus *, cudaStream_t);
 template void pack_solve_syncfree<float>(const LevelPack &, const float *, float *, void *, long long, bool,

@@ -477,28 +477,35 @@ void TriPlan::release_graph() {
 
 TriPlan::~TriPlan() { release_graph(); }
 
-bool syncfree_suits(const TriPlan &p) {
+bool syncfree_suits(const TriPlan &p, int64_t k) {
     const int64_t L = p.n_levels();
-    return p.n_rows >= (1 << 17) && L > 0 && p.n_rows >= L * 32768;
+    if (L <= 0) return false;
+    if (k == 1) return p.n_rows >= (1 << 17) && p.n_rows >= L * 32768;
+    return p.n_rows >= (1 << 16) && L >= 64 && p.n_rows <= L * 16384;
 }
 
 template <typename VT>
 bool tri_solve_syncfree(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, uint64_t tag, DevBuf &ctl,
-                        long long limit, bool force_timeout, DevStatus *st, cudaStream_t s) {
-    if (p.n_rows == 0) return true;
+                        long long limit, bool force_timeout, DevStatus *st, cudaStream_t s, int64_t k,
+                        bool row_major) {
+    if (p.n_rows == 0 || k == 0) return true;
+    if (k > 1 && !row_major) return false;
     const uintptr_t b0 = reinterpret_cast<uintptr_t>(B), x0 = reinterpret_cast<uintptr_t>(X);
-    const uintptr_t len = sizeof(VT) * (uintptr_t)p.n_rows;
+    const uintptr_t len = sizeof(VT) * (uintptr_t)p.n_rows * (uintptr_t)k;
     if (b0 < x0 + len && x0 < b0 + len) return false;  // B is read while X fills
     if (!p.ensure_syncfree(a.rp(), a.ci(), a.val.p, D, sizeof(VT), tag, s)) return false;
     ctl.ensure(64);
-    pack_solve_syncfree<VT>(p.sf_pack, B, X, ctl.p, limit, force_timeout, st, s);
+    if (k == 1)
+        pack_solve_syncfree<VT>(p.sf_pack, B, X, ctl.p, limit, force_timeout, st, s);
+    else
+        solve_syncfree_rows<VT>(p.sf_pack, a.rp(), a.ci(), a.val.as<VT>(), D, B, X, k, ctl.p, limit, st, s);
     return true;
 }
 
 template bool tri_solve_syncfree<double>(TriPlan &, const DevCRS &, const double *, const double *, double *, uint64_t,
-                                         DevBuf &, long long, bool, DevStatus *, cudaStream_t);
+                                         DevBuf &, long long, bool, DevStatus *, cudaStream_t, int64_t, bool);
 template bool tri_solve_syncfree<float>(TriPlan &, const DevCRS &, const float *, const float *, float *, uint64_t,
-                                        DevBuf &, long long, bool, DevStatus *, cudaStream_t);
+                                        DevBuf &, long long, bool, DevStatus *, cudaStream_t, int64_t, bool);
 template void tri_solve<double>(TriPlan &, const DevCRS &, const double *, const double *, double *, int64_t, bool,
                                 int64_t, int, uint64_t, cudaStream_t);
 template void tri_solve<float>(TriPlan &, const DevCRS &, const float *, const float *, float *, int64_t, bool,

@@ -115,12 +115,18 @@ void tri_solve_raw(TriPlan &p, const int *rp, const int *ci, const VT *val, cons
 // The sync-free solve of one right-hand side (pack_solve_syncfree).  Returns
 // false, launching nothing, when it does not apply: the matrix does not pack,
 // an entry reads a row not solved before it, or B and X overlap.
-// Whether the default scheme (SMAX_SOLVE_AUTO, one right-hand side) runs
-// sync-free: at least 2^17 rows in levels of 32768 rows on average.
-bool syncfree_suits(const TriPlan &p);
+// Whether the default scheme (SMAX_SOLVE_AUTO) runs sync-free.  One
+// right-hand side: at least 2^17 rows in levels of 32768 rows or more on
+// average (few wide levels, whose launches the sync-free solve saves).  k > 1
+// in row-major blocks: at least 2^16 rows in 64 levels or more of at most
+// 16384 rows on average (many narrow levels, launch-bound as level launches).
+bool syncfree_suits(const TriPlan &p, int64_t k = 1);
+// k > 1 runs the row-major kernel (solve_syncfree_rows); column-major blocks
+// do not apply.
 template <typename VT>
 bool tri_solve_syncfree(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, uint64_t tag, DevBuf &ctl,
-                        long long limit, bool force_timeout, DevStatus *st, cudaStream_t s);
+                        long long limit, bool force_timeout, DevStatus *st, cudaStream_t s, int64_t k = 1,
+                        bool row_major = true);
 // The same launch sequence, captured once into a CUDA graph and replayed.
 template <typename VT>
 void tri_solve_graph(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, int64_t k, bool row_major,

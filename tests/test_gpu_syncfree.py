@@ -223,3 +223,61 @@ def test_autotune_considers_syncfree():
     assert r["n_candidates"] >= 9
     assert r["solve_mode"] in (2, 3, 4, 5)
     assert normwise(x, O.sptrsv(lrp, lcol, lval, b)) <= 1e-12
+
+
+# ------------------------------------------------ SpTRSM, row-major blocks --
+def _solve_m(rp, col, val, B, k_, mode, row_major=True, upper=False):
+    from smaxkernels_b200 import FloatType, Interface, IntType, KernelType, PlatformType
+    n = len(rp) - 1
+    smax = Interface()
+    smax.register_kernel("t", KernelType.SPTRSM, PlatformType.CUDA, IntType.INT32,
+                         FloatType.FLOAT64 if val.dtype == np.float64 else FloatType.FLOAT32)
+    k = smax.kernel("t")
+    k.set_solve_mode(mode)
+    if mode == MERGED:
+        k.set_level_merge(0)
+    if upper:
+        k.set_mat_upper_triang(True)
+    X = np.zeros(n * k_, val.dtype)
+    k.register_A(n, n, len(col), col.copy(), rp, val.copy())
+    k.register_B(n, k_, X)
+    k.register_C(n, k_, np.ascontiguousarray(B, val.dtype))
+    k.set_vec_row_major(row_major)
+    k.run()
+    smax.close()
+    return X
+
+
+@pytest.mark.parametrize("vt", [np.float64, np.float32])
+@pytest.mark.parametrize("k_", [2, 32, 40])
+@pytest.mark.parametrize("upper", [False, True])
+def test_syncfree_sptrsm_row_major(vt, k_, upper):
+    """A warp per row, lanes over the right-hand sides (two passes for 40):
+    the plain kernels' arithmetic, so the merged solve's bits."""
+    rp, col, val = rand_crs(2500, 7, 81, vt=vt, lower=True)
+    if upper:
+        rp, col, val = _upper(rp, col, val)
+    B = np.random.default_rng(82).uniform(-1, 1, 2500 * k_).astype(vt)
+    X = _solve_m(rp, col, val, B, k_, SYNCFREE, upper=upper)
+    assert normwise(X, O.sptrsm(rp, col, val, B, k_, row_major=True, lower=not upper)) <= tol(vt)
+    np.testing.assert_array_equal(X, _solve_m(rp, col, val, B, k_, MERGED, upper=upper))
+
+
+def test_syncfree_sptrsm_laplace_natural_default():
+    """The natural 5-point 300^2 lower triangle with 32 right-hand sides
+    (90,000 rows, 599 levels): the default scheme runs it sync-free."""
+    from smaxkernels_b200 import matrices as M
+    lrp, lcol, lval = M.lower_triangle(*M.laplace2d_5pt(300))
+    n = len(lrp) - 1
+    B = np.random.default_rng(3).uniform(-1, 1, n * 32)
+    X = _solve_m(lrp, lcol, lval, B, 32, 0)
+    assert normwise(X, O.sptrsm(lrp, lcol, lval, B, 32, row_major=True)) <= 1e-12
+    np.testing.assert_array_equal(X, _solve_m(lrp, lcol, lval, B, 32, MERGED))
+
+
+def test_syncfree_sptrsm_column_major_falls_back():
+    rp, col, val = rand_crs(1200, 6, 83, lower=True)
+    B = np.random.default_rng(84).uniform(-1, 1, 1200 * 5)
+    X = _solve_m(rp, col, val, B, 5, SYNCFREE, row_major=False)
+    np.testing.assert_array_equal(X, _solve_m(rp, col, val, B, 5, MERGED, row_major=False))
+    assert normwise(X, O.sptrsm(rp, col, val, B, 5, row_major=False)) <= 1e-12
