@@ -351,6 +351,38 @@ __global__ void __launch_bounds__(kSmallThreads)
 
 // (D+L) has its diagonal as the last entry of every row (the SpTRSV kernel's
 // peeled copy) and is solved level by level over `order`
+// A thread's first row of level l of the Gauss-Seidel sweep (r = -1: none):
+// its row index, entry range and first two entries (diagonal last, so e is
+// the diagonal's slot), right-hand side and 1/D.
+template <typename VT> struct GsRow {
+    int r, j, e, c0, c1;
+    VT v0, v1, t, d;
+};
+
+template <typename VT>
+__device__ __forceinline__ GsRow<VT> gs_row(int l, int n_levels, const int *lvl_ptr, const int *order,
+                                            const int *lrp, const int *lci, const VT *lval, const VT *tmp,
+                                            const VT *D) {
+    GsRow<VT> g{-1, 0, 0, 0, 0, VT(0), VT(0), VT(0), VT(0)};
+    if (l >= n_levels) return g;
+    const int i = lvl_ptr[l] + (int)threadIdx.x;
+    if (i >= lvl_ptr[l + 1]) return g;
+    g.r = order[i];
+    g.j = lrp[g.r];
+    g.e = lrp[g.r + 1] - 1;
+    if (g.j < g.e) {
+        g.c0 = lci[g.j];
+        g.v0 = lval[g.j];
+    }
+    if (g.j + 1 < g.e) {
+        g.c1 = lci[g.j + 1];
+        g.v1 = lval[g.j + 1];
+    }
+    g.t = tmp[g.r];
+    g.d = D[g.r];
+    return g;
+}
+
 template <typename VT>
 __global__ void __launch_bounds__(kSmallThreads)
     small_gauss_seidel(const int *__restrict__ arp, const int *__restrict__ aci, const VT *__restrict__ aval,
@@ -402,8 +434,23 @@ __global__ void __launch_bounds__(kSmallThreads)
             tmp[r] = b[r] - s;
         }
         __syncthreads();
+        // Each thread's first row of the next level -- its row index, its
+        // first two entries, its right-hand side and 1/D -- is loaded while
+        // the current level is solved, so a level's chain is only the reads
+        // of x, the products and the store.  Further rows of a level wider
+        // than the CTA are read in place.
+        GsRow<VT> cur = gs_row<VT>(0, n_levels, lvl_ptr, order, lrp_s, lci_s, lval_s, tmp, D);
         for (int l = 0; l < n_levels; ++l) {
-            for (int i = lvl_ptr[l] + threadIdx.x; i < lvl_ptr[l + 1]; i += blockDim.x) {
+            const GsRow<VT> nxt = gs_row<VT>(l + 1, n_levels, lvl_ptr, order, lrp_s, lci_s, lval_s, tmp, D);
+            if (cur.r >= 0) {
+                VT s = VT(0);
+                if (cur.j < cur.e) s += cur.v0 * x[cur.c0];
+                if (cur.j + 1 < cur.e) s += cur.v1 * x[cur.c1];
+#pragma unroll 4
+                for (int j = cur.j + 2; j < cur.e; ++j) s += lval_s[j] * x[lci_s[j]];
+                x[cur.r] = (cur.t - s) * cur.d;
+            }
+            for (int i = lvl_ptr[l] + threadIdx.x + blockDim.x; i < lvl_ptr[l + 1]; i += blockDim.x) {
                 const int r = order[i];
                 VT s = VT(0);
                 const int e = lrp_s[r + 1] - 1;
@@ -412,6 +459,7 @@ __global__ void __launch_bounds__(kSmallThreads)
                 x[r] = (tmp[r] - s) * D[r];
             }
             __syncthreads();
+            cur = nxt;
         }
         ++it;
         if (it % cl == 0) {
