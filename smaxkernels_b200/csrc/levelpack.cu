@@ -407,7 +407,7 @@ __device__ __forceinline__ void st_relaxed(float *p, float v) {
 template <typename VT>
 __device__ __noinline__ VT wait_solved(const VT *p, long long limit, int *abort_flag, DevStatus *st) {
     for (long long it = 1;; ++it) {
-        __nanosleep(64);
+        if (it > 32) __nanosleep(64);  // the first polls back to back: most waits are short
         const VT v = ld_relaxed(p);
         if (!Pending<VT>::is(v)) return v;
         if ((it & 63) == 0 && *(volatile int *)abort_flag) return VT(NAN);
