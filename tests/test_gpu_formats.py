@@ -227,6 +227,24 @@ def test_bcrs_long_block_rows_vs_oracle(vt, shape, col_major):
     assert normwise(y[rows], y_ref[rows]) <= tol(vt)
 
 
+@pytest.mark.parametrize("vt", [np.float64, np.float32])
+@pytest.mark.parametrize("col_major", [False, True])
+def test_bcrs_short_block_rows_laplace(vt, col_major):
+    """The 7-point 32^3 Laplacian in 4x4 blocks: under two warp steps per block
+    row, so a lane group per block row (odd and even block counts per row)."""
+    from smaxkernels_b200 import matrices as M
+    rp, col, val = M.laplace3d_7pt(32, dtype=vt)
+    n = len(rp) - 1
+    smax = _iface()
+    b = smax.utils.convert_crs_to_bcrs(n, n, len(col), col, rp, val, 4, 4, 4, 4, col_major)
+    smax.close()
+    x = np.random.default_rng(45).uniform(-1, 1, n).astype(vt)
+    y = gpu_bcrs_spmv(b, x, col_major)
+    y_ref = O.spmv_bcrs(b["n_rows"], 4, 4, 4, 4, b["row_ptr"], b["col"], b["val"], col_major, x)
+    assert normwise(y, y_ref) <= tol(vt)
+    assert normwise(y, O.spmv_crs(rp, col, val.astype(np.float64), x.astype(np.float64))) <= tol(vt)
+
+
 def test_bcrs_conversion_rejects_bad_blocks():
     from smaxkernels_b200 import SmaxError
     rp, col, val = rand_crs(10, 3, 1)
