@@ -193,9 +193,11 @@ def run_reference(args):
             "steps": n, "warmup": warm, "ms_per_step": round(t * 1e3, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": args.dtype,
             "data": "synthetic (seeded lognormal CRS matrix)",
-            "config": config_dict(len(col), vbytes, 1),
+            "config": config_dict(len(col), vbytes, max(args.gpus, 1)),
             "cpu_baseline": {"value": round(gbs, 3), "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": f"{n} full applies of the workload after {warm} warm-up applies"},
+                             "sample": f"{n} full applies of the workload after {warm} warm-up applies"
+                                       + ("" if args.gpus <= 1 else
+                                          " (the 2^22-row matrix of one rank: the per-rank block of the weak-scaled job)")},
             "e2e": {"value": round(gbs, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
