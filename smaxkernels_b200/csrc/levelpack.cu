@@ -255,75 +255,92 @@ template <int CS> __device__ __forceinline__ void run_barrier() {
     else cooperative_groups::this_cluster().sync();  // barrier.cluster arrive.release / wait.acquire
 }
 
+// One level s of a run: loads level s+1's rows into `nxt` (and prefetches
+// level s+2 into L2) while it solves level s from `cur`, then the run's
+// barrier.  Returns level s+2's descriptor.
+template <typename VT, int T, int CS, int NR>
+__device__ __forceinline__ Level sweep_level(const Level *__restrict__ lv, int s, int s1, const Level &Lc,
+                                             const Level &Ln, const int *__restrict__ psrc,
+                                             const VT *__restrict__ pval, const VT *__restrict__ pinv,
+                                             const VT *__restrict__ bp, VT *xp, VT *ring, int g, int warp0,
+                                             unsigned rank, RowRegs<VT> (&cur)[NR], RowRegs<VT> (&nxt)[NR]) {
+    constexpr int G = T * CS;
+    const Level Lnn = load_level(lv, s + 2 < s1 ? s + 2 : s);
+    if (s + 1 < s1 && warp0 < Ln.m) load_rows<VT, T, CS, NR>(Ln, g, psrc, pval, pinv, bp, nxt);
+    if (s + 2 < s1) prefetch_level_l2<VT>(Lnn, g, psrc, pval, pinv, bp);
+    if (warp0 < Lc.m) {
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+            const int t = g + k * G;
+            if (t < Lc.m) {
+                VT sum = VT(0);
+                bool more = true;
+#pragma unroll
+                for (int i = 0; i < kEnts; ++i) {
+                    const int src = cur[k].src[i];
+                    if (src == kPad) { more = false; break; }
+                    sum += cur[k].v[i] * solution<VT, CS>(src, ring, xp, rank);
+                }
+                if (more)
+                    for (int i = kEnts; i < Lc.w; ++i) {
+                        const int idx = Lc.base + i * Lc.m + t;
+                        const int src = psrc[idx];
+                        if (src == kPad) break;
+                        sum += pval[idx] * solution<VT, CS>(src, ring, xp, rank);
+                    }
+                const int p = Lc.pos + t;
+                const VT x = (cur[k].b - sum) * cur[k].inv;
+                ring[p & (kRing - 1)] = x;
+                xp[p] = x;
+            }
+        }
+        // rows beyond the register slots (levels wider than the slots cover)
+        for (int t = g + NR * G; t < Lc.m; t += G) {
+            VT sum = VT(0);
+            for (int i = 0; i < Lc.w; ++i) {
+                const int idx = Lc.base + i * Lc.m + t;
+                const int src = psrc[idx];
+                if (src == kPad) break;
+                sum += pval[idx] * solution<VT, CS>(src, ring, xp, rank);
+            }
+            const int p = Lc.pos + t;
+            const VT x = (bp[p] - sum) * pinv[p];
+            ring[p & (kRing - 1)] = x;
+            xp[p] = x;
+        }
+    }
+    // every CTA of a cluster passes this barrier after its last level too,
+    // so no CTA leaves while another may still read its ring
+    run_barrier<CS>();
+    return Lnn;
+}
+
 // Sweeps steps [s0, s1) of the pack with CS CTAs of T threads (one CTA or one
 // cluster); thread g of the run solves rows g, g + T*CS, ... of every level,
-// the first NR of them from registers loaded one level ahead.
+// the first NR of them from registers loaded one level ahead.  Two register
+// sets alternate between "this level" and "the next", two levels per turn,
+// so no set is copied into the other.
 template <typename VT, int T, int CS, int NR = kRowsPerThread>
 __device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const int *__restrict__ psrc,
                           const VT *__restrict__ pval, const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp,
                           VT *ring) {
     if (s0 >= s1) return;
-    constexpr int G = T * CS;
     unsigned rank = 0;
     if constexpr (CS > 1) rank = cooperative_groups::this_cluster().block_rank();
     const int g = (int)rank * T + (int)threadIdx.x;
     const int warp0 = g & ~31;
-    RowRegs<VT> cur[NR], nxt[NR];
-    Level Lc = load_level(lv, s0);
-    Level Ln = load_level(lv, s0 + 1 < s1 ? s0 + 1 : s0);
-    load_rows<VT, T, CS, NR>(Lc, g, psrc, pval, pinv, bp, cur);
-    for (int s = s0; s < s1; ++s) {
-        const Level Lnn = load_level(lv, s + 2 < s1 ? s + 2 : s);
-        if (s + 1 < s1 && warp0 < Ln.m) load_rows<VT, T, CS, NR>(Ln, g, psrc, pval, pinv, bp, nxt);
-        if (s + 2 < s1) prefetch_level_l2<VT>(Lnn, g, psrc, pval, pinv, bp);
-        if (warp0 < Lc.m) {
-#pragma unroll
-            for (int k = 0; k < NR; ++k) {
-                const int t = g + k * G;
-                if (t < Lc.m) {
-                    VT sum = VT(0);
-                    bool more = true;
-#pragma unroll
-                    for (int i = 0; i < kEnts; ++i) {
-                        const int src = cur[k].src[i];
-                        if (src == kPad) { more = false; break; }
-                        sum += cur[k].v[i] * solution<VT, CS>(src, ring, xp, rank);
-                    }
-                    if (more)
-                        for (int i = kEnts; i < Lc.w; ++i) {
-                            const int idx = Lc.base + i * Lc.m + t;
-                            const int src = psrc[idx];
-                            if (src == kPad) break;
-                            sum += pval[idx] * solution<VT, CS>(src, ring, xp, rank);
-                        }
-                    const int p = Lc.pos + t;
-                    const VT x = (cur[k].b - sum) * cur[k].inv;
-                    ring[p & (kRing - 1)] = x;
-                    xp[p] = x;
-                }
-            }
-            // rows beyond the register slots (levels wider than the slots cover)
-            for (int t = g + NR * G; t < Lc.m; t += G) {
-                VT sum = VT(0);
-                for (int i = 0; i < Lc.w; ++i) {
-                    const int idx = Lc.base + i * Lc.m + t;
-                    const int src = psrc[idx];
-                    if (src == kPad) break;
-                    sum += pval[idx] * solution<VT, CS>(src, ring, xp, rank);
-                }
-                const int p = Lc.pos + t;
-                const VT x = (bp[p] - sum) * pinv[p];
-                ring[p & (kRing - 1)] = x;
-                xp[p] = x;
-            }
-        }
-        // every CTA of a cluster passes this barrier after its last level too,
-        // so no CTA leaves while another may still read its ring
-        run_barrier<CS>();
-        Lc = Ln;
-        Ln = Lnn;
-#pragma unroll
-        for (int k = 0; k < NR; ++k) cur[k] = nxt[k];
+    RowRegs<VT> ra[NR], rb[NR];
+    Level La = load_level(lv, s0);
+    Level Lb = load_level(lv, s0 + 1 < s1 ? s0 + 1 : s0);
+    load_rows<VT, T, CS, NR>(La, g, psrc, pval, pinv, bp, ra);
+    for (int s = s0; s < s1; s += 2) {
+        const Level L2 =
+            sweep_level<VT, T, CS, NR>(lv, s, s1, La, Lb, psrc, pval, pinv, bp, xp, ring, g, warp0, rank, ra, rb);
+        if (s + 1 >= s1) break;
+        const Level L3 = sweep_level<VT, T, CS, NR>(lv, s + 1, s1, Lb, L2, psrc, pval, pinv, bp, xp, ring, g, warp0,
+                                                    rank, rb, ra);
+        La = L2;
+        Lb = L3;
     }
 }
 
