@@ -6,15 +6,15 @@
 // y is produced in the permuted order (y[perm[r]] is row r of the CRS product).
 //
 // SpMV (SPMV::CPU::naive_scs_spmv, src/kernels/spmv/spmv_cpu/spmv_cpu_scs_impl.hpp:9-49):
-//   * C a multiple of VEC = 16 / sizeof(VT) and C/VEC <= 32: warp tasks of at
+//   * C a multiple of VEC = 2 and C/VEC <= 32: warp tasks of at
 //     most kScsTaskCols chunk columns (a long chunk -- sigma sorting puts the
 //     longest rows together -- is split over several warps, whose partial
 //     sums a fix-up pass adds in task order, so no warp holds a long tail);
-//     each lane owns VEC adjacent rows and reads them with one 128-bit load per
+//     each lane owns VEC adjacent rows and reads them with one 8- or 16-byte load per
 //     chunk column, so C/VEC lanes cover a chunk column and the warp covers
 //     32*VEC/C columns per instruction (chunk-column-major, fully coalesced);
 //     the lanes holding the same rows combine with shuffles at the end and y is
-//     stored with 128-bit stores.
+//     stored with vector stores.
 //   * any other C: one thread per row, consecutive threads on consecutive rows.
 //
 // Conversion (Utils::convert_crs_to_scs): row lengths, a per-sigma-window sort
@@ -35,13 +35,13 @@ namespace {
 
 template <typename VT> struct Vec;
 template <> struct Vec<double> { using T = double2; static constexpr int N = 2; };
-template <> struct Vec<float> { using T = float4; static constexpr int N = 4; };
+// FP32 lanes own two rows too (8-byte loads): with four, each lane held
+// sixteen gathers in flight and the registers cost occupancy
+template <> struct Vec<float> { using T = float2; static constexpr int N = 2; };
 
 template <typename VT> __device__ __forceinline__ void vec_get(const typename Vec<VT>::T &v, VT *o);
 template <> __device__ __forceinline__ void vec_get<double>(const double2 &v, double *o) { o[0] = v.x; o[1] = v.y; }
-template <> __device__ __forceinline__ void vec_get<float>(const float4 &v, float *o) {
-    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
-}
+template <> __device__ __forceinline__ void vec_get<float>(const float2 &v, float *o) { o[0] = v.x; o[1] = v.y; }
 
 // one warp per chunk; LPC = C / VEC lanes per chunk column
 template <typename VT, int LPC>
@@ -275,7 +275,8 @@ __global__ void scs_scatter_kernel(const int *__restrict__ row_ptr, const int *_
 }  // namespace
 
 bool scs_vector_path(int64_t C, int vbytes) {
-    const int vec = 16 / vbytes;
+    (void)vbytes;
+    const int vec = 2;  // Vec<VT>::N for both value types
     return C % vec == 0 && C / vec >= 1 && C / vec <= 32 && ((C / vec) & (C / vec - 1)) == 0;
 }
 
