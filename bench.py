@@ -1232,7 +1232,9 @@ def main():
     y_dev = y.cpu().numpy()
     if ke is not None:
         rel = float(np.linalg.norm(yh.numpy() - y_dev) / max(np.linalg.norm(y_dev), 1e-300))
-        if rel > 1e-12:
+        # the host path's row blocks cut the entry slices elsewhere, so the
+        # sums round differently: the parity tolerance of the value type
+        if rel > (1e-12 if args.dtype == "f64" else 1e-5):
             raise RuntimeError(f"host-path and device-path results differ: {rel}")
 
     total_bytes = bytes_rank * world

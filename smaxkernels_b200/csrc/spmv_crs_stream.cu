@@ -33,7 +33,9 @@ constexpr int kWarpsPerCta = 8;  // 256-thread CTAs
 
 template <typename VT> struct StreamCfg;
 template <> struct StreamCfg<double> { static constexpr int U = 4; };
-template <> struct StreamCfg<float> { static constexpr int U = 8; };
+// FP32 lanes take four entries too (16-byte column and value loads): with
+// eight, each lane held eight gathers in flight and registers cost occupancy
+template <> struct StreamCfg<float> { static constexpr int U = 4; };
 
 // U consecutive entries of col and val starting at a multiple of U.
 template <typename VT, int U> struct Chunk;
@@ -48,18 +50,14 @@ template <> struct Chunk<double, 4> {
         v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
     }
 };
-template <> struct Chunk<float, 8> {
-    int c[8];
-    float v[8];
+template <> struct Chunk<float, 4> {
+    int c[4];
+    float v[4];
     __device__ __forceinline__ void load(const int *col, const float *val, int64_t e) {
-        int4 c0 = __ldcs(reinterpret_cast<const int4 *>(col + e));
-        int4 c1 = __ldcs(reinterpret_cast<const int4 *>(col + e + 4));
+        int4 ci = __ldcs(reinterpret_cast<const int4 *>(col + e));
         float4 a = __ldcs(reinterpret_cast<const float4 *>(val + e));
-        float4 b = __ldcs(reinterpret_cast<const float4 *>(val + e + 4));
-        c[0] = c0.x; c[1] = c0.y; c[2] = c0.z; c[3] = c0.w;
-        c[4] = c1.x; c[5] = c1.y; c[6] = c1.z; c[7] = c1.w;
+        c[0] = ci.x; c[1] = ci.y; c[2] = ci.z; c[3] = ci.w;
         v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-        v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
     }
 };
 
