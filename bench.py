@@ -1086,6 +1086,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--pipe-blocks", type=int, default=None,
+                    help="e2e: row blocks of the host-pointer SpMV pipeline (default: the library's)")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=N_ROWS, help="rows per rank (default 2^22)")
@@ -1205,6 +1207,8 @@ def main():
         if args.e2e_steps > 0:
             smax.register_kernel("spmv_host", KernelType.SPMV, PlatformType.CUDA, IntType.INT32, ft)
             ke = smax.kernel("spmv_host")
+            if args.pipe_blocks is not None:
+                ke._flag("spmv_pipeline", args.pipe_blocks)
             if args.variant:
                 ke.set_spmv_variant(args.variant)
             xh = torch.empty(n_cols, dtype=tdt).pin_memory()
