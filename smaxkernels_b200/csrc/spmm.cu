@@ -216,10 +216,12 @@ void crs_spmm_row_major(const DevCRS &a, int64_t k, const VT *X, VT *Y, cudaStre
     case 8: launch_rm<VT, 8, 1, VEC>(a, k, X, Y, st, w); break;
     // 16 and 32 vectors: 8 lanes per row with 2 / 4 vectors each (k = 64 on
     // the 27-point stencil: FP32 0.99 -> 0.84 ms, FP64 2.05 -> 1.58 ms against
-    // one vector per lane); more vectors per lane cost occupancy
+    // one vector per lane); 64 vectors: 16 lanes with 4 each (k = 128 FP64
+    // 2.91 -> 2.85 ms, k = 256 FP32 2.84 -> 2.73 ms); more vectors per lane
+    // cost occupancy
     case 16: launch_rm<VT, 8, 2, VEC>(a, k, X, Y, st, w); break;
     case 32: launch_rm<VT, 8, 4, VEC>(a, k, X, Y, st, w); break;
-    case 64: launch_rm<VT, 32, 2, VEC>(a, k, X, Y, st, w); break;
+    case 64: launch_rm<VT, 16, 4, VEC>(a, k, X, Y, st, w); break;
     case 128: launch_rm<VT, 32, 4, VEC>(a, k, X, Y, st, w); break;
     default: done = false;
     }
