@@ -103,14 +103,14 @@ typedef int smax_status;
 /* SpTRSV / SpTRSM launch schemes (SMAX_FLAG_SOLVE_MODE) */
 #define SMAX_SOLVE_AUTO 0        /* the default: SMAX_SOLVE_SYNCFREE for one right-hand side and few wide
                                     levels (>= 2^17 rows, >= 32768 rows per level on average) and for
-                                    row-major SpTRSM over many narrow levels (>= 2^16 rows, >= 64 levels,
+                                    SpTRSM over many narrow levels (>= 2^16 rows, >= 64 levels,
                                     <= 16384 rows per level on average), else SMAX_SOLVE_GRAPH */
 #define SMAX_SOLVE_PER_LEVEL 1   /* one kernel launch per level, no merging, no graph */
 #define SMAX_SOLVE_MERGED 2      /* narrow levels merged into single-CTA runs, no graph */
 #define SMAX_SOLVE_GRAPH 3       /* the merged launch sequence captured into a CUDA graph */
 #define SMAX_SOLVE_PERSISTENT 4  /* one cooperative launch, bounded grid barrier per level (SpTRSV, k = 1) */
 #define SMAX_SOLVE_SYNCFREE 5    /* one launch, no level barriers: each row waits (bounded) on the rows it reads
-                                    (SpTRSV, and SpTRSM with row-major blocks; falls back to SMAX_SOLVE_MERGED
+                                    (SpTRSV and SpTRSM, both block layouts; falls back to SMAX_SOLVE_MERGED
                                     where it does not apply) */
 
 typedef struct smax_ctx_s *smax_ctx;

@@ -229,10 +229,10 @@ template <typename VT> void tri_apply_t(smax_kernel_s *k, const VT *Bv, VT *Xv) 
         return;
     }
     // the default runs sync-free (no barrier, no launch between levels) one
-    // right-hand side over few wide levels, and row-major blocks of k > 1 over
-    // many narrow ones
+    // right-hand side over few wide levels, and blocks of k > 1 over many
+    // narrow ones
     if (k->solve_mode == SMAX_SOLVE_SYNCFREE ||
-        (k->solve_mode == SMAX_SOLVE_AUTO && (kk == 1 || rm) && syncfree_suits(k->tri, kk))) {
+        (k->solve_mode == SMAX_SOLVE_AUTO && syncfree_suits(k->tri, kk))) {
         if (tri_solve_syncfree<VT>(k->tri, k->dA, k->D.as<VT>(), Bv, Xv, k->vals_version, k->sf_ctl, k->spin_limit,
                                    k->force_timeout, dstatus(k), k->stream, kk, rm))
             return;

@@ -120,7 +120,7 @@ void tune_kernel(smax_kernel_s *k, smax_tuning &r) {
             cands.push_back({SMAX_SOLVE_PERSISTENT, 0, false});
             cands.push_back({SMAX_SOLVE_SYNCFREE, 0, false});
         }
-        if (k->ktype == SMAX_KERNEL_SPTRSM && k->f_row_major) cands.push_back({SMAX_SOLVE_SYNCFREE, 0, false});
+        if (k->ktype == SMAX_KERNEL_SPTRSM) cands.push_back({SMAX_SOLVE_SYNCFREE, 0, false});
         for (const Cand &c : cands) {
             k->solve_mode = c.mode;
             k->level_merge = c.merge;

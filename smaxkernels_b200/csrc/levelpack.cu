@@ -518,7 +518,8 @@ __global__ void __launch_bounds__(kSfThreads)
     }
 }
 
-// k > 1 right-hand sides, row-major (element (r, v) at r*k + v): a warp per
+// k > 1 right-hand sides, element (r, v) at r*rs + v*vs (row-major: rs = k,
+// vs = 1; column-major: rs = 1, vs = the leading dimension): a warp per
 // row with its lanes over the vectors, 32 at a time; a CTA claims 8
 // consecutive positions, one per warp, with one atomic.  Per row the plain
 // solves' arithmetic: x[r][v] = (b[r][v] - sum_j val[j] x[col[j]][v]) / D[r],
@@ -527,7 +528,7 @@ template <typename VT>
 __global__ void __launch_bounds__(kSfThreads)
     syncfree_rows_kernel(const int *__restrict__ prow, int n, const int *__restrict__ rp, const int *__restrict__ ci,
                          const VT *__restrict__ val, const VT *__restrict__ D, const VT *__restrict__ B, VT *X,
-                         int64_t k, int *ctl, long long limit, DevStatus *st) {
+                         int64_t k, int64_t rs, int64_t vs, int *ctl, long long limit, DevStatus *st) {
     __shared__ int base_sh;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int *abort_flag = ctl + 1;
@@ -554,10 +555,10 @@ __global__ void __launch_bounds__(kSfThreads)
                 for (int t = 0; t < cnt; ++t) {
                     const int c = __shfl_sync(0xffffffffu, cj, t);
                     const VT a = __shfl_sync(0xffffffffu, aj, t);
-                    if (act) sum += a * solved(X + (int64_t)c * k + v, limit, abort_flag, st);
+                    if (act) sum += a * solved(X + (int64_t)c * rs + v * vs, limit, abort_flag, st);
                 }
             }
-            if (act) st_relaxed(X + (int64_t)r * k + v, (B[(int64_t)r * k + v] - sum) / d);
+            if (act) st_relaxed(X + (int64_t)r * rs + v * vs, (B[(int64_t)r * rs + v * vs] - sum) / d);
         }
     }
 }
@@ -856,7 +857,7 @@ void pack_solve_syncfree(const LevelPack &pk, const VT *B, VT *X, void *ctl, lon
 
 template <typename VT>
 void solve_syncfree_rows(const LevelPack &pk, const int *rp, const int *ci, const VT *val, const VT *D, const VT *B,
-                         VT *X, int64_t k, void *ctl, long long limit, DevStatus *st, cudaStream_t s) {
+                         VT *X, int64_t k, bool row_major, void *ctl, long long limit, DevStatus *st, cudaStream_t s) {
     if (pk.n == 0 || k == 0) return;
     if (!pk.row_sources) fail(SMAX_ERR_STATE, "the sync-free solve needs a row-sourced pack");
     int *c = static_cast<int *>(ctl);
@@ -876,16 +877,18 @@ void solve_syncfree_rows(const LevelPack &pk, const int *rp, const int *ci, cons
     const int64_t avg = pk.n / std::max(1, pk.n_levels());
     const int64_t cap = std::max<int64_t>(8, (4 * avg + rows_per_claim - 1) / rows_per_claim);
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>({claims, (int64_t)per_sm * sm_count(), cap}));
-    syncfree_rows_kernel<VT><<<grid, kSfThreads, 0, s>>>(pk.prow.as<int>(), (int)pk.n, rp, ci, val, D, B, X, k, c,
+    // column-major blocks: the leading dimension is the matrix's row count
+    const int64_t rs = row_major ? k : 1, vs = row_major ? 1 : pk.n;
+    syncfree_rows_kernel<VT><<<grid, kSfThreads, 0, s>>>(pk.prow.as<int>(), (int)pk.n, rp, ci, val, D, B, X, k, rs, vs, c,
                                                          limit, st);
     SMAX_CUDA(cudaGetLastError());
 }
 
 template void solve_syncfree_rows<double>(const LevelPack &, const int *, const int *, const double *,
-                                          const double *, const double *, double *, int64_t, void *, long long,
+                                          const double *, const double *, double *, int64_t, bool, void *, long long,
                                           DevStatus *, cudaStream_t);
 template void solve_syncfree_rows<float>(const LevelPack &, const int *, const int *, const float *, const float *,
-                                         const float *, float *, int64_t, void *, long long, DevStatus *,
+                                         const float *, float *, int64_t, bool, void *, long long, DevStatus *,
                                          cudaStream_t);
 template void pack_solve_syncfree<double>(const LevelPack &, const double *, double *, void *, long long, bool,
                                           DevStatus *, cudaStream_t);

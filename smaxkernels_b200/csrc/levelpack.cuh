@@ -93,13 +93,15 @@ template <typename VT>
 void pack_solve_syncfree(const LevelPack &pk, const VT *B, VT *X, void *ctl, long long limit, bool force_timeout,
                          DevStatus *st, cudaStream_t s);
 
-// The sync-free solve for k > 1 right-hand sides in row-major blocks, on the
-// matrix's own CRS arrays (diagonal last in each row) with the rows in the
-// sweep order of a row_sources pack: a warp per row, lanes over vectors,
-// bounded waits as above.  B and X (n * k values each) must not overlap.
+// The sync-free solve for k > 1 right-hand sides, on the matrix's own CRS
+// arrays (diagonal last in each row) with the rows in the sweep order of a
+// row_sources pack: a warp per row, lanes over vectors, bounded waits as
+// above.  Blocks are row-major (r*k + v) or column-major (r + v*n, the
+// matrix's row count as the leading dimension).  B and X (n * k values each)
+// must not overlap.
 template <typename VT>
 void solve_syncfree_rows(const LevelPack &pk, const int *rp, const int *ci, const VT *val, const VT *D, const VT *B,
-                         VT *X, int64_t k, void *ctl, long long limit, DevStatus *st, cudaStream_t s);
+                         VT *X, int64_t k, bool row_major, void *ctl, long long limit, DevStatus *st, cudaStream_t s);
 
 // One single-CTA sweep per matrix of a batch, matrices taken from a device
 // work queue: mat_steps[m] .. mat_steps[m+1] are matrix m's sweep steps.

@@ -489,7 +489,6 @@ bool tri_solve_syncfree(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, V
                         long long limit, bool force_timeout, DevStatus *st, cudaStream_t s, int64_t k,
                         bool row_major) {
     if (p.n_rows == 0 || k == 0) return true;
-    if (k > 1 && !row_major) return false;
     const uintptr_t b0 = reinterpret_cast<uintptr_t>(B), x0 = reinterpret_cast<uintptr_t>(X);
     const uintptr_t len = sizeof(VT) * (uintptr_t)p.n_rows * (uintptr_t)k;
     if (b0 < x0 + len && x0 < b0 + len) return false;  // B is read while X fills
@@ -498,7 +497,8 @@ bool tri_solve_syncfree(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, V
     if (k == 1)
         pack_solve_syncfree<VT>(p.sf_pack, B, X, ctl.p, limit, force_timeout, st, s);
     else
-        solve_syncfree_rows<VT>(p.sf_pack, a.rp(), a.ci(), a.val.as<VT>(), D, B, X, k, ctl.p, limit, st, s);
+        solve_syncfree_rows<VT>(p.sf_pack, a.rp(), a.ci(), a.val.as<VT>(), D, B, X, k, row_major, ctl.p, limit, st,
+                                s);
     return true;
 }
 

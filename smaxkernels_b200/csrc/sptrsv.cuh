@@ -117,12 +117,11 @@ void tri_solve_raw(TriPlan &p, const int *rp, const int *ci, const VT *val, cons
 // an entry reads a row not solved before it, or B and X overlap.
 // Whether the default scheme (SMAX_SOLVE_AUTO) runs sync-free.  One
 // right-hand side: at least 2^17 rows in levels of 32768 rows or more on
-// average (few wide levels, whose launches the sync-free solve saves).  k > 1
-// in row-major blocks: at least 2^16 rows in 64 levels or more of at most
-// 16384 rows on average (many narrow levels, launch-bound as level launches).
+// average (few wide levels, whose launches the sync-free solve saves).  k > 1:
+// at least 2^16 rows in 64 levels or more of at most 16384 rows on average
+// (many narrow levels, launch-bound as level launches).
 bool syncfree_suits(const TriPlan &p, int64_t k = 1);
-// k > 1 runs the row-major kernel (solve_syncfree_rows); column-major blocks
-// do not apply.
+// k > 1 runs the row kernel (solve_syncfree_rows), in either block layout.
 template <typename VT>
 bool tri_solve_syncfree(TriPlan &p, const DevCRS &a, const VT *D, const VT *B, VT *X, uint64_t tag, DevBuf &ctl,
                         long long limit, bool force_timeout, DevStatus *st, cudaStream_t s, int64_t k = 1,

@@ -275,9 +275,27 @@ def test_syncfree_sptrsm_laplace_natural_default():
     np.testing.assert_array_equal(X, _solve_m(lrp, lcol, lval, B, 32, MERGED))
 
 
-def test_syncfree_sptrsm_column_major_falls_back():
+@pytest.mark.parametrize("k_", [5, 33])
+@pytest.mark.parametrize("upper", [False, True])
+def test_syncfree_sptrsm_column_major(k_, upper):
+    """Column-major blocks (element (r, v) at r + v * n_rows, the reference's
+    leading dimension): the same row kernel with strided vectors."""
     rp, col, val = rand_crs(1200, 6, 83, lower=True)
-    B = np.random.default_rng(84).uniform(-1, 1, 1200 * 5)
-    X = _solve_m(rp, col, val, B, 5, SYNCFREE, row_major=False)
-    np.testing.assert_array_equal(X, _solve_m(rp, col, val, B, 5, MERGED, row_major=False))
-    assert normwise(X, O.sptrsm(rp, col, val, B, 5, row_major=False)) <= 1e-12
+    if upper:
+        rp, col, val = _upper(rp, col, val)
+    B = np.random.default_rng(84).uniform(-1, 1, 1200 * k_)
+    X = _solve_m(rp, col, val, B, k_, SYNCFREE, row_major=False, upper=upper)
+    np.testing.assert_array_equal(X, _solve_m(rp, col, val, B, k_, MERGED, row_major=False, upper=upper))
+    assert normwise(X, O.sptrsm(rp, col, val, B, k_, row_major=False, lower=not upper)) <= 1e-12
+
+
+def test_syncfree_sptrsm_column_major_natural_default():
+    """The natural 5-point 300^2 lower triangle, 8 column-major right-hand
+    sides: the default scheme runs it sync-free."""
+    from smaxkernels_b200 import matrices as M
+    lrp, lcol, lval = M.lower_triangle(*M.laplace2d_5pt(300))
+    n = len(lrp) - 1
+    B = np.random.default_rng(5).uniform(-1, 1, n * 8)
+    X = _solve_m(lrp, lcol, lval, B, 8, 0, row_major=False)
+    assert normwise(X, O.sptrsm(lrp, lcol, lval, B, 8, row_major=False)) <= 1e-12
+    np.testing.assert_array_equal(X, _solve_m(lrp, lcol, lval, B, 8, MERGED, row_major=False))
