@@ -1208,7 +1208,7 @@ def main():
             smax.register_kernel("spmv_host", KernelType.SPMV, PlatformType.CUDA, IntType.INT32, ft)
             ke = smax.kernel("spmv_host")
             if args.pipe_blocks is not None:
-                ke._flag("spmv_pipeline", args.pipe_blocks)
+                ke.set_spmv_pipeline(args.pipe_blocks)
             if args.variant:
                 ke.set_spmv_variant(args.variant)
             xh = torch.empty(n_cols, dtype=tdt).pin_memory()

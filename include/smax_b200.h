@@ -93,7 +93,7 @@ typedef int smax_status;
                                           0 auto (= 1), 1 a grid of all rows, 2 one CTA per SM walking a row range */
 #define SMAX_FLAG_SOLVE_MODE 11        /* SpTRSV/SpTRSM launch scheme, one of SMAX_SOLVE_* */
 #define SMAX_FLAG_LEVEL_MERGE 12       /* levels with <= this many rows*rhs run merged in one CTA (0: never) */
-#define SMAX_FLAG_SPIN_LIMIT 13        /* polls (x 1000) before a persistent solve's grid barrier times out */
+#define SMAX_FLAG_SPIN_LIMIT 13        /* polls (x 1000) before a wait of the persistent or sync-free solve times out */
 #define SMAX_FLAG_TEST_FORCE_TIMEOUT 14 /* test only: the persistent solve's barrier waits for a missing arrival */
 #define SMAX_FLAG_REFINE 15            /* float64 SpTRSV: solve in FP32, then this many FP64-residual corrections (0: off) */
 #define SMAX_FLAG_REFINE_TOL 16        /* stop refining once max|dx| <= 10^-value * max|x| (host check per step; 0: run all) */

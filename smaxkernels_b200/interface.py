@@ -226,8 +226,14 @@ class Kernel:
         return self._flag("kernel_impl", int(impl))
 
     def set_spmv_variant(self, v: int):
-        """CRS SpMV kernel: 0 auto, 1 warp-stream, 2 row-tile."""
+        """CRS SpMV kernel: 0 auto, 1 warp-stream, 2 row-tile.  Row-major SpMM:
+        0 auto, 1 a grid of all rows, 2 one CTA per SM walking a row range."""
         return self._flag("spmv_variant", v)
+
+    def set_spmv_pipeline(self, blocks: int):
+        """CRS SpMV with host operands: row blocks whose part of y is downloaded
+        while later blocks compute (default 4; 0 or 1: off)."""
+        return self._flag("spmv_pipeline", blocks)
 
     def set_solve_mode(self, mode: int):
         """SpTRSV/SpTRSM launch scheme: SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED, SOLVE_GRAPH,
@@ -235,7 +241,7 @@ class Kernel:
         return self._flag("solve_mode", mode)
 
     def set_spin_limit(self, kilo_polls: int):
-        """Polls (x 1000) before a persistent solve's grid barrier gives up with TIMEOUT."""
+        """Polls (x 1000) before a wait of the persistent or sync-free solve gives up with TIMEOUT."""
         return self._flag("spin_limit", kilo_polls)
 
     def set_sweep_cluster(self, v: bool):
