@@ -6,11 +6,11 @@
 // y is produced in the permuted order (y[perm[r]] is row r of the CRS product).
 //
 // SpMV (SPMV::CPU::naive_scs_spmv, src/kernels/spmv/spmv_cpu/spmv_cpu_scs_impl.hpp:9-49):
-//   * C a multiple of VEC = 2 and C/VEC <= 32: warp tasks of at
+//   * C a multiple of VEC (rows per lane, scs_vec: 1 or 2) and C/VEC <= 32: warp tasks of at
 //     most kScsTaskCols chunk columns (a long chunk -- sigma sorting puts the
 //     longest rows together -- is split over several warps, whose partial
 //     sums a fix-up pass adds in task order, so no warp holds a long tail);
-//     each lane owns VEC adjacent rows and reads them with one 8- or 16-byte load per
+//     each lane owns VEC adjacent rows and reads them with one load per
 //     chunk column, so C/VEC lanes cover a chunk column and the warp covers
 //     32*VEC/C columns per instruction (chunk-column-major, fully coalesced);
 //     the lanes holding the same rows combine with shuffles at the end and y is
@@ -33,26 +33,55 @@ namespace smax {
 
 namespace {
 
-template <typename VT> struct Vec;
-template <> struct Vec<double> { using T = double2; static constexpr int N = 2; };
-// FP32 lanes own two rows too (8-byte loads): with four, each lane held
-// sixteen gathers in flight and the registers cost occupancy
-template <> struct Vec<float> { using T = float2; static constexpr int N = 2; };
+// Rows per lane (VEC): FP64 lanes own one row when a chunk column fits in a
+// warp (C <= 32; two rows, 16-byte loads, for C = 64), FP32 lanes two rows
+// (8-byte loads).  More rows per lane put more gathers in flight per lane,
+// and the registers that costs lost occupancy (FP32 with four rows: 0.440 ms
+// against 0.398 ms on the lognormal 2^22 matrix).
+int scs_vec(int64_t C, int vbytes) { return vbytes == 8 ? (C <= 32 ? 1 : 2) : 2; }
 
-template <typename VT> __device__ __forceinline__ void vec_get(const typename Vec<VT>::T &v, VT *o);
-template <> __device__ __forceinline__ void vec_get<double>(const double2 &v, double *o) { o[0] = v.x; o[1] = v.y; }
-template <> __device__ __forceinline__ void vec_get<float>(const float2 &v, float *o) { o[0] = v.x; o[1] = v.y; }
+// VEC adjacent values / column indices from p (8-byte aligned for VEC == 2)
+template <typename VT, int VEC> __device__ __forceinline__ void load_vals(const VT *p, VT *o) {
+    static_assert(VEC == 1 || VEC == 2, "one or two rows per lane");
+    if constexpr (VEC == 1) {
+        o[0] = __ldcs(p);
+    } else if constexpr (sizeof(VT) == 8) {
+        const double2 t = __ldcs(reinterpret_cast<const double2 *>(p));
+        o[0] = t.x;
+        o[1] = t.y;
+    } else {
+        const float2 t = __ldcs(reinterpret_cast<const float2 *>(p));
+        o[0] = t.x;
+        o[1] = t.y;
+    }
+}
+template <int VEC> __device__ __forceinline__ void load_cols(const int *p, int *o) {
+    if constexpr (VEC == 1) {
+        o[0] = __ldcs(p);
+    } else {
+        const int2 t = __ldcs(reinterpret_cast<const int2 *>(p));
+        o[0] = t.x;
+        o[1] = t.y;
+    }
+}
+template <typename VT, int VEC> __device__ __forceinline__ void store_vals(VT *p, const VT *a) {
+    if constexpr (VEC == 1) {
+        __stcs(p, a[0]);
+    } else if constexpr (sizeof(VT) == 8) {
+        __stcs(reinterpret_cast<double2 *>(p), make_double2(a[0], a[1]));
+    } else {
+        __stcs(reinterpret_cast<float2 *>(p), make_float2(a[0], a[1]));
+    }
+}
 
 // one warp per chunk; LPC = C / VEC lanes per chunk column
-template <typename VT, int LPC>
+template <typename VT, int LPC, int VEC>
 __global__ void __launch_bounds__(256) scs_warp_kernel(const int *__restrict__ chunk_ptr,
                                                        const int *__restrict__ chunk_len, int64_t n_chunks,
                                                        const int *__restrict__ col, const VT *__restrict__ val,
                                                        const VT *__restrict__ x, VT *__restrict__ y) {
-    constexpr int VEC = Vec<VT>::N;
     constexpr int C = LPC * VEC;
     constexpr int CPI = 32 / LPC;  // chunk columns per warp instruction
-    using VV = typename Vec<VT>::T;
     const int lane = threadIdx.x & 31;
     const int64_t c = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
     if (c >= n_chunks) return;
@@ -66,15 +95,9 @@ __global__ void __launch_bounds__(256) scs_warp_kernel(const int *__restrict__ c
     for (int j = j0; j < len; j += CPI) {
         const int64_t idx = cs + (int64_t)j * C + sub * VEC;
         VT v[VEC];
-        vec_get<VT>(__ldcs(reinterpret_cast<const VV *>(val + idx)), v);
+        load_vals<VT, VEC>(val + idx, v);
         int cc[VEC];
-        if constexpr (VEC == 2) {
-            int2 t = __ldcs(reinterpret_cast<const int2 *>(col + idx));
-            cc[0] = t.x; cc[1] = t.y;
-        } else {
-            int4 t = __ldcs(reinterpret_cast<const int4 *>(col + idx));
-            cc[0] = t.x; cc[1] = t.y; cc[2] = t.z; cc[3] = t.w;
-        }
+        load_cols<VEC>(col + idx, cc);
 #pragma unroll
         for (int i = 0; i < VEC; ++i) acc[i] += v[i] * ld_keep(x + cc[i]);
     }
@@ -83,18 +106,13 @@ __global__ void __launch_bounds__(256) scs_warp_kernel(const int *__restrict__ c
     for (int o = LPC; o < 32; o <<= 1)
 #pragma unroll
         for (int i = 0; i < VEC; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
-    if (j0 == 0) {
-        VV out;
-        if constexpr (VEC == 2) { out.x = acc[0]; out.y = acc[1]; }
-        else { out.x = acc[0]; out.y = acc[1]; out.z = acc[2]; out.w = acc[3]; }
-        __stcs(reinterpret_cast<VV *>(y + c * C + sub * VEC), out);
-    }
+    if (j0 == 0) store_vals<VT, VEC>(y + c * C + sub * VEC, acc);
 }
 
 // One warp per task: chunk columns [j0, min(len, j0 + kScsTaskCols)) of one
 // chunk, unrolled four instructions deep so the gathers of several columns
 // are in flight together.
-template <typename VT, int LPC>
+template <typename VT, int LPC, int VEC>
 __global__ void __launch_bounds__(256) scs_task_kernel(const int *__restrict__ chunk_ptr,
                                                        const int *__restrict__ chunk_len,
                                                        const int *__restrict__ task_chunk,
@@ -103,10 +121,8 @@ __global__ void __launch_bounds__(256) scs_task_kernel(const int *__restrict__ c
                                                        const int *__restrict__ col, const VT *__restrict__ val,
                                                        const VT *__restrict__ x, VT *__restrict__ y,
                                                        VT *__restrict__ partial) {
-    constexpr int VEC = Vec<VT>::N;
     constexpr int C = LPC * VEC;
     constexpr int CPI = 32 / LPC;  // chunk columns per warp instruction
-    using VV = typename Vec<VT>::T;
     const int lane = threadIdx.x & 31;
     const int64_t t = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
     if (t >= n_tasks) return;
@@ -123,15 +139,9 @@ __global__ void __launch_bounds__(256) scs_task_kernel(const int *__restrict__ c
     auto step = [&](int jj) {
         const int64_t idx = cs + (int64_t)jj * C + sub * VEC;
         VT v[VEC];
-        vec_get<VT>(__ldcs(reinterpret_cast<const VV *>(val + idx)), v);
+        load_vals<VT, VEC>(val + idx, v);
         int cc[VEC];
-        if constexpr (VEC == 2) {
-            int2 q = __ldcs(reinterpret_cast<const int2 *>(col + idx));
-            cc[0] = q.x; cc[1] = q.y;
-        } else {
-            int4 q = __ldcs(reinterpret_cast<const int4 *>(col + idx));
-            cc[0] = q.x; cc[1] = q.y; cc[2] = q.z; cc[3] = q.w;
-        }
+        load_cols<VEC>(col + idx, cc);
 #pragma unroll
         for (int i = 0; i < VEC; ++i) acc[i] += v[i] * __ldcg(x + cc[i]);
     };
@@ -143,14 +153,8 @@ __global__ void __launch_bounds__(256) scs_task_kernel(const int *__restrict__ c
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int64_t idx = i0 + (int64_t)u * CPI * C;
-            vec_get<VT>(__ldcs(reinterpret_cast<const VV *>(val + idx)), v[u]);
-            if constexpr (VEC == 2) {
-                int2 q = __ldcs(reinterpret_cast<const int2 *>(col + idx));
-                cc[u][0] = q.x; cc[u][1] = q.y;
-            } else {
-                int4 q = __ldcs(reinterpret_cast<const int4 *>(col + idx));
-                cc[u][0] = q.x; cc[u][1] = q.y; cc[u][2] = q.z; cc[u][3] = q.w;
-            }
+            load_vals<VT, VEC>(val + idx, v[u]);
+            load_cols<VEC>(col + idx, cc[u]);
         }
         VT xv[4][VEC];
 #pragma unroll
@@ -168,11 +172,8 @@ __global__ void __launch_bounds__(256) scs_task_kernel(const int *__restrict__ c
 #pragma unroll
         for (int i = 0; i < VEC; ++i) acc[i] += __shfl_xor_sync(0xffffffffu, acc[i], o);
     if (lane < LPC) {
-        VV out;
-        if constexpr (VEC == 2) { out.x = acc[0]; out.y = acc[1]; }
-        else { out.x = acc[0]; out.y = acc[1]; out.z = acc[2]; out.w = acc[3]; }
         VT *dst = slot < 0 ? y + (int64_t)c * C : partial + (int64_t)slot * C;
-        __stcs(reinterpret_cast<VV *>(dst + sub * VEC), out);
+        store_vals<VT, VEC>(dst + sub * VEC, acc);
     }
 }
 
@@ -275,8 +276,7 @@ __global__ void scs_scatter_kernel(const int *__restrict__ row_ptr, const int *_
 }  // namespace
 
 bool scs_vector_path(int64_t C, int vbytes) {
-    (void)vbytes;
-    const int vec = 2;  // Vec<VT>::N for both value types
+    const int vec = scs_vec(C, vbytes);
     return C % vec == 0 && C / vec >= 1 && C / vec <= 32 && ((C / vec) & (C / vec - 1)) == 0;
 }
 
@@ -319,10 +319,42 @@ void scs_plan(DevSCS &m, int vbytes, cudaStream_t st) {
     SMAX_CUDA(cudaStreamSynchronize(st));
 }
 
+namespace {
+
+template <typename VT, int VEC>
+void launch_task(int64_t lpc, unsigned grid, const int *cp, const int *cl, const int *tc, const int *tj, const int *ts,
+                 int64_t n_tasks, const int *ci, const VT *v, const VT *x, VT *y, VT *part, cudaStream_t st) {
+    switch (lpc) {
+    case 1: scs_task_kernel<VT, 1, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part); break;
+    case 2: scs_task_kernel<VT, 2, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part); break;
+    case 4: scs_task_kernel<VT, 4, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part); break;
+    case 8: scs_task_kernel<VT, 8, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part); break;
+    case 16: scs_task_kernel<VT, 16, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part); break;
+    case 32: scs_task_kernel<VT, 32, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part); break;
+    default: fail(SMAX_ERR_STATE, "unexpected SELL chunk width");
+    }
+}
+
+template <typename VT, int VEC>
+void launch_warp(int64_t lpc, unsigned grid, const int *cp, const int *cl, int64_t n_chunks, const int *ci, const VT *v,
+                 const VT *x, VT *y, cudaStream_t st) {
+    switch (lpc) {
+    case 1: scs_warp_kernel<VT, 1, VEC><<<grid, 256, 0, st>>>(cp, cl, n_chunks, ci, v, x, y); break;
+    case 2: scs_warp_kernel<VT, 2, VEC><<<grid, 256, 0, st>>>(cp, cl, n_chunks, ci, v, x, y); break;
+    case 4: scs_warp_kernel<VT, 4, VEC><<<grid, 256, 0, st>>>(cp, cl, n_chunks, ci, v, x, y); break;
+    case 8: scs_warp_kernel<VT, 8, VEC><<<grid, 256, 0, st>>>(cp, cl, n_chunks, ci, v, x, y); break;
+    case 16: scs_warp_kernel<VT, 16, VEC><<<grid, 256, 0, st>>>(cp, cl, n_chunks, ci, v, x, y); break;
+    case 32: scs_warp_kernel<VT, 32, VEC><<<grid, 256, 0, st>>>(cp, cl, n_chunks, ci, v, x, y); break;
+    default: fail(SMAX_ERR_STATE, "unexpected SELL chunk width");
+    }
+}
+
+}  // namespace
+
 template <typename VT>
 void scs_spmv(const DevSCS &m, const VT *x, VT *y, cudaStream_t st) {
     if (m.n_chunks == 0) return;
-    const int vec = Vec<VT>::N;
+    const int vec = scs_vec(m.C, sizeof(VT));
     // y is written with 16-byte stores: an offset given to apply() may unalign it
     const bool y_aligned = (reinterpret_cast<uintptr_t>(y) & 15) == 0;
     if (y_aligned && scs_vector_path(m.C, sizeof(VT)) && m.plan_vbytes == (int)sizeof(VT) && m.n_tasks > 0) {
@@ -331,15 +363,8 @@ void scs_spmv(const DevSCS &m, const VT *x, VT *y, cudaStream_t st) {
         const int *tc = m.task_chunk.as<int>(), *tj = m.task_j0.as<int>(), *ts = m.task_slot.as<int>();
         const VT *v = m.val.as<VT>();
         VT *part = m.partial.as<VT>();
-        switch (m.C / vec) {
-        case 1: scs_task_kernel<VT, 1><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part); break;
-        case 2: scs_task_kernel<VT, 2><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part); break;
-        case 4: scs_task_kernel<VT, 4><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part); break;
-        case 8: scs_task_kernel<VT, 8><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part); break;
-        case 16: scs_task_kernel<VT, 16><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part); break;
-        case 32: scs_task_kernel<VT, 32><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part); break;
-        default: fail(SMAX_ERR_STATE, "unexpected SELL chunk width");
-        }
+        if (vec == 1) launch_task<VT, 1>(m.C, grid, cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part, st);
+        else launch_task<VT, 2>(m.C / 2, grid, cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part, st);
         if (m.n_multi > 0)
             scs_fixup_kernel<VT><<<ceil_div_u(m.n_multi * m.C, 256), 256, 0, st>>>(
                 m.multi_chunk.as<int>(), m.multi_first.as<int>(), m.multi_count.as<int>(), m.n_multi, (int)m.C, part,
@@ -348,15 +373,8 @@ void scs_spmv(const DevSCS &m, const VT *x, VT *y, cudaStream_t st) {
         const unsigned grid = ceil_div_u(m.n_chunks, 8);
         const int *cp = m.chunk_ptr.as<int>(), *cl = m.chunk_len.as<int>(), *ci = m.col.as<int>();
         const VT *v = m.val.as<VT>();
-        switch (m.C / vec) {
-        case 1: scs_warp_kernel<VT, 1><<<grid, 256, 0, st>>>(cp, cl, m.n_chunks, ci, v, x, y); break;
-        case 2: scs_warp_kernel<VT, 2><<<grid, 256, 0, st>>>(cp, cl, m.n_chunks, ci, v, x, y); break;
-        case 4: scs_warp_kernel<VT, 4><<<grid, 256, 0, st>>>(cp, cl, m.n_chunks, ci, v, x, y); break;
-        case 8: scs_warp_kernel<VT, 8><<<grid, 256, 0, st>>>(cp, cl, m.n_chunks, ci, v, x, y); break;
-        case 16: scs_warp_kernel<VT, 16><<<grid, 256, 0, st>>>(cp, cl, m.n_chunks, ci, v, x, y); break;
-        case 32: scs_warp_kernel<VT, 32><<<grid, 256, 0, st>>>(cp, cl, m.n_chunks, ci, v, x, y); break;
-        default: fail(SMAX_ERR_STATE, "unexpected SELL chunk width");
-        }
+        if (vec == 1) launch_warp<VT, 1>(m.C, grid, cp, cl, m.n_chunks, ci, v, x, y, st);
+        else launch_warp<VT, 2>(m.C / 2, grid, cp, cl, m.n_chunks, ci, v, x, y, st);
     } else {
         scs_thread_kernel<VT><<<ceil_div_u(m.n_rows_padded, 256), 256, 0, st>>>(
             m.chunk_ptr.as<int>(), m.chunk_len.as<int>(), m.C, m.n_rows_padded, m.col.as<int>(), m.val.as<VT>(),
