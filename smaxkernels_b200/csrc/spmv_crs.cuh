@@ -20,6 +20,8 @@ int crs_default_cap(int vbits);
 // mask, per-slice rank of the open row, carries for rows crossing slices.
 struct CrsStreamPlan {
     int64_t n_rows = 0, nnz = 0, n_tasks = 0, n_empty = 0, n_nonempty = 0;
+    const int *row_ptr = nullptr;  // the matrix's device row pointer given to build (not owned)
+    bool short_rows = true;        // no row has more than 32 entries: slices need no carries
     DevBuf endbits, task_rank, carry_val, carry_rank, row_list, empty_rows;
     void build(const int *d_row_ptr, int64_t n_rows, int64_t nnz, int vbytes, cudaStream_t st);
 };

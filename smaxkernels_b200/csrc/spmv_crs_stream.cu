@@ -15,7 +15,10 @@
 // lanes and chunks, and every row that ends inside the slice is written by
 // the lane holding its last entry.  The sum a slice holds for the row still
 // open at its end is written to carry[t]; a small fix-up pass then adds each
-// run of carries to its row in task order (deterministic).  Rows without
+// run of carries to its row in task order (deterministic).  When no row has
+// more than 32 entries, a slice instead sums the head of its first row (the
+// entries before the slice, at most 31) itself, one entry per lane, and
+// neither carries nor the fix-up launch are needed.  Rows without
 // entries get y = 0 from a separate list.  HBM traffic: val, col, one bit per
 // entry, one int per 512 entries, y; x is gathered through L2.
 #include "spmv_crs.cuh"
@@ -63,12 +66,24 @@ template <> struct Chunk<float, 4> {
 
 __device__ __forceinline__ int row_of_rank(const int *row_list, int q) { return row_list ? row_list[q] : q; }
 
+// Sum over the entries [rs, base) of the row open at a slice start, one entry
+// per lane (base - rs < 32), reduced in a fixed lane order.
 template <typename VT>
+__device__ __forceinline__ VT head_sum(const int *__restrict__ col, const VT *__restrict__ val,
+                                       const VT *__restrict__ x, int64_t rs, int64_t base, int lane) {
+    VT h = VT(0);
+    if (rs + lane < base) h = __ldg(val + rs + lane) * __ldcg(x + __ldg(col + rs + lane));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+    return h;
+}
+
+template <typename VT, bool SHORT>
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
     crs_stream_kernel(const int *__restrict__ col, const VT *__restrict__ val,
                       const uint32_t *__restrict__ endbits, const int *__restrict__ task_rank,
-                      const int *__restrict__ row_list, int64_t n_tasks, int n_nonempty,
-                      const VT *__restrict__ x, VT *__restrict__ y, VT *__restrict__ carry_val,
+                      const int *__restrict__ row_list, const int *__restrict__ row_ptr, int64_t n_tasks,
+                      int n_nonempty, const VT *__restrict__ x, VT *__restrict__ y, VT *__restrict__ carry_val,
                       int *__restrict__ carry_rank) {
     constexpr int U = StreamCfg<VT>::U;
     constexpr int CH = 32 * U;  // entries per chunk
@@ -79,12 +94,15 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32)
     if (t >= n_tasks) return;  // uniform per warp
     const int64_t base = t * kW;
     int q = task_rank[t];      // rank (among non-empty rows) of the row open at the slice start
-    VT carry = VT(0);          // partial sum of the open row, from this slice only
+    VT carry = VT(0);          // partial sum of the open row, from this slice only (SHORT: the whole row)
 
     Chunk<VT, U> cur;
     int64_t e0 = base + lane * U;
     cur.load(col, val, e0);
     uint32_t word = endbits[e0 >> 5];
+    // SHORT: every row has at most 32 entries, so the open row ends in this
+    // slice and at most 31 of its entries lie before it
+    if constexpr (SHORT) carry = head_sum(col, val, x, (int64_t)row_ptr[row_of_rank(row_list, q)], base, lane);
 
 #pragma unroll
     for (int k = 0; k < NC; ++k) {
@@ -156,7 +174,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32)
             e0 += CH;
         }
     }
-    if (lane == 0) {
+    if (!SHORT && lane == 0) {
         carry_val[t] = carry;
         carry_rank[t] = q < n_nonempty ? q : -1;
     }
@@ -182,7 +200,8 @@ __global__ void zero_rows(const int *__restrict__ rows, int64_t n, VT *__restric
 }
 
 __global__ void row_flags_kernel(const int *__restrict__ row_ptr, int64_t n, unsigned char *__restrict__ empty,
-                                 unsigned char *__restrict__ nonempty, uint32_t *__restrict__ endbits) {
+                                 unsigned char *__restrict__ nonempty, uint32_t *__restrict__ endbits,
+                                 int *__restrict__ max_len) {
     int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n) return;
     const int s = row_ptr[r], e = row_ptr[r + 1];
@@ -190,6 +209,7 @@ __global__ void row_flags_kernel(const int *__restrict__ row_ptr, int64_t n, uns
     empty[r] = em;
     nonempty[r] = !em;
     if (!em) atomicOr(endbits + ((e - 1) >> 5), 1u << ((e - 1) & 31));
+    if (e - s > 32) atomicMax(max_len, e - s);  // only "more than 32" matters
 }
 
 // rank of the row holding entry t*W: the largest r with row_ptr[r] <= t*W
@@ -229,10 +249,14 @@ void CrsStreamPlan::build(const int *d_row_ptr, int64_t n, int64_t nnz_, int vby
     SMAX_CUDA(cudaMemsetAsync(endbits.p, 0, endbits.bytes, st));
     n_empty = 0;
     n_nonempty = 0;
+    row_ptr = d_row_ptr;
+    short_rows = true;
     if (n > 0) {
-        DevBuf fe(n), fne(n), cnt(sizeof(int) * 2);
+        DevBuf fe(n), fne(n), cnt(sizeof(int) * 3);
+        SMAX_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes, st));
         row_flags_kernel<<<ceil_div_u(n, 256), 256, 0, st>>>(d_row_ptr, n, fe.as<unsigned char>(),
-                                                             fne.as<unsigned char>(), endbits.as<uint32_t>());
+                                                             fne.as<unsigned char>(), endbits.as<uint32_t>(),
+                                                             cnt.as<int>() + 2);
         SMAX_CUDA(cudaGetLastError());
         thrust::counting_iterator<int> it(0);
         empty_rows.alloc(sizeof(int) * n);
@@ -242,10 +266,11 @@ void CrsStreamPlan::build(const int *d_row_ptr, int64_t n, int64_t nnz_, int vby
         DevBuf tmp(tb);
         SMAX_CUDA(cub::DeviceSelect::Flagged(tmp.p, tb, it, fe.as<unsigned char>(), empty_rows.as<int>(),
                                              cnt.as<int>(), (int)n, st));
-        int h = 0;
-        SMAX_CUDA(cudaMemcpyAsync(&h, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        int h[3] = {0, 0, 0};
+        SMAX_CUDA(cudaMemcpyAsync(h, cnt.p, sizeof(h), cudaMemcpyDeviceToHost, st));
         SMAX_CUDA(cudaStreamSynchronize(st));
-        n_empty = h;
+        n_empty = h[0];
+        short_rows = h[2] == 0;
         n_nonempty = n - n_empty;
         if (n_empty > 0) {
             row_list.alloc(sizeof(int) * (n_nonempty > 0 ? n_nonempty : 1));
@@ -273,13 +298,20 @@ void crs_spmv_stream(const CrsStreamPlan &p, const int *col, const VT *val, cons
     const int *rl = p.row_list.p ? p.row_list.as<int>() : nullptr;
     if (p.n_tasks > 0) {
         unsigned grid = ceil_div_u(p.n_tasks, kWarpsPerCta);
-        crs_stream_kernel<VT><<<grid, kWarpsPerCta * 32, 0, st>>>(
-            col, val, p.endbits.as<uint32_t>(), p.task_rank.as<int>(), rl, p.n_tasks, (int)p.n_nonempty, x, y,
-            p.carry_val.as<VT>(), p.carry_rank.as<int>());
-        SMAX_CUDA(cudaGetLastError());
-        crs_stream_fixup<VT><<<ceil_div_u(p.n_tasks, 256), 256, 0, st>>>(p.carry_val.as<VT>(),
-                                                                         p.carry_rank.as<int>(), rl, p.n_tasks, y);
-        SMAX_CUDA(cudaGetLastError());
+        auto launch = [&](auto kern) {
+            kern<<<grid, kWarpsPerCta * 32, 0, st>>>(col, val, p.endbits.as<uint32_t>(), p.task_rank.as<int>(), rl,
+                                                     p.row_ptr, p.n_tasks, (int)p.n_nonempty, x, y,
+                                                     p.carry_val.as<VT>(), p.carry_rank.as<int>());
+            SMAX_CUDA(cudaGetLastError());
+        };
+        if (p.short_rows) {
+            launch(crs_stream_kernel<VT, true>);  // no carries: one launch
+        } else {
+            launch(crs_stream_kernel<VT, false>);
+            crs_stream_fixup<VT><<<ceil_div_u(p.n_tasks, 256), 256, 0, st>>>(
+                p.carry_val.as<VT>(), p.carry_rank.as<int>(), rl, p.n_tasks, y);
+            SMAX_CUDA(cudaGetLastError());
+        }
     }
     if (p.n_empty > 0) {
         zero_rows<VT><<<ceil_div_u(p.n_empty, 256), 256, 0, st>>>(p.empty_rows.as<int>(), p.n_empty, y);
