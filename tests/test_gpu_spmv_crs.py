@@ -35,6 +35,20 @@ def test_random_vs_oracle(vt, case, variant):
     assert normwise(y, y64) <= tol(vt)
 
 
+@pytest.mark.parametrize("vt", [np.float64, np.float32])
+@pytest.mark.parametrize("longest", [32, 33])
+def test_stream_short_row_bound(vt, longest):
+    """Rows of at most 32 entries run the one-launch mode (each slice sums the
+    head of its first row); one row of 33 switches to slice carries."""
+    rp, col, val = rand_crs(50000, 32, seed=41, vt=vt, empty_frac=0.1, long_rows=(longest,) * 3)
+    assert np.diff(rp).max() == longest
+    x = np.random.default_rng(42).uniform(-1, 1, len(rp) - 1).astype(vt)
+    y = gpu_spmv(rp, col, val, x, variant=1)
+    assert normwise(y, O.spmv_crs(rp, col, val, x)) <= tol(vt)
+    y64 = O.spmv_crs(rp, col, val.astype(np.float64), x.astype(np.float64))
+    assert normwise(y, y64) <= tol(vt)
+
+
 @pytest.mark.parametrize("variant", [1, 2])
 def test_all_rows_empty(variant):
     n = 1000
