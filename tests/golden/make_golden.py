@@ -158,7 +158,8 @@ def solver_apps_fixture() -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--ref-root", default=os.environ.get("SMAX_REF_ROOT", "/root/reference"),
+                    help="the reference checkout (default: $SMAX_REF_ROOT, else /root/reference)")
     a = ap.parse_args()
     tdir = os.path.join(a.ref_root, "examples", "tests")
     data = {}

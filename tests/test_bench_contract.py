@@ -41,3 +41,19 @@ def test_reference_arm_other_ranks_print_nothing():
              {"RANK": "1", "LOCAL_RANK": "1", "WORLD_SIZE": "2"})
     assert r.returncode == 0, r.stderr[-2000:]
     assert not [l for l in r.stdout.splitlines() if l.startswith("{")]
+
+
+def test_reference_arm_does_not_load_the_product_library():
+    """The reference arm times the reference's own CPU kernel: the process must
+    never map libsmax_b200.so (the generators it imports are plain numpy)."""
+    code = ("import runpy, sys\n"
+            "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0']\n"
+            "try:\n"
+            "    runpy.run_path('bench.py', run_name='__main__')\n"
+            "except SystemExit as e:\n"
+            "    assert not e.code, e.code\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print('MAPPED' if 'libsmax_b200.so' in maps else 'CLEAN')\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=REPO, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip().splitlines()[-1] == "CLEAN"
