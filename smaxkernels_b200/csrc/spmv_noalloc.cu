@@ -113,8 +113,11 @@ __global__ void na_prepare(const int *__restrict__ row_ptr, const int *__restric
     int nonempty = 0;
     if (r < n) {
         const int a = row_ptr[r], b = row_ptr[r + 1];
-        if (b < a) report(s.status, SMAX_ERR_BAD_ARG, r);
-        if (b > a && b <= nnz) {
+        // any bound outside [0, nnz] or a decreasing pair is an error; the
+        // row-end bit is set only for 0 <= a < b <= nnz, so a malformed
+        // row_ptr never writes outside the bit mask
+        if (b < a || a < 0 || (int64_t)b > nnz) report(s.status, SMAX_ERR_BAD_ARG, r);
+        if (a >= 0 && b > a && (int64_t)b <= nnz) {
             nonempty = 1;
             atomicOr(s.endbits + ((b - 1) >> 5), 1u << ((b - 1) & 31));
         } else if (b == a) {
