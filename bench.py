@@ -214,7 +214,7 @@ def config_dict(nnz, vbytes, world):
 # The other workloads of the hot path (--workload NAME, or "all"): one JSON
 # line per case, same keys as the headline line.  Single GPU.
 # ---------------------------------------------------------------------------
-EXTRA_WORKLOADS = ("spmv_laplace64", "scs_spmv", "bcrs_spmv", "spmm", "spgemm", "sptrsv", "sptrsv_batch",
+EXTRA_WORKLOADS = ("gather_ceiling", "spmv_laplace64", "scs_spmv", "bcrs_spmv", "spmm", "spgemm", "sptrsv", "sptrsv_batch",
                    "sptrsv_refine", "adjoint", "solvers", "cusparse", "mtx", "colour")
 
 
@@ -326,6 +326,84 @@ class Bench:
 
 def _dt(vt):
     return "f64" if vt == np.float64 else "f32"
+
+
+def wl_gather_ceiling(b: Bench):
+    """The memory-traffic floor of the CRS SpMV on the lognormal 2^22 matrix
+    (smax_measure_gather): val/col streamed exactly as the warp-stream kernel
+    reads them and one x gather per entry, without row bookkeeping.  Lanes
+    [0, tma_lanes) gather through TMA tile::gather4, the rest through L2 loads;
+    the stream-only mode drops the gathers.  Every TMA configuration must give
+    per-warp sums bit-identical to the all-L2-load one (same products, same
+    order).  The CRS SpMV itself is timed on the same arrays for comparison."""
+    import ctypes
+    from smaxkernels_b200 import KernelType, _lib
+    from smaxkernels_b200 import matrices as M
+    from smaxkernels_b200.matrices import crs_bytes
+    torch = b.torch
+    dts = (np.float64, np.float32) if b.args.extra_dtype == "both" else \
+        ((np.float64,) if b.args.extra_dtype == "f64" else (np.float32,))
+    for vt in dts:
+        vb = np.dtype(vt).itemsize
+        rp, col, val = M.lognormal_random(1 << 22, seed=1, dtype=vt)
+        n, nnz = len(rp) - 1, len(col)
+        x = M.uniform_vector(n, 100, vt)
+        n_slices = (nnz + 511) // 512
+        colp = np.zeros(n_slices * 512, np.int32)
+        colp[:nnz] = col
+        valp = np.zeros(n_slices * 512, vt)
+        valp[:nnz] = val
+        cd, vd, xd = b.dev(colp), b.dev(valp), b.dev(x)
+        out = b.zeros(n_slices, vt)
+        err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        ft = 1 if vt == np.float64 else 0
+        P = ctypes.c_void_p
+
+        def probe(mode, lanes, depth):
+            rc = _lib.lib.smax_measure_gather(ft, mode, lanes, depth, n_slices, P(cd.data_ptr()), P(vd.data_ptr()),
+                                              P(xd.data_ptr()), n, P(out.data_ptr()), P(err.data_ptr()),
+                                              P(b.stream.cuda_stream))
+            if rc != 0:
+                raise RuntimeError(_lib.lib.smax_last_error().decode())
+
+        nbytes = crs_bytes(n, nnz, n, vb)
+        stream_bytes = (vb + 4) * n_slices * 512
+        results = {}
+        with b.clocks() as clk:
+            probe(0, 0, 2)
+            torch.cuda.synchronize()
+            ref_sums = out.clone()
+            t, _ = b.time(lambda: probe(1, 0, 2))
+            results["stream_only_d2"] = {"ms": round(t * 1e3, 5), "stream_gbs": round(stream_bytes / t / 1e9, 1)}
+            for depth in (1, 2, 4):
+                for lanes in (0, 8, 16, 24, 32):
+                    out.fill_(0)
+                    err.zero_()
+                    probe(0, lanes, depth)
+                    torch.cuda.synchronize()
+                    same = bool(torch.equal(out, ref_sums)) and int(err.item()) == 0
+                    t, _ = b.time(lambda: probe(0, lanes, depth))
+                    results[f"tma{lanes}_d{depth}"] = {"ms": round(t * 1e3, 5),
+                                                       "crs_equiv_gbs": round(nbytes / t / 1e9, 1),
+                                                       "bit_identical": same}
+            smax, k = b.kernel(KernelType.SPMV, vt)
+            yd = b.zeros(n, vt)
+            k.register_A(n, n, nnz, col, rp, val)
+            k.register_B(n, xd)
+            k.register_C(n, yd)
+            k.set_stream(b.stream.cuda_stream)
+            k.initialize()
+            t_spmv, reps = b.time(k.apply)
+            smax.close()
+        best = min((v["ms"] for kk, v in results.items() if kk.startswith("tma")))
+        b.emit(f"gather_ceiling_{_dt(vt)}_lognormal_4194304", "CRS SpMV traffic floor (ms per pass)", best, "ms",
+               best * 1e-3, reps, _dt(vt),
+               {"n_rows": n, "nnz": nnz, "n_slices": n_slices, "l2": "inputs larger than L2 (no flush)"},
+               clk.summary(), b.hbm(nbytes, best * 1e-3, "gather_probe_kernel"), None, launches=reps, higher=False,
+               probes=results, crs_spmv_ms=round(t_spmv * 1e3, 5),
+               crs_spmv_frac_of_floor=round(best / (t_spmv * 1e3), 4))
+        del cd, vd, xd, out
+        torch.cuda.empty_cache()
 
 
 def wl_spmv_laplace64(b: Bench):

@@ -467,6 +467,23 @@ smax_status smax_solver_solve(smax_solver s, const void *b, void *x, const smax_
 smax_status smax_solver_get_history(smax_solver s, double *out, int cap, int *count);
 smax_status smax_solver_destroy(smax_solver s);
 
+/* ------------------------------------------------------------ measurement */
+/* The memory-traffic floor of the warp-stream CRS SpMV on given arrays: the
+ * same 512-entry warp slices and 16-byte streaming loads of col and val, one
+ * x gather per entry, products summed per slice into out[] (no row
+ * bookkeeping).  No counterpart exists in the reference; the benchmark uses
+ * it to measure the gather ceiling the SpMV kernels are judged against.
+ *   mode 0: gathers -- lanes [0, tma_lanes) of every warp fetch x through TMA
+ *           tile::gather4 loads, the others through ordinary L2 loads;
+ *   mode 1: stream only (x is not read).
+ * depth (1, 2 or 4) chunks of 128 entries are kept in flight per warp.
+ * d_col/d_val: n_slices*512 entries (16-byte aligned, columns in
+ * [0, n_cols)); d_out: n_slices values; d_err: one int, set to 1 when a TMA
+ * wait gave up (never expected).  Asynchronous on `stream`. */
+smax_status smax_measure_gather(int float_type, int mode, int tma_lanes, int depth, uint64_t n_slices,
+                                const void *d_col, const void *d_val, const void *d_x, uint64_t n_cols, void *d_out,
+                                void *d_err, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

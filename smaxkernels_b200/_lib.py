@@ -72,6 +72,7 @@ SIGNATURES = {
     "smax_utils_convert_coo_to_crs": (I32, [I32, U64, U64, U64, P, P, P, PP, PP, PP]),
     "smax_free_host": (None, [P]),
     "smax_spmv_crs_noalloc": (I32, [I32, U64, U64, U64, P, P, P, P, P, P]),
+    "smax_measure_gather": (I32, [I32, I32, I32, I32, U64, P, P, P, U64, P, P, P]),
     "smax_solver_create": (I32, [PP, I32, I32, U64, U64, P, P, P]),
     "smax_solver_solve": (I32, [P, P, P, P, P, P]),
     "smax_solver_get_history": (I32, [P, P, I32, C.POINTER(I32)]),
