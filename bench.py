@@ -169,6 +169,42 @@ def cpu_reference_time(rp, col, val, x, max_s=20.0, reps=None, warm=1):
     return (time.perf_counter() - t0) / n, 1, "port", n
 
 
+def gather_floor_time(col, val, x_dev, n_cols, vt, stream, steps):
+    """Seconds per pass of smax_measure_gather (L2-load gathers, two chunks in
+    flight per warp) over this matrix's val/col, padded to 512-entry slices:
+    the floor of the CRS SpMV's access pattern on this GPU."""
+    import ctypes
+    import torch
+    from smaxkernels_b200 import _lib
+    nnz = len(col)
+    n_slices = (nnz + 511) // 512
+    cd = torch.zeros(n_slices * 512, dtype=torch.int32, device="cuda")
+    vd = torch.zeros(n_slices * 512, dtype=torch.float64 if vt == np.float64 else torch.float32, device="cuda")
+    cd[:nnz] = torch.from_numpy(col).cuda()
+    vd[:nnz] = torch.from_numpy(val).cuda()
+    out = torch.empty(n_slices, dtype=vd.dtype, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    P = ctypes.c_void_p
+
+    def probe():
+        rc = _lib.lib.smax_measure_gather(1 if vt == np.float64 else 0, 0, 0, 2, n_slices, P(cd.data_ptr()),
+                                          P(vd.data_ptr()), P(x_dev.data_ptr()), n_cols, P(out.data_ptr()),
+                                          P(err.data_ptr()), P(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(_lib.lib.smax_last_error().decode())
+
+    for _ in range(3):
+        probe()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        probe()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) * 1e-3 / steps
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -1168,6 +1204,8 @@ def main():
                     help="e2e: row blocks of the host-pointer SpMV pipeline (default: the library's)")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-gather-floor", action="store_true",
+                    help="skip the gather-floor measurement beside the headline kernel")
     ap.add_argument("--rows", type=int, default=N_ROWS, help="rows per rank (default 2^22)")
     ap.add_argument("--variant", type=int, default=0, help="CRS kernel: 0 auto, 1 warp-stream, 2 row-tile")
     ap.add_argument("--workload", default="crs_spmv", choices=("crs_spmv", "all") + EXTRA_WORKLOADS,
@@ -1278,6 +1316,8 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
         t_kernel = ev0.elapsed_time(ev1) * 1e-3 / args.steps
+        t_floor = None if args.no_gather_floor else gather_floor_time(col, val, x_glob, n_cols, vt, stream,
+                                                                      args.steps)
 
         # ---- end to end through the C ABI: pinned host x and y ----------------
         ke = None
@@ -1352,6 +1392,10 @@ def main():
             "value": round(bytes_rank * world / t_e2e / 1e9, 3), "unit": UNIT,
             "h2d_bytes_per_step": int(n_cols * vbytes), "d2h_bytes_per_step": int(N_ROWS * vbytes),
             "ms_per_step": round(t_e2e * 1e3, 4)},
+        "gather_floor": None if t_floor is None else {
+            "ms": round(t_floor * 1e3, 5), "frac_of_floor": round(t_floor / t_kernel, 4),
+            "what": "smax_measure_gather on this rank's matrix: the same val/col stream and one x gather per "
+                    "entry through L2 loads, no row bookkeeping (the request-rate floor of this access pattern)"},
         "gpu_launches": args.steps * (1 if args.variant == 2 else 2),  # SpMV kernel (+ carry fix-up) per step
         "clocks": clocks,
     }
