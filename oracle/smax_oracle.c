@@ -364,26 +364,150 @@ void orc_spgemm_fill_cols(int64_t a_n_rows, const I *a_col, const I *a_row_ptr,
 /* src/utils/convert_formats.hpp:27-30,57-78: n_chunks = ceil(n/C),
  * n_rows_padded = n_chunks*C, chunk length = longest row of the chunk after
  * the sigma-window sort.  Returns the permutation perm[old] = new (:81-86),
- * chunk_lengths and chunk_ptr; *n_elements = chunk_ptr[n_chunks]. */
+ * chunk_lengths and chunk_ptr; *n_elements = chunk_ptr[n_chunks].
+ *
+ * The window sort (:46-55) is std::sort over (index, count) pairs with the
+ * comparator a.count > b.count.  That sort is not stable: rows of equal
+ * length end up in whatever order the library's algorithm leaves them.  The
+ * reference is built with GCC 13.3, whose libstdc++ std::sort is the
+ * published introsort restated below (and in the GPU conversion,
+ * smaxkernels_b200/csrc/scs_window_sort.cuh), so the permutation is
+ * reproduced exactly:
+ *   sort(a, n):  if n > 0: introsort_loop(a, 0, n, 2*floor(log2 n));
+ *                          final_insertion_sort(a, 0, n)
+ *   introsort_loop(lo, hi, depth): while hi - lo > 16:
+ *       depth == 0 -> heapsort [lo, hi) (make_heap + sort_heap), return;
+ *       --depth; cut = partition around the median of a[lo+1], a[mid],
+ *       a[hi-1] moved to a[lo]; introsort_loop(cut, hi, depth); hi = cut
+ *   final_insertion_sort: insertion sort of the first 16, then unguarded
+ *       insertion of the rest (plain insertion sort when n <= 16). */
 typedef struct { int idx; int cnt; } orc_pair;
 
-static void orc_sort_window_desc(orc_pair *a, int64_t n) {
-    /* stable insertion sort, longer rows first, ties by ascending index */
-    for (int64_t i = 1; i < n; ++i) {
-        orc_pair v = a[i];
-        int64_t k = i - 1;
-        while (k >= 0 && a[k].cnt < v.cnt) {
-            a[k + 1] = a[k];
-            --k;
-        }
-        a[k + 1] = v;
+/* the reference's comparator: longer rows first */
+static int orc_before(orc_pair x, orc_pair y) { return x.cnt > y.cnt; }
+
+static void orc_swap(orc_pair *a, int64_t i, int64_t j) {
+    orc_pair t = a[i];
+    a[i] = a[j];
+    a[j] = t;
+}
+
+static void orc_median_to_first(orc_pair *a, int64_t r, int64_t x, int64_t y, int64_t z) {
+    if (orc_before(a[x], a[y])) {
+        if (orc_before(a[y], a[z])) orc_swap(a, r, y);
+        else if (orc_before(a[x], a[z])) orc_swap(a, r, z);
+        else orc_swap(a, r, x);
+    } else if (orc_before(a[x], a[z])) {
+        orc_swap(a, r, x);
+    } else if (orc_before(a[y], a[z])) {
+        orc_swap(a, r, z);
+    } else {
+        orc_swap(a, r, y);
     }
 }
 
-static int orc_cmp_pair(const void *pa, const void *pb) {
-    const orc_pair *a = (const orc_pair *)pa, *b = (const orc_pair *)pb;
-    if (a->cnt != b->cnt) return a->cnt > b->cnt ? -1 : 1;
-    return a->idx < b->idx ? -1 : (a->idx > b->idx);
+/* Hoare partition of [lo, hi) around a[pivot]; no bounds checks needed
+ * because the median-of-three leaves sentinels on both sides */
+static int64_t orc_partition(orc_pair *a, int64_t lo, int64_t hi, int64_t pivot) {
+    for (;;) {
+        while (orc_before(a[lo], a[pivot])) ++lo;
+        --hi;
+        while (orc_before(a[pivot], a[hi])) --hi;
+        if (!(lo < hi)) return lo;
+        orc_swap(a, lo, hi);
+        ++lo;
+    }
+}
+
+/* sift `v` down from `hole` in the heap a[base .. base+len), then up to `top` */
+static void orc_adjust_heap(orc_pair *a, int64_t base, int64_t hole, int64_t len, orc_pair v) {
+    const int64_t top = hole;
+    int64_t child = hole;
+    while (child < (len - 1) / 2) {
+        child = 2 * (child + 1);
+        if (orc_before(a[base + child], a[base + child - 1])) --child;
+        a[base + hole] = a[base + child];
+        hole = child;
+    }
+    if ((len & 1) == 0 && child == (len - 2) / 2) {
+        child = 2 * (child + 1);
+        a[base + hole] = a[base + child - 1];
+        hole = child - 1;
+    }
+    int64_t parent = (hole - 1) / 2;
+    while (hole > top && orc_before(a[base + parent], v)) {
+        a[base + hole] = a[base + parent];
+        hole = parent;
+        parent = (hole - 1) / 2;
+    }
+    a[base + hole] = v;
+}
+
+static void orc_heapsort(orc_pair *a, int64_t lo, int64_t hi) {
+    const int64_t len = hi - lo;
+    if (len >= 2)
+        for (int64_t parent = (len - 2) / 2;; --parent) {
+            orc_adjust_heap(a, lo, parent, len, a[lo + parent]);
+            if (parent == 0) break;
+        }
+    for (int64_t last = hi; last - lo > 1;) {
+        --last;
+        orc_pair v = a[last];
+        a[last] = a[lo];
+        orc_adjust_heap(a, lo, 0, last - lo, v);
+    }
+}
+
+static void orc_linear_insert(orc_pair *a, int64_t i) {
+    orc_pair v = a[i];
+    int64_t j = i - 1;
+    while (orc_before(v, a[j])) {
+        a[i] = a[j];
+        i = j;
+        --j;
+    }
+    a[i] = v;
+}
+
+static void orc_insertion_sort(orc_pair *a, int64_t lo, int64_t hi) {
+    if (lo == hi) return;
+    for (int64_t i = lo + 1; i < hi; ++i) {
+        if (orc_before(a[i], a[lo])) {
+            orc_pair v = a[i];
+            for (int64_t j = i; j > lo; --j) a[j] = a[j - 1];
+            a[lo] = v;
+        } else {
+            orc_linear_insert(a, i);
+        }
+    }
+}
+
+static void orc_introsort_loop(orc_pair *a, int64_t lo, int64_t hi, int depth) {
+    while (hi - lo > 16) {
+        if (depth == 0) {
+            orc_heapsort(a, lo, hi);
+            return;
+        }
+        --depth;
+        const int64_t mid = lo + (hi - lo) / 2;
+        orc_median_to_first(a, lo, lo + 1, mid, hi - 1);
+        const int64_t cut = orc_partition(a, lo + 1, hi, lo);
+        orc_introsort_loop(a, cut, hi, depth);
+        hi = cut;
+    }
+}
+
+static void orc_std_sort_window(orc_pair *a, int64_t n) {
+    if (n <= 0) return;
+    int lg = 0;
+    while (((int64_t)1 << (lg + 1)) <= n) ++lg;
+    orc_introsort_loop(a, 0, n, 2 * lg);
+    if (n > 16) {
+        orc_insertion_sort(a, 0, 16);
+        for (int64_t i = 16; i < n; ++i) orc_linear_insert(a, i);
+    } else {
+        orc_insertion_sort(a, 0, n);
+    }
 }
 
 int orc_scs_layout(int64_t n_rows, const I *row_ptr, int64_t C, int64_t sigma,
@@ -399,10 +523,7 @@ int orc_scs_layout(int64_t n_rows, const I *row_ptr, int64_t C, int64_t sigma,
     }
     for (int64_t w = 0; w < npad; w += sigma) {
         int64_t len = (w + sigma < npad) ? sigma : npad - w;
-        if (len <= 64)
-            orc_sort_window_desc(e + w, len);
-        else
-            qsort(e + w, (size_t)len, sizeof(orc_pair), orc_cmp_pair);
+        orc_std_sort_window(e + w, len);
     }
     I cur = 0;
     for (int64_t c = 0; c < n_chunks; ++c) {

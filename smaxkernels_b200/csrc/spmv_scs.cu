@@ -18,16 +18,18 @@
 //   * any other C: one thread per row, consecutive threads on consecutive rows.
 //
 // Conversion (Utils::convert_crs_to_scs): row lengths, a per-sigma-window sort
-// by descending length with ties broken by ascending row (a segmented radix
-// sort of (length, row) keys), chunk lengths as the chunk's maximum, chunk_ptr
-// by scan, perm[old] = new, and a scatter of col/val into the zero-filled
-// chunk-column-major arrays -- all on the GPU.
+// by descending length that leaves rows of equal length in exactly the order
+// the reference's std::sort leaves them (scs_window_sort.cuh), chunk lengths
+// as the chunk's maximum, chunk_ptr by scan, perm[old] = new, and a scatter
+// of col/val into the zero-filled chunk-column-major arrays -- all on the GPU.
+// perm, col and val are therefore bit-exact with the reference's for every
+// sigma, not only where ties cannot occur.
 #include "spmv_formats.cuh"
+#include "scs_window_sort.cuh"
 
 #include <vector>
 
 #include <cub/device/device_scan.cuh>
-#include <cub/device/device_segmented_radix_sort.cuh>
 
 namespace smax {
 
@@ -216,15 +218,30 @@ __global__ void scs_keys_kernel(const int *__restrict__ row_ptr, int64_t n, int6
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npad) return;
     const unsigned cnt = i < n ? (unsigned)(row_ptr[i + 1] - row_ptr[i]) : 0u;
-    // ascending key order == longer rows first, then lower original row
+    // high half orders longer rows first (the reference compares counts only);
+    // the low half carries the row through the sort
     keys[i] = ((unsigned long long)(0x7fffffffu - cnt) << 32) | (unsigned long long)i;
 }
 
-__global__ void scs_window_offsets(int64_t npad, int64_t sigma, int64_t n_windows, int *__restrict__ off) {
-    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (w > n_windows) return;
-    const int64_t o = w * sigma;
-    off[w] = (int)(o < npad ? o : npad);
+// One sigma window per single-thread block, ordered exactly as the
+// reference's std::sort orders it (scs_window_sort.cuh).  A single thread per
+// block keeps the data-dependent loops free of warp divergence; up to 32
+// windows share an SM.  SMEM: the window is staged in shared memory (windows
+// of up to kScsSortSmemKeys keys), else it is sorted in place in `out`.
+constexpr int64_t kScsSortSmemKeys = 4096;  // 32 KB of keys per block
+
+template <bool SMEM>
+__global__ void __launch_bounds__(1) scs_window_sort_kernel(const unsigned long long *__restrict__ keys,
+                                                            unsigned long long *__restrict__ out, int64_t npad,
+                                                            int64_t sigma, int *__restrict__ err) {
+    extern __shared__ unsigned long long win[];
+    const int64_t lo = (int64_t)blockIdx.x * sigma;
+    const int64_t len = (lo + sigma < npad ? lo + sigma : npad) - lo;
+    unsigned long long *a = SMEM ? win : out + lo;
+    for (int64_t i = 0; i < len; ++i) a[i] = keys[lo + i];
+    if (!scs_sort::std_sort_order(a, len)) atomicExch(err, 1);
+    if (SMEM)
+        for (int64_t i = 0; i < len; ++i) out[lo + i] = a[i];
 }
 
 // chunk lengths (max row length in the chunk) and perm[old] = new
@@ -410,17 +427,21 @@ void crs_to_scs(const DevCRS &a, int vbytes, int64_t C, int64_t sigma, DevSCS &o
     scs_keys_kernel<<<ceil_div_u(npad, 256), 256, 0, st>>>(a.rp(), n, npad, keys.as<unsigned long long>());
     SMAX_CUDA(cudaGetLastError());
     const int64_t n_windows = (npad + sigma - 1) / sigma;
-    DevBuf woff(sizeof(int) * (n_windows + 1));
-    scs_window_offsets<<<ceil_div_u(n_windows + 1, 256), 256, 0, st>>>(npad, sigma, n_windows, woff.as<int>());
+    if (n_windows > 0x7fffffffll) fail(SMAX_ERR_UNSUPPORTED, "too many sigma windows");
+    DevBuf sort_err(sizeof(int));
+    SMAX_CUDA(cudaMemsetAsync(sort_err.p, 0, sizeof(int), st));
+    const int64_t win_keys = sigma < npad ? sigma : npad;
+    if (win_keys <= kScsSortSmemKeys) {
+        const size_t smem = sizeof(unsigned long long) * (size_t)win_keys;
+        SMAX_CUDA(cudaFuncSetAttribute(scs_window_sort_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+        scs_window_sort_kernel<true><<<(unsigned)n_windows, 1, smem, st>>>(
+            keys.as<unsigned long long>(), sorted.as<unsigned long long>(), npad, sigma, sort_err.as<int>());
+    } else {
+        scs_window_sort_kernel<false><<<(unsigned)n_windows, 1, 0, st>>>(
+            keys.as<unsigned long long>(), sorted.as<unsigned long long>(), npad, sigma, sort_err.as<int>());
+    }
     SMAX_CUDA(cudaGetLastError());
-    size_t tb = 0;
-    SMAX_CUDA(cub::DeviceSegmentedRadixSort::SortKeys(nullptr, tb, keys.as<unsigned long long>(),
-                                                      sorted.as<unsigned long long>(), (int)npad, (int)n_windows,
-                                                      woff.as<int>(), woff.as<int>() + 1, 0, 64, st));
-    DevBuf tmp(tb);
-    SMAX_CUDA(cub::DeviceSegmentedRadixSort::SortKeys(tmp.p, tb, keys.as<unsigned long long>(),
-                                                      sorted.as<unsigned long long>(), (int)npad, (int)n_windows,
-                                                      woff.as<int>(), woff.as<int>() + 1, 0, 64, st));
     scs_chunks_kernel<<<ceil_div_u(n_chunks, 256), 256, 0, st>>>(sorted.as<unsigned long long>(), n, C, n_chunks,
                                                                  out.chunk_len.as<int>(), perm.as<int>());
     SMAX_CUDA(cudaGetLastError());
@@ -435,9 +456,12 @@ void crs_to_scs(const DevCRS &a, int vbytes, int64_t C, int64_t sigma, DevSCS &o
     SMAX_CUDA(cub::DeviceScan::InclusiveSum(tmp2.p, tb2, sizes.as<long long>(), incl.as<long long>(),
                                             (int)n_chunks, st));
     long long ne = 0;
+    int h_sort_err = 0;
     SMAX_CUDA(cudaMemcpyAsync(&ne, incl.as<long long>() + n_chunks - 1, sizeof(long long), cudaMemcpyDeviceToHost,
                               st));
+    SMAX_CUDA(cudaMemcpyAsync(&h_sort_err, sort_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     SMAX_CUDA(cudaStreamSynchronize(st));
+    if (h_sort_err) fail(SMAX_ERR_UNSUPPORTED, "sigma-window sort exceeded its stack");
     if (ne >= (1ll << 31)) fail(SMAX_ERR_UNSUPPORTED, "SELL-C-sigma matrix exceeds int32 indexing");
     out.n_elements = ne;
     scs_ptr_kernel<<<ceil_div_u(n_chunks + 1, 256), 256, 0, st>>>(incl.as<long long>(), n_chunks,

@@ -124,6 +124,43 @@ def test_scs_random_vs_oracle(vt, C_, sigma):
     assert normwise(y[got["perm"]], y_ref) <= tol(vt)
 
 
+@pytest.mark.parametrize("C_,sigma", [(32, 1024), (32, 4096), (32, 8192), (8, 64), (4, 17), (2, 16), (1, 1),
+                                      (32, 1 << 20)])
+def test_scs_conversion_window_order_matches_oracle(C_, sigma):
+    """Every array bit-exact with the oracle, whose window order is the
+    reference's std::sort order (pinned in tests/test_scs_sort_order.py):
+    shared-memory windows (<= 4096 rows) and in-place global-memory windows."""
+    from smaxkernels_b200 import matrices as M
+    rp, col, val = M.lognormal_random(1 << 16, seed=11)
+    n = len(rp) - 1
+    smax = _iface()
+    got = smax.utils.convert_crs_to_scs(n, n, len(col), col, rp, val, C_, sigma)
+    smax.close()
+    ref = O.scs(rp, col, val, C_, sigma)
+    for kk in ("chunk_ptr", "chunk_lengths", "perm", "col", "val"):
+        np.testing.assert_array_equal(got[kk], ref[kk], err_msg=kk)
+
+
+@pytest.mark.parametrize("n", [256, 2048, 6000])
+def test_scs_conversion_heapsort_fallback_matches_oracle(n):
+    """Windows crafted to reach introsort's heapsort fallback, with equal
+    lengths (tests/sort_adversary.py); 6000 rows take the global-memory path."""
+    from sort_adversary import heap_row_lengths
+    lens = np.asarray(heap_row_lengths(n), np.int64)
+    rng = np.random.default_rng(12)
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum(lens)
+    col = np.concatenate([np.sort(rng.choice(n, int(l), replace=False)) for l in lens]).astype(np.int32)
+    val = rng.uniform(-1, 1, len(col))
+    for C_, sigma in ((1, n), (4, n)):
+        smax = _iface()
+        got = smax.utils.convert_crs_to_scs(n, n, len(col), col, rp, val, C_, sigma)
+        smax.close()
+        ref = O.scs(rp, col, val, C_, sigma)
+        for kk in ("chunk_ptr", "chunk_lengths", "perm", "col", "val"):
+            np.testing.assert_array_equal(got[kk], ref[kk], err_msg=f"{kk} C={C_} sigma={sigma}")
+
+
 @pytest.mark.slow
 @pytest.mark.parametrize("vt", [np.float64, np.float32])
 def test_scs_config1_full_size(vt):
@@ -134,7 +171,7 @@ def test_scs_config1_full_size(vt):
     got = smax.utils.convert_crs_to_scs(n, n, len(col), col, rp, val, 32, 1024)
     smax.close()
     ref = O.scs(rp, col, val, 32, 1024)
-    for kk in ("chunk_ptr", "chunk_lengths", "perm"):
+    for kk in ("chunk_ptr", "chunk_lengths", "perm", "col", "val"):
         np.testing.assert_array_equal(got[kk], ref[kk], err_msg=kk)
     assert got["n_elements"] == ref["n_elements"]
     x = M.uniform_vector(n, 1, dtype=vt)
