@@ -120,6 +120,17 @@ typedef struct smax_kernel_s *smax_kernel;
 int smax_abi_version(void);
 const char *smax_last_error(void);
 
+/* Allocation-failure injection for tests (no counterpart in the reference,
+ * whose CUDA path only prints a failed allocation, src/platforms/cuda/
+ * cuda.cuh:23-44).  Every device allocation of this library is counted; with
+ * n >= 1 the n-th allocation from this call on fails as an out-of-memory
+ * cudaMalloc would (the call in progress returns SMAX_ERR_OOM, cudaMalloc is
+ * not called) and the injection disarms itself; n = 0 disarms.  Process-wide,
+ * host-side only: no GPU is faulted. */
+smax_status smax_test_fail_device_alloc(int64_t n);
+/* Device allocations attempted since the library was loaded. */
+uint64_t smax_test_device_alloc_count(void);
+
 /* ---------------------------------------------------------------- context */
 /* Interface-level state; kernels created from one context share its level
  * sets (src/interface.hpp:23-26, src/interface.cpp:53-57). */

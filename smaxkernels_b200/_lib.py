@@ -27,6 +27,8 @@ PU64 = C.POINTER(C.c_uint64)
 SIGNATURES = {
     "smax_abi_version": (I32, []),
     "smax_last_error": (C.c_char_p, []),
+    "smax_test_fail_device_alloc": (I32, [C.c_int64]),
+    "smax_test_device_alloc_count": (U64, []),
     "smax_ctx_create": (I32, [PP]),
     "smax_ctx_destroy": (I32, [P]),
     "smax_ctx_get_n_levels": (I32, [P]),

@@ -460,11 +460,10 @@ void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
     if (k->ktype == SMAX_KERNEL_SPGEMM) {
         // offsets are ignored, as in the reference (src/kernels/spgemm.hpp:108-130)
         k->timers["apply"] += k->apply_events.trim(512);
-        auto ev = k->apply_events.acquire();
-        SMAX_CUDA(cudaEventRecord(ev.first, k->stream));
+        EventInterval iv(k->apply_events, k->stream);
         if (k->vbytes == 8) spgemm<double>(k->dA, k->dBm, k->dCm, k->spgemm_work, &k->spgemm_times, k->stream);
         else spgemm<float>(k->dA, k->dBm, k->dCm, k->spgemm_work, &k->spgemm_times, k->stream);
-        SMAX_CUDA(cudaEventRecord(ev.second, k->stream));
+        iv.close();
         const SpgemmTimes &t = k->spgemm_times;
         k->timers["Symbolic_Setup"] += t.setup;
         k->timers["Fused_Gustavson"] += t.fused;
@@ -477,15 +476,14 @@ void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
     }
     check_extents(k, b_off, c_off);
     k->timers["apply"] += k->apply_events.trim(512);
-    auto ev = k->apply_events.acquire();
-    SMAX_CUDA(cudaEventRecord(ev.first, k->stream));
+    EventInterval iv(k->apply_events, k->stream);
     if (!k->f_device && pipe_ready(k)) {
         apply_pipelined(k, b_off, c_off);  // records one output range per row block
     } else {
         apply_core(k, b_off, c_off);
         if (!k->f_device) record_out(k, out_offset(k, b_off, c_off), out_count(k));
     }
-    SMAX_CUDA(cudaEventRecord(ev.second, k->stream));
+    iv.close();
 }
 
 }  // namespace
@@ -566,6 +564,17 @@ extern "C" {
 int smax_abi_version(void) { return SMAX_B200_ABI_VERSION; }
 
 const char *smax_last_error(void) { return smax::last_error(); }
+
+smax_status smax_test_fail_device_alloc(int64_t n) {
+    if (n < 0) {
+        smax::set_last_error("smax_test_fail_device_alloc: n must be >= 0");
+        return SMAX_ERR_BAD_ARG;
+    }
+    smax::arm_device_alloc_failure(n);
+    return SMAX_OK;
+}
+
+uint64_t smax_test_device_alloc_count(void) { return (uint64_t)smax::device_alloc_count(); }
 
 smax_status smax_ctx_create(smax_ctx *out) {
     return guarded([&] {

@@ -57,6 +57,16 @@ template <typename F> int guarded(F &&f) {
     }
 }
 
+// ------------------------------------------------- allocation accounting --
+// Every device allocation of the platform goes through DevBuf::alloc, which
+// counts it and asks this hook first.  When a test has armed it
+// (smax_test_fail_device_alloc(n)), the n-th allocation from then on fails
+// exactly as an out-of-memory cudaMalloc would (SMAX_ERR_OOM), without
+// calling cudaMalloc, and the hook disarms itself.
+bool device_alloc_should_fail();
+void arm_device_alloc_failure(long long n);  // n >= 1: fail the n-th allocation from now; 0: off
+long long device_alloc_count();
+
 // --------------------------------------------------------- device buffers --
 // Owning, move-only device allocation.  Size 0 allocates nothing.
 struct DevBuf {
@@ -79,6 +89,8 @@ struct DevBuf {
     void alloc(size_t b) {
         release();
         if (b) {
+            if (device_alloc_should_fail())
+                fail(SMAX_ERR_OOM, "cudaMalloc of " + std::to_string(b) + " bytes failed (injected by the test hook)");
             cudaError_t e = cudaMalloc(&p, b);
             if (e != cudaSuccess) {
                 p = nullptr;

@@ -76,7 +76,37 @@ struct PendingEvents {
     // sums and recycles all but the newest `keep` intervals once more than
     // 2*keep are live (bounds the event count of long apply() loops)
     double trim(size_t keep);
+    // returns an acquired interval to the spare list unsummed (its end event
+    // was never recorded: the timed work threw)
+    void drop(std::pair<cudaEvent_t, cudaEvent_t> p);
     ~PendingEvents();
+};
+
+// One stopwatch interval around a block of launches on `s`: the start event
+// is recorded on construction, the end event by close().  If the block
+// throws before close(), the interval is dropped, so a later drain() never
+// reads an event that was not recorded.
+struct EventInterval {
+    PendingEvents &pe;
+    cudaStream_t s;
+    std::pair<cudaEvent_t, cudaEvent_t> ev;
+    bool closed = false;
+    EventInterval(PendingEvents &p, cudaStream_t st) : pe(p), s(st), ev(p.acquire()) {
+        const cudaError_t e = cudaEventRecord(ev.first, s);
+        if (e != cudaSuccess) {
+            pe.drop(ev);
+            cuda_check(e, "cudaEventRecord(interval start)");
+        }
+    }
+    void close() {
+        SMAX_CUDA(cudaEventRecord(ev.second, s));
+        closed = true;
+    }
+    ~EventInterval() {
+        if (!closed) pe.drop(ev);
+    }
+    EventInterval(const EventInterval &) = delete;
+    EventInterval &operator=(const EventInterval &) = delete;
 };
 
 double wall_s();

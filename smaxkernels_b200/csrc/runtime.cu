@@ -1,6 +1,7 @@
 // runtime.cu -- shared host-side runtime of the platform: error capture, device
 // queries, CUDA-event stopwatches, uploads and the validation passes that run
 // once per registered matrix before any kernel trusts it.
+#include <atomic>
 #include <chrono>
 
 #include "kernel_obj.cuh"
@@ -13,6 +14,20 @@ thread_local std::string g_last_error;
 
 void set_last_error(const std::string &m) { g_last_error = m; }
 const char *last_error() { return g_last_error.c_str(); }
+
+namespace {
+std::atomic<long long> g_alloc_count{0};    // device allocations attempted since load
+std::atomic<long long> g_alloc_fail_at{0};  // armed: g_alloc_count value that fails; 0 = off
+}  // namespace
+
+bool device_alloc_should_fail() {
+    const long long k = ++g_alloc_count;
+    long long at = g_alloc_fail_at.load();
+    return at != 0 && k == at && g_alloc_fail_at.compare_exchange_strong(at, 0);
+}
+
+void arm_device_alloc_failure(long long n) { g_alloc_fail_at = n > 0 ? g_alloc_count.load() + n : 0; }
+long long device_alloc_count() { return g_alloc_count.load(); }
 
 double wall_s() {
     using clk = std::chrono::steady_clock;
@@ -123,6 +138,15 @@ double PendingEvents::drain() {
     }
     live.clear();
     return s;
+}
+
+void PendingEvents::drop(std::pair<cudaEvent_t, cudaEvent_t> p) {
+    for (size_t i = live.size(); i-- > 0;)
+        if (live[i] == p) {
+            live.erase(live.begin() + (ptrdiff_t)i);
+            spare.push_back(p);
+            return;
+        }
 }
 
 PendingEvents::~PendingEvents() {
