@@ -167,6 +167,7 @@ void spmm_upload(smax_kernel_s *k) {
     validate_crs(k->dA, dstatus(k), k->stream);
     read_status(k);
     k->crs_stream = CrsStreamPlan();
+    k->spmm_plan = SpmmPlan();  // its row ranges and staged tiles describe the previous matrix
     if (!k->f_row_major) k->crs_stream.build(k->dA.rp(), k->dA.n_rows, k->dA.nnz, k->vbytes, k->stream);
 }
 
