@@ -267,6 +267,7 @@ class Bench:
         self.gpu = gpu_id_for_nvsmi(0)
         self._flush_buf = None
         self._flip = 0
+        self.collect = None
         self.ref = None
         if not args.no_cpu_baseline:
             from oracle.oracle import Reference, reference_available
@@ -338,7 +339,10 @@ class Bench:
              "config": dict({"workload": workload}, **config), "roofline": roofline, "cpu_baseline": cpu,
              "e2e": None, "gpu_launches": launches, "clocks": clocks}
         d.update(extra)
-        print(json.dumps(d), flush=True)
+        if self.collect is not None:  # gathered into the headline line instead of printed
+            self.collect.append(d)
+        else:
+            print(json.dumps(d), flush=True)
         return d
 
     # -- kernels with device operands ---------------------------------------
@@ -776,41 +780,93 @@ def wl_sptrsv_batch(b: Bench):
                b.hbm(nbytes, t, "batch_sptrsv_kernel"), cpu,
                launches=total_levels * reps if mode == 1 else reps,
                speedup_vs_per_level=(round(times[1] / t, 3) if 1 in times else None))
+    # the honest "why batch": the same 64 solves back to back, each a single
+    # SpTRSV kernel with the platform's default (best) scheme for its matrix
+    from smaxkernels_b200 import Interface, KernelType
+    smax = Interface()
+    ks = []
+    for m, (rp, c, v) in enumerate(mats):
+        nm = len(rp) - 1
+        o = tb.row_offset(m)
+        smax.register_kernel(f"t{m}", KernelType.SPTRSV)
+        k = smax.kernel(f"t{m}")
+        k.register_A(nm, nm, len(c), c.copy(), rp, v.copy())
+        k.register_B(nm, xd[o:o + nm])
+        k.register_C(nm, bd[o:o + nm])
+        k.set_stream(b.stream.cuda_stream)
+        k.initialize()
+        ks.append(k)
+
+    def singles():
+        for k in ks:
+            k.apply()
+    with b.clocks() as clk:
+        t1, reps = b.time(singles, budget_s=3.0, max_reps=50)
+    b.emit("sptrsv_64_single_solves_f64_laplace2d", "64 single SpTRSV solves back to back (ms)", t1 * 1e3, "ms", t1,
+           reps, "f64", {"matrices": 64, "n_rows": n, "nnz": nnz, "scheme": "one default SpTRSV kernel per matrix"},
+           clk.summary(), b.hbm(nbytes, t1, "per-matrix solve kernels"), None, launches=None, higher=False,
+           batch_speedup_over_singles=round(t1 / times[3], 3))
+    smax.close()
     tb.close()
 
 
 def wl_sptrsv_refine(b: Bench):
-    """FP32 solve + FP64-residual refinement vs the FP64 solve, to 1e-12,
-    natural and permuted 2048^2 triangles."""
-    from smaxkernels_b200 import KernelType
+    """FP32 solve + FP64-residual refinement vs the FP64 solve, to 1e-12, on
+    the 2048^2 lower triangle in natural order (4095 levels, latency-bound)
+    and after the seed-3 random symmetric permutation with RS levels (15
+    levels, bandwidth-side: where halving the value bytes could pay)."""
+    from smaxkernels_b200 import Interface, KernelType
     from smaxkernels_b200 import matrices as M
     A = M.laplace2d_5pt(2048)
-    rp, col, val = M.lower_triangle(*A)
-    n, nnz = len(rp) - 1, len(col)
+    n = len(A[0]) - 1
     rhs = M.uniform_vector(n, 3)
     bd = b.dev(rhs)
-    out = {}
-    for steps in (0, 2):
-        smax, k = b.kernel(KernelType.SPTRSV, np.float64, lambda k: k.set_refine(steps))
-        xd = b.zeros(n, np.float64)
-        k.register_A(n, n, nnz, col.copy(), rp, val.copy())
-        k.register_B(n, xd)
-        k.register_C(n, bd)
-        k.set_stream(b.stream.cuda_stream)
-        k.initialize()
-        with b.clocks() as clk:
-            t, reps = b.time(k.apply, budget_s=2.0, max_reps=100)
-        b.torch.cuda.synchronize()
-        out[steps] = (t, reps, xd.clone(), clk.summary())
-        smax.close()
-    t64, _, x64, _ = out[0]
-    t32, reps, x32, clk = out[2]
-    err = float(b.torch.linalg.norm(x32 - x64) / b.torch.linalg.norm(x64))
-    nbytes = _tri_bytes(n, nnz, 8)
-    b.emit("sptrsv_refine2_vs_f64_laplace2d_2048_natural", "refined FP32 SpTRSV speed-up over FP64",
-           t64 / t32, "x", t32, reps, "f32+f64", {"n_rows": n, "nnz": nnz, "corrections": 2}, clk,
-           b.hbm(nbytes, t32, "level kernels (FP32) + residual_kernel"), None,
-           fp64_ms=round(t64 * 1e3, 4), refined_ms=round(t32 * 1e3, 4), rel_diff_vs_fp64=err)
+    cases = {"natural": (M.lower_triangle(*A), None)}
+    Ar, Ac, Av, _ = M.random_symmetric_permutation(*A, seed=3)
+    smax0 = Interface()
+    perm = np.zeros(n, np.int32)
+    inv = np.zeros(n, np.int32)
+    smax0.utils.generate_perm(n, Ar, Ac, perm, inv, "RS")
+    lvl = np.array([smax0.get_level_ptr_at(i) for i in range(smax0.get_n_levels() + 1)], np.int32)
+    prp = np.zeros(n + 1, np.int32)
+    pcol = np.zeros(len(Ac), np.int32)
+    pval = np.zeros(len(Ac))
+    smax0.utils.apply_mat_perm(n, Ar, Ac, Av, prp, pcol, pval, perm, inv)
+    smax0.close()
+    cases["permuted"] = (M.lower_triangle(prp, pcol, pval), lvl)
+    for name, ((rp, col, val), levels) in cases.items():
+        nnz = len(col)
+        out = {}
+        for steps in (0, 1, 2):
+            def setup(k):
+                k.set_refine(steps)
+                if levels is not None:
+                    k.set_mat_perm(True)
+            smax, k = b.kernel(KernelType.SPTRSV, np.float64, setup)
+            if levels is not None:
+                smax.set_levels(levels)
+            xd = b.zeros(n, np.float64)
+            k.register_A(n, n, nnz, col.copy(), rp, val.copy())
+            k.register_B(n, xd)
+            k.register_C(n, bd)
+            k.set_stream(b.stream.cuda_stream)
+            k.initialize()
+            with b.clocks() as clk:
+                t, reps = b.time(k.apply, budget_s=2.0, max_reps=200)
+            b.torch.cuda.synchronize()
+            out[steps] = (t, reps, xd.clone(), clk.summary())
+            smax.close()
+        t64, _, x64, _ = out[0]
+        errs = {s: float(b.torch.linalg.norm(out[s][2] - x64) / b.torch.linalg.norm(x64)) for s in (1, 2)}
+        t32, reps, x32, clk = out[2]
+        nbytes = _tri_bytes(n, nnz, 8)
+        b.emit(f"sptrsv_refine2_vs_f64_laplace2d_2048_{name}", "refined FP32 SpTRSV speed-up over FP64",
+               t64 / t32, "x", t32, reps, "f32+f64",
+               {"n_rows": n, "nnz": nnz, "corrections": 2, "order": name,
+                "levels": int(len(levels) - 1) if levels is not None else 4095}, clk,
+               b.hbm(nbytes, t32, "solve kernels (FP32) + residual_kernel"), None,
+               fp64_ms=round(t64 * 1e3, 4), refined1_ms=round(out[1][0] * 1e3, 4),
+               refined2_ms=round(t32 * 1e3, 4), rel_diff_vs_fp64={"1": errs[1], "2": errs[2]})
 
 
 def wl_adjoint(b: Bench):
@@ -1180,6 +1236,41 @@ def wl_colour(b: Bench):
                    n_colours=n_col)
 
 
+ALSO_KEYS = ("value", "unit", "ms_per_step", "higher_is_better", "dtype", "us_per_level", "speedup_vs_per_level",
+             "batch_speedup_over_singles", "bitwise_equal_to_graph")
+
+
+def also_results(args):
+    """The rest of the headline metric ("SpMV/SpTRSV ...; batched+adjoint vs
+    plain"), measured in the same run on the same GPU: SpTRSV on the 2048^2
+    lower triangle in natural order (default scheme: graph-captured level
+    launches) and after the seed-3 permutation (default: sync-free), the
+    64-matrix batch against one launch per level and against 64 single
+    solves, and the SpMV / SpTRSV adjoints against their forward passes.
+    Each entry is the compact form of that workload's own bench line."""
+    import torch
+    sub = argparse.Namespace(**vars(args))
+    sub.tri_side, sub.tri_cases, sub.tri_modes, sub.tri_permuted_modes = 2048, "natural,permuted", "3", "0"
+    sub.tri_natural_only = False
+    b = Bench(sub)
+    b.collect = []
+    for fn in (wl_sptrsv, wl_sptrsv_batch, wl_adjoint):
+        fn(b)
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    out = []
+    for d in b.collect:
+        e = {"workload": d["config"]["workload"], "metric": d["metric"]}
+        e.update({k: d[k] for k in ALSO_KEYS if k in d and d[k] is not None})
+        if d.get("roofline"):
+            e["hbm_frac"] = d["roofline"]["frac"]
+        if d.get("cpu_baseline"):
+            e["cpu_baseline_ms"] = d["cpu_baseline"].get("ms_per_call")
+        e["clocks"] = d.get("clocks")
+        out.append(e)
+    return out
+
+
 def run_extra(args):
     import torch
     torch.cuda.set_device(0)
@@ -1204,6 +1295,8 @@ def main():
                     help="e2e: row blocks of the host-pointer SpMV pipeline (default: the library's)")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-also", action="store_true",
+                    help="skip the SpTRSV / batch / adjoint companions of the headline line")
     ap.add_argument("--no-gather-floor", action="store_true",
                     help="skip the gather-floor measurement beside the headline kernel")
     ap.add_argument("--rows", type=int, default=N_ROWS, help="rows per rank (default 2^22)")
@@ -1372,6 +1465,12 @@ def main():
         cpu = {"value": round(bytes_rank / t_cpu / 1e9, 3), "unit": UNIT, "cores": threads, "kind": kind,
                "sample": f"{n} full applies of the same matrix (0.89 GB each) after 1 warm-up"}
 
+    also = None
+    if world == 1 and not args.no_also:
+        # outside every timed region above: each companion times itself
+        also = also_results(args)
+        torch.cuda.set_stream(stream)
+
     peak, peak_kind = measured_peaks()
     achieved = bytes_rank / t_kernel / 1e9
     workload = config_dict(nnz, vbytes, world)["workload"]
@@ -1396,6 +1495,7 @@ def main():
             "ms": round(t_floor * 1e3, 5), "frac_of_floor": round(t_floor / t_kernel, 4),
             "what": "smax_measure_gather on this rank's matrix: the same val/col stream and one x gather per "
                     "entry through L2 loads, no row bookkeeping (the request-rate floor of this access pattern)"},
+        "also": also,
         "gpu_launches": args.steps * (1 if args.variant == 2 else 2),  # SpMV kernel (+ carry fix-up) per step
         "clocks": clocks,
     }

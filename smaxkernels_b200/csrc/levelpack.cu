@@ -17,9 +17,9 @@
 //   at pack time (the ring slot of position q is q % kRing; it survives until
 //   position q + kRing is written, so it is safe while q >= level_end - kRing).
 // * While a level is computed, each thread already loads the next level's
-//   entries, right-hand sides and diagonals into registers, and after the
-//   compute the block prefetches the level after that into L2: the critical
-//   path per level is ring reads, a few FMAs, the division and the CTA barrier.
+//   entries, right-hand sides and diagonals into registers, and the block
+//   prefetches the level kL2Ahead steps ahead into L2: the critical path per
+//   level is ring reads, a few FMAs, the division and the CTA barrier.
 // * Right-hand sides are gathered into position order before the sweep and
 //   the solution scattered back after it (two coalesced passes over n).
 #include "levelpack.cuh"
@@ -39,6 +39,14 @@ constexpr int kRing = LevelPack::kRing;
 constexpr int kRingShift = 13;     // kRing == 1 << kRingShift
 constexpr int kRowsPerThread = 2;  // rows of a level held in registers per thread (default sweeps)
 constexpr int kEnts = 2;           // prefetched entries per row (the rest are loaded when used)
+#ifndef SMAX_SWEEP_L2_AHEAD
+#define SMAX_SWEEP_L2_AHEAD 3
+#endif
+// levels between a level's L2 prefetch and its sweep (>= 2).  Three: the
+// 64-matrix batch 1.464 -> 1.265 ms and the natural 2048^2 sweep 5.41 -> 5.02
+// ms against two; four measured the same as three.
+constexpr int kL2Ahead = SMAX_SWEEP_L2_AHEAD;
+static_assert(kL2Ahead >= 2, "the next level is loaded into registers; L2 prefetch runs further ahead");
 constexpr int kClusterCTAs = 8;    // CTAs of a cluster run (portable cluster size)
 constexpr int kClusterThreads = 256;
 static_assert(kRing == (1 << kRingShift), "ring size");
@@ -267,7 +275,8 @@ __device__ __forceinline__ Level sweep_level(const Level *__restrict__ lv, int s
     constexpr int G = T * CS;
     const Level Lnn = load_level(lv, s + 2 < s1 ? s + 2 : s);
     if (s + 1 < s1 && warp0 < Ln.m) load_rows<VT, T, CS, NR>(Ln, g, psrc, pval, pinv, bp, nxt);
-    if (s + 2 < s1) prefetch_level_l2<VT>(Lnn, g, psrc, pval, pinv, bp);
+    if (s + kL2Ahead < s1)
+        prefetch_level_l2<VT>(kL2Ahead == 2 ? Lnn : load_level(lv, s + kL2Ahead), g, psrc, pval, pinv, bp);
     if (warp0 < Lc.m) {
 #pragma unroll
         for (int k = 0; k < NR; ++k) {
