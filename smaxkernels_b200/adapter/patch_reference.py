@@ -12,7 +12,8 @@
    library, smax_b200_platform.hpp) and SMAX_B200_ROUTE_ALL=1 (every kernel
    registered, whatever platform the test names, runs on the B200 platform),
    linked against smaxkernels_b200/libsmax_b200.so.  The runner is
-   OUT/run_tests; run it on a GPU machine.
+   OUT/run_tests (OUT defaults to smaxkernels_b200/adapter/_build, git-ignored);
+   run it on a GPU machine.
 
 The edits (file: what):
   common.hpp        KernelContext holds the platform's per-kernel state and
@@ -185,7 +186,7 @@ def build_runner(ref_root: str, out: str, cxx: str = "g++") -> str:
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--ref-root", default=os.environ.get("SMAX_REF_ROOT", "/root/reference"))
-    ap.add_argument("--out", default=os.path.join(REPO, "oracle", "_ref", "adapter"))
+    ap.add_argument("--out", default=os.path.join(HERE, "_build"))
     ap.add_argument("--build", action="store_true")
     ap.add_argument("--diff", action="store_true")
     a = ap.parse_args(argv)

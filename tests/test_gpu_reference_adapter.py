@@ -18,7 +18,7 @@ import tempfile
 import pytest
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-RUNNER = os.path.join(REPO, "oracle", "_ref", "adapter", "run_tests")
+RUNNER = os.path.join(REPO, "smaxkernels_b200", "adapter", "_build", "run_tests")
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not os.path.exists(RUNNER),
                                                   reason="the adapter's test runner is not built")]
