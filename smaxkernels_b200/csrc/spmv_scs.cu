@@ -225,9 +225,10 @@ __global__ void scs_keys_kernel(const int *__restrict__ row_ptr, int64_t n, int6
 
 // One sigma window per single-thread block, ordered exactly as the
 // reference's std::sort orders it (scs_window_sort.cuh).  A single thread per
-// block keeps the data-dependent loops free of warp divergence; up to 32
-// windows share an SM.  SMEM: the window is staged in shared memory (windows
-// of up to kScsSortSmemKeys keys), else it is sorted in place in `out`.
+// block keeps the data-dependent loops free of warp divergence; as many
+// windows share an SM as its block slots and shared memory allow (7 staged
+// windows of 4096 keys).  SMEM: the window is staged in shared memory
+// (windows of up to kScsSortSmemKeys keys), else it is sorted in place in `out`.
 constexpr int64_t kScsSortSmemKeys = 4096;  // 32 KB of keys per block
 
 template <bool SMEM>
