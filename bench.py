@@ -617,7 +617,7 @@ def wl_spgemm(b: Bench):
     b.emit("spgemm_f64_laplace3d_96", "SpGEMM GB/s (2A + 2B + C bytes)", nbytes / t / 1e9, "GB/s", t, reps, "f64",
            {"n_rows": n, "nnz_a": nnz, "nnz_c": nnz_c, "products": products,
             "l2": "A, B (77 MB) L2-resident across the fused pass"},
-           clk.summary(), b.hbm(nbytes, t, "gustavson_warp"), cpu, launches=None,
+           clk.summary(), b.hbm(nbytes, t, "gustavson_merge"), cpu, launches=None,
            gflops=round(2 * products / t / 1e9, 3), reference_gflops_2nnzC=round(2 * nnz_c / t / 1e9, 3))
     smax.close()
 

@@ -40,11 +40,17 @@ constexpr int kWarpP = 256, kWarpTS = 512;     // warp path
 constexpr int kCtaP = 4096, kCtaTS = 8192;     // CTA path
 constexpr int kCtaThreads = 512;
 constexpr int kWarpsPerCta = 4;
-constexpr int kBins = 4;
+constexpr int kMergeLists = 8;                 // merge path: at most this many entries in the row of A
+constexpr int kBins = 5;                       // small (hash), warp, CTA, global, merge
 
 __device__ __forceinline__ unsigned hash_col(int c) { return (unsigned)c * 0x9E3779B1u; }
 
 constexpr int kRowGroup = 8;  // lanes per row of the per-row helper passes (short rows)
+
+unsigned grid_cap(int64_t items) {  // a grid-stride launch of 256-thread blocks, at most 8 per SM
+    const int64_t want = (items + 255) / 256, cap = 8ll * sm_count();
+    return (unsigned)(want < 1 ? 1 : (want < cap ? want : cap));
+}
 
 // product count of every row of A (kRowGroup lanes per row)
 __global__ void row_products(const int *__restrict__ arp, const int *__restrict__ acol, const int *__restrict__ brp,
@@ -62,13 +68,29 @@ __global__ void row_products(const int *__restrict__ arp, const int *__restrict_
     if (i < n && lane == 0) P[i] = s;
 }
 
-// rows into four lists by product count (small-row warp, warp, CTA and global
-// paths); the order inside a list is irrelevant (rows are independent)
-__global__ void bin_rows(const long long *__restrict__ P, int64_t n, int *__restrict__ lists, int *counts) {
+// b_sorted = 1 unless some row of B has columns that do not strictly increase
+__global__ void b_sorted_kernel(const int *__restrict__ brp, const int *__restrict__ bcol, int64_t n,
+                                int *__restrict__ b_sorted) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride)
+        for (int j = brp[r] + 1; j < brp[r + 1]; ++j)
+            if (bcol[j] <= bcol[j - 1]) {
+                atomicAnd(b_sorted, 0);
+                return;
+            }
+}
+
+// rows into five lists: the merge path (B's rows sorted, at most kMergeLists
+// entries in the row of A and kSmallP products), then by product count the
+// small-row, warp, CTA and global hash paths; the order inside a list is
+// irrelevant (rows are independent)
+__global__ void bin_rows(const long long *__restrict__ P, const int *__restrict__ arp, int64_t n,
+                         const int *__restrict__ b_sorted, int *__restrict__ lists, int *counts) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < n;
     const long long p = valid ? P[i] : 0;
-    const int bin = p <= kSmallP ? 0 : (p <= kWarpP ? 1 : (p <= kCtaP ? 2 : 3));
+    const bool merge = valid && *b_sorted && p <= kSmallP && arp[i + 1] - arp[i] <= kMergeLists;
+    const int bin = merge ? 4 : (p <= kSmallP ? 0 : (p <= kWarpP ? 1 : (p <= kCtaP ? 2 : 3)));
     const unsigned active = __ballot_sync(0xffffffffu, valid);
     const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -289,6 +311,111 @@ __global__ void __launch_bounds__(WARPS * 32) gustavson_small(
     }
 }
 
+// The merge path: one thread per row of A with at most kMergeLists entries
+// and kSmallP products, when every row of B has strictly increasing columns.
+// The row's products are then the union of at most kMergeLists sorted lists
+// (the B rows its entries select), merged in registers.
+//   Pass 1 marks, for every distinct column, the product index p of its first
+//   touch in a 64-bit mask (the column's first occurrence in the lowest list
+//   holding it: lists are in the reference's (j, k) order).
+//   Pass 2 merges again; a column's value is 0 plus its products added in
+//   ascending list order -- the product order of the reference's zeroed
+//   accumulator -- and it is written at its first-touch rank, the number of
+//   mask bits below its p.
+// No shared memory, no atomics; a warp serves 32 rows.  MODE 0 runs both
+// passes and writes at the row's product offset (rows: a bin list); MODE 1
+// runs pass 1 only and stores the mask and the count; MODE 2 runs pass 2
+// with the stored mask and writes straight into C at its row pointer.  Modes
+// 1 and 2 cover every row of A in order (rows == nullptr).
+template <typename VT, int MODE>
+__global__ void __launch_bounds__(256) gustavson_merge(
+    const int *__restrict__ rows, int64_t n_rows_bin, const long long *__restrict__ Poff, const int *__restrict__ arp,
+    const int *__restrict__ acol, const VT *__restrict__ aval, const int *__restrict__ brp,
+    const int *__restrict__ bcol, const VT *__restrict__ bval, int *__restrict__ pcol, VT *__restrict__ pval,
+    int *__restrict__ count, unsigned long long *__restrict__ masks, const int *__restrict__ crp) {
+    constexpr int K = kMergeLists;
+    constexpr int INF = 0x7fffffff;
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rows_bin) return;
+    const int i = rows ? rows[r] : (int)r;
+    const int a0 = arp[i], la = arp[i + 1] - a0;
+    int kb[K], ke[K], off[K];  // list j: B entries [kb, ke); its products start at index off + kb
+    VT av[K];
+    int o = 0;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        kb[j] = ke[j] = off[j] = 0;
+        av[j] = VT(0);
+        if (j < la) {
+            const int c = acol[a0 + j];
+            av[j] = aval[a0 + j];
+            kb[j] = brp[c];
+            ke[j] = brp[c + 1];
+            off[j] = o - kb[j];
+            o += ke[j] - kb[j];
+        }
+    }
+    unsigned long long mask = 0ull;
+    if (MODE != 2) {  // pass 1: first-touch mask
+        int k[K], h[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            k[j] = kb[j];
+            h[j] = k[j] < ke[j] ? bcol[k[j]] : INF;
+        }
+        while (true) {
+            int m = INF;
+#pragma unroll
+            for (int j = 0; j < K; ++j) m = min(m, h[j]);
+            if (m == INF) break;
+            int fp = -1;
+#pragma unroll
+            for (int j = 0; j < K; ++j)
+                if (h[j] == m) {
+                    if (fp < 0) fp = off[j] + k[j];
+                    ++k[j];
+                    h[j] = k[j] < ke[j] ? bcol[k[j]] : INF;
+                }
+            mask |= 1ull << fp;
+        }
+        if (MODE == 1) {
+            masks[i] = mask;
+            count[i] = __popcll(mask);
+            return;
+        }
+    } else {
+        mask = masks[i];
+    }
+    // pass 2: sums in product order, written at first-touch ranks
+    const long long out = MODE == 2 ? (long long)crp[i] : Poff[i];
+    int k[K], h[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        k[j] = kb[j];
+        h[j] = k[j] < ke[j] ? bcol[k[j]] : INF;
+    }
+    while (true) {
+        int m = INF;
+#pragma unroll
+        for (int j = 0; j < K; ++j) m = min(m, h[j]);
+        if (m == INF) break;
+        int fp = -1;
+        VT sum = VT(0);
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            if (h[j] == m) {
+                if (fp < 0) fp = off[j] + k[j];
+                sum += av[j] * bval[k[j]];
+                ++k[j];
+                h[j] = k[j] < ke[j] ? bcol[k[j]] : INF;
+            }
+        const int pos = __popcll(mask & ((1ull << fp) - 1ull));
+        pcol[out + pos] = m;
+        pval[out + pos] = sum;
+    }
+    if (MODE == 0) count[i] = __popcll(mask);
+}
+
 template <typename VT>
 __global__ void __launch_bounds__(kCtaThreads) gustavson_cta(
     const int *__restrict__ rows, int n_rows_bin, const long long *__restrict__ P, const long long *__restrict__ Poff,
@@ -376,30 +503,38 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     w.P.ensure(sizeof(long long) * (n ? n : 1));
     w.Poff.ensure(sizeof(long long) * (n + 1));
     w.lists.ensure(sizeof(int) * kBins * (n ? n : 1));
-    w.counts.ensure(sizeof(int) * 4);
+    w.counts.ensure(sizeof(int) * (kBins + 1));  // the bin counts, then the b_sorted flag
     w.count.ensure(sizeof(int) * (n ? n : 1));
     long long *P = w.P.as<long long>(), *Poff = w.Poff.as<long long>();
-    SMAX_CUDA(cudaMemsetAsync(w.counts.p, 0, sizeof(int) * 4, st));
+    SMAX_CUDA(cudaMemsetAsync(w.counts.p, 0, sizeof(int) * kBins, st));
+    int *b_sorted = w.counts.as<int>() + kBins;
+    const int one = 1;
+    SMAX_CUDA(cudaMemcpyAsync(b_sorted, &one, sizeof(int), cudaMemcpyHostToDevice, st));
     if (n > 0) {
         row_products<<<ceil_div_u((uint64_t)n * kRowGroup, 256), 256, 0, st>>>(A.rp(), A.ci(), B.rp(), n, P);
-        bin_rows<<<ceil_div_u(n, 256), 256, 0, st>>>(P, n, w.lists.as<int>(), w.counts.as<int>());
+        if (B.n_rows > 0)
+            b_sorted_kernel<<<grid_cap(B.n_rows), 256, 0, st>>>(B.rp(), B.ci(), B.n_rows, b_sorted);
+        bin_rows<<<ceil_div_u(n, 256), 256, 0, st>>>(P, A.rp(), n, b_sorted, w.lists.as<int>(),
+                                                     w.counts.as<int>());
         SMAX_CUDA(cudaGetLastError());
     }
     excl_scan<long long>(P, Poff, n, w.scan_tmp, st);
     struct {
         long long total_p;
-        int counts[4];
+        int counts[kBins];
     } h{};
     SMAX_CUDA(cudaMemcpyAsync(&h.total_p, Poff + n, sizeof(long long), cudaMemcpyDeviceToHost, st));
-    SMAX_CUDA(cudaMemcpyAsync(h.counts, w.counts.p, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
+    SMAX_CUDA(cudaMemcpyAsync(h.counts, w.counts.p, sizeof(int) * kBins, cudaMemcpyDeviceToHost, st));
     SMAX_CUDA(cudaStreamSynchronize(st));
     const long long total_p = h.total_p;
-    const int ns = h.counts[0], nw = h.counts[1], nc = h.counts[2], ng = h.counts[3];
-    const int *rs = w.lists.as<int>(), *rw = rs + n, *rc = rs + 2 * n, *rg = rs + 3 * n;
+    const int ns = h.counts[0], nw = h.counts[1], nc = h.counts[2], ng = h.counts[3], nm = h.counts[4];
+    const int *rs = w.lists.as<int>(), *rw = rs + n, *rc = rs + 2 * n, *rg = rs + 3 * n, *rm = rs + 4 * n;
     SMAX_CUDA(cudaEventRecord(ev[1], st));
     // --- fused Gustavson pass into product-offset (padded) buffers
-    w.pcol.ensure(sizeof(int) * (total_p ? total_p : 1));
-    w.pval.ensure(sizeof(VT) * (total_p ? total_p : 1));
+    if (nm != n || n == 0) {  // the direct merge path writes C itself
+        w.pcol.ensure(sizeof(int) * (total_p ? total_p : 1));
+        w.pval.ensure(sizeof(VT) * (total_p ? total_p : 1));
+    }
     int *pcol = w.pcol.as<int>(), *count = w.count.as<int>();
     VT *pval = w.pval.as<VT>();
     if (ns > 0) {
@@ -416,6 +551,19 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
         const unsigned grid = (unsigned)std::min<int64_t>(need, (int64_t)ps * sm_count());
         kern<<<grid, kSmallWarps * 32, 0, st>>>(rs, ns, P, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(),
                                                 B.val.as<VT>(), pcol, pval, count);
+    }
+    // every row on the merge path: pass 1 counts, C's row pointer by scan,
+    // pass 2 writes C directly (no padded buffer, no compaction)
+    const bool direct = nm == n && n > 0;
+    if (direct) {
+        w.masks.ensure(sizeof(unsigned long long) * n);
+        gustavson_merge<VT, 1><<<ceil_div_u(n, 256), 256, 0, st>>>(
+            nullptr, n, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), nullptr, nullptr, count,
+            w.masks.as<unsigned long long>(), nullptr);
+    } else if (nm > 0) {
+        gustavson_merge<VT, 0><<<ceil_div_u(nm, 256), 256, 0, st>>>(
+            rm, nm, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), pcol, pval, count, nullptr,
+            nullptr);
     }
     if (nw > 0)
         gustavson_warp<VT, kWarpP, kWarpTS, kWarpsPerCta, 32><<<ceil_div_u(nw, kWarpsPerCta), kWarpsPerCta * 32, 0, st>>>(
@@ -456,7 +604,12 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     C.col.ensure(sizeof(int) * (nnz ? nnz : 1));
     C.val.ensure(sizeof(VT) * (nnz ? nnz : 1));
     SMAX_CUDA(cudaEventRecord(ev[3], st));
-    if (n > 0) {
+    if (direct) {
+        gustavson_merge<VT, 2><<<ceil_div_u(n, 256), 256, 0, st>>>(
+            nullptr, n, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), C.col.as<int>(),
+            C.val.as<VT>(), count, w.masks.as<unsigned long long>(), C.rp());
+        SMAX_CUDA(cudaGetLastError());
+    } else if (n > 0) {
         compact_kernel<VT><<<ceil_div_u((uint64_t)n * kRowGroup, 256), 256, 0, st>>>(C.rp(), Poff, n, pcol, pval,
                                                                               C.col.as<int>(), C.val.as<VT>());
         SMAX_CUDA(cudaGetLastError());

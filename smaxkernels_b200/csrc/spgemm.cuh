@@ -16,6 +16,7 @@ struct SpgemmTimes {
 struct SpgemmWork {
     DevBuf P, Poff, lists, counts, count, pcol, pval, scan_tmp;
     DevBuf wts, wsz, woff, wkeys, wfirst, wvals, wpos;
+    DevBuf masks;  // merge path: each row's first-touch mask
 };
 
 // C's columns per row are in first-touch order and its values are summed in

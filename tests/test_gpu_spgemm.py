@@ -86,3 +86,58 @@ def test_spgemm_config2_laplace96():
     np.testing.assert_array_equal(rp, orp)
     np.testing.assert_array_equal(col, ocol)
     assert normwise(val, oval) <= 1e-12
+
+
+def _shuffle_rows(rp, col, val, seed):
+    """The same matrix with each row's entries in a random order."""
+    rng = np.random.default_rng(seed)
+    col, val = col.copy(), val.copy()
+    for r in range(len(rp) - 1):
+        a, b = rp[r], rp[r + 1]
+        o = rng.permutation(b - a)
+        col[a:b], val[a:b] = col[a:b][o], val[a:b][o]
+    return rp, col, val
+
+
+@pytest.mark.parametrize("sorted_b", [True, False])
+def test_spgemm_merge_and_hash_paths_vs_oracle(sorted_b):
+    """Rows of A with at most 8 entries and 64 products take the merge path
+    when every row of B has increasing columns; with B's rows shuffled every
+    row takes the hash paths.  Both give the first-touch pattern and the
+    product-order sums of the oracle.  The matrix mixes rows at the merge
+    limits (8 entries, products up to 64), rows of 9+ entries, empty rows of
+    A and of B."""
+    rng = np.random.default_rng(120)
+    n = 3000
+    lens = rng.integers(0, 10, n)
+    lens[::7] = 8
+    lens[::11] = 0
+    rows = [np.sort(rng.choice(n, int(l), replace=False)) for l in lens]
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum(lens)
+    col = np.concatenate(rows).astype(np.int32)
+    A = (rp, col, rng.uniform(-1, 1, len(col)))
+    blens = rng.integers(0, 9, n)
+    blens[::13] = 0
+    brows = [np.sort(rng.choice(n, int(l), replace=False)) for l in blens]
+    brp = np.zeros(n + 1, np.int32)
+    brp[1:] = np.cumsum(blens)
+    B = (brp, np.concatenate(brows).astype(np.int32), rng.uniform(-1, 1, int(blens.sum())))
+    if not sorted_b:
+        B = _shuffle_rows(*B, seed=121)
+    n_rows, n_cols, nnz, crp, ccol, cval = gpu_spgemm(A, B, n, n)
+    orp, ocol, oval = O.spgemm(*A, *B, n)
+    np.testing.assert_array_equal(crp, orp)
+    np.testing.assert_array_equal(ccol, ocol)
+    assert normwise(cval, oval) <= 1e-12
+
+
+def test_spgemm_merge_path_rectangular():
+    A = rand_crs(1200, 8, 122, n_cols=700)
+    B = rand_crs(700, 8, 123, n_cols=2500)
+    n_rows, n_cols, nnz, rp, col, val = gpu_spgemm(A, B, 700, 2500)
+    orp, ocol, oval = O.spgemm(*A, *B, 2500)
+    assert (n_rows, n_cols) == (1200, 2500)
+    np.testing.assert_array_equal(rp, orp)
+    np.testing.assert_array_equal(col, ocol)
+    assert normwise(val, oval) <= 1e-12
