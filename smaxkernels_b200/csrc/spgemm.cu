@@ -7,7 +7,11 @@
 // (numerical_phase_impl.hpp:9-91) accumulates every product in that (j, k)
 // order.  C_n_rows = A_n_rows, C_n_cols = B_n_cols.
 //
-// Design.  One fused pass per row of A, binned by its product count P_i:
+// Design.  When every row of B has increasing columns, a row of A with at most
+// 8 entries and 64 products takes the merge path: one thread merges the row's
+// B lists in registers (no table; see gustavson_merge).  If every row of A
+// qualifies, C is written directly by a counting pass and a writing pass.
+// Other rows take one fused hash pass, binned by their product count P_i:
 //   * P_i <= 64:    a team of 8 lanes, hash table in shared memory (128 slots),
 //                   persistent teams that reset only the slots a row used;
 //   * P_i <= 256:   one warp, hash table in shared memory (512 slots);
@@ -42,6 +46,7 @@ constexpr int kCtaThreads = 512;
 constexpr int kWarpsPerCta = 4;
 constexpr int kMergeLists = 8;                 // merge path: at most this many entries in the row of A
 constexpr int kBins = 5;                       // small (hash), warp, CTA, global, merge
+constexpr int kMergeWriteThreads = 128;        // direct write pass: 4 warps, each staging its rows in shared memory
 
 __device__ __forceinline__ unsigned hash_col(int c) { return (unsigned)c * 0x9E3779B1u; }
 
@@ -322,77 +327,47 @@ __global__ void __launch_bounds__(WARPS * 32) gustavson_small(
 //   ascending list order -- the product order of the reference's zeroed
 //   accumulator -- and it is written at its first-touch rank, the number of
 //   mask bits below its p.
-// No shared memory, no atomics; a warp serves 32 rows.  MODE 0 runs both
-// passes and writes at the row's product offset (rows: a bin list); MODE 1
-// runs pass 1 only and stores the mask and the count; MODE 2 runs pass 2
-// with the stored mask and writes straight into C at its row pointer.  Modes
-// 1 and 2 cover every row of A in order (rows == nullptr).
-template <typename VT, int MODE>
-__global__ void __launch_bounds__(256) gustavson_merge(
-    const int *__restrict__ rows, int64_t n_rows_bin, const long long *__restrict__ Poff, const int *__restrict__ arp,
-    const int *__restrict__ acol, const VT *__restrict__ aval, const int *__restrict__ brp,
-    const int *__restrict__ bcol, const VT *__restrict__ bval, int *__restrict__ pcol, VT *__restrict__ pval,
-    int *__restrict__ count, unsigned long long *__restrict__ masks, const int *__restrict__ crp) {
-    constexpr int K = kMergeLists;
-    constexpr int INF = 0x7fffffff;
-    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n_rows_bin) return;
-    const int i = rows ? rows[r] : (int)r;
+// No atomics on the data; a warp serves 32 rows.
+template <typename VT>
+struct MergeLists {  // list j: B entries [kb, ke); its products start at index off + kb
+    int kb[kMergeLists], ke[kMergeLists], off[kMergeLists];
+    VT av[kMergeLists];
+};
+
+template <typename VT>
+__device__ __forceinline__ void merge_lists(int i, const int *__restrict__ arp, const int *__restrict__ acol,
+                                            const VT *__restrict__ aval, const int *__restrict__ brp,
+                                            MergeLists<VT> &L) {
     const int a0 = arp[i], la = arp[i + 1] - a0;
-    int kb[K], ke[K], off[K];  // list j: B entries [kb, ke); its products start at index off + kb
-    VT av[K];
     int o = 0;
 #pragma unroll
-    for (int j = 0; j < K; ++j) {
-        kb[j] = ke[j] = off[j] = 0;
-        av[j] = VT(0);
+    for (int j = 0; j < kMergeLists; ++j) {
+        L.kb[j] = L.ke[j] = L.off[j] = 0;
+        L.av[j] = VT(0);
         if (j < la) {
             const int c = acol[a0 + j];
-            av[j] = aval[a0 + j];
-            kb[j] = brp[c];
-            ke[j] = brp[c + 1];
-            off[j] = o - kb[j];
-            o += ke[j] - kb[j];
+            L.av[j] = aval[a0 + j];
+            L.kb[j] = brp[c];
+            L.ke[j] = brp[c + 1];
+            L.off[j] = o - L.kb[j];
+            o += L.ke[j] - L.kb[j];
         }
     }
-    unsigned long long mask = 0ull;
-    if (MODE != 2) {  // pass 1: first-touch mask
-        int k[K], h[K];
-#pragma unroll
-        for (int j = 0; j < K; ++j) {
-            k[j] = kb[j];
-            h[j] = k[j] < ke[j] ? bcol[k[j]] : INF;
-        }
-        while (true) {
-            int m = INF;
-#pragma unroll
-            for (int j = 0; j < K; ++j) m = min(m, h[j]);
-            if (m == INF) break;
-            int fp = -1;
-#pragma unroll
-            for (int j = 0; j < K; ++j)
-                if (h[j] == m) {
-                    if (fp < 0) fp = off[j] + k[j];
-                    ++k[j];
-                    h[j] = k[j] < ke[j] ? bcol[k[j]] : INF;
-                }
-            mask |= 1ull << fp;
-        }
-        if (MODE == 1) {
-            masks[i] = mask;
-            count[i] = __popcll(mask);
-            return;
-        }
-    } else {
-        mask = masks[i];
-    }
-    // pass 2: sums in product order, written at first-touch ranks
-    const long long out = MODE == 2 ? (long long)crp[i] : Poff[i];
+}
+
+// Visits the union of the lists in ascending column order: f(col, p, sum)
+// with p the column's first product index and (SUM) its products summed in
+// list order.
+template <bool SUM, typename VT, typename F>
+__device__ __forceinline__ void merge_walk(const MergeLists<VT> &L, const int *__restrict__ bcol,
+                                           const VT *__restrict__ bval, F f) {
+    constexpr int K = kMergeLists;
+    constexpr int INF = 0x7fffffff;
     int k[K], h[K];
 #pragma unroll
     for (int j = 0; j < K; ++j) {
-        k[j] = kb[j];
-        h[j] = k[j] < ke[j] ? bcol[k[j]] : INF;
+        k[j] = L.kb[j];
+        h[j] = k[j] < L.ke[j] ? bcol[k[j]] : INF;
     }
     while (true) {
         int m = INF;
@@ -404,16 +379,100 @@ __global__ void __launch_bounds__(256) gustavson_merge(
 #pragma unroll
         for (int j = 0; j < K; ++j)
             if (h[j] == m) {
-                if (fp < 0) fp = off[j] + k[j];
-                sum += av[j] * bval[k[j]];
+                if (fp < 0) fp = L.off[j] + k[j];
+                if (SUM) sum += L.av[j] * bval[k[j]];
                 ++k[j];
-                h[j] = k[j] < ke[j] ? bcol[k[j]] : INF;
+                h[j] = k[j] < L.ke[j] ? bcol[k[j]] : INF;
             }
-        const int pos = __popcll(mask & ((1ull << fp) - 1ull));
+        f(m, fp, sum);
+    }
+}
+
+__device__ __forceinline__ int first_touch_rank(unsigned long long mask, int p) {
+    return __popcll(mask & ((1ull << p) - 1ull));
+}
+
+// MODE 0: both passes for the rows of a bin list, written at each row's
+// product offset.  MODE 1: pass 1 for every row of A in order; stores the
+// mask and the count, and raises *warp_max to the largest number of C
+// entries that one warp's 32 rows hold (the staging size of the write pass).
+template <typename VT, int MODE>
+__global__ void __launch_bounds__(256) gustavson_merge(
+    const int *__restrict__ rows, int64_t n_rows_bin, const long long *__restrict__ Poff, const int *__restrict__ arp,
+    const int *__restrict__ acol, const VT *__restrict__ aval, const int *__restrict__ brp,
+    const int *__restrict__ bcol, const VT *__restrict__ bval, int *__restrict__ pcol, VT *__restrict__ pval,
+    int *__restrict__ count, unsigned long long *__restrict__ masks, int *__restrict__ warp_max) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (MODE == 0 && r >= n_rows_bin) return;
+    const bool valid = r < n_rows_bin;
+    const int i = rows ? rows[r] : (int)r;
+    unsigned long long mask = 0ull;
+    MergeLists<VT> L;
+    if (valid) {
+        merge_lists<VT>(i, arp, acol, aval, brp, L);
+        merge_walk<false>(L, bcol, bval, [&](int, int fp, VT) { mask |= 1ull << fp; });
+    }
+    const int cnt = __popcll(mask);
+    if (MODE == 1) {
+        if (valid) {
+            masks[i] = mask;
+            count[i] = cnt;
+        }
+        int t = cnt;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if ((threadIdx.x & 31) == 0 && t > 0) atomicMax(warp_max, t);
+        return;
+    }
+    const long long out = Poff[i];
+    merge_walk<true>(L, bcol, bval, [&](int m, int fp, VT sum) {
+        const int pos = first_touch_rank(mask, fp);
         pcol[out + pos] = m;
         pval[out + pos] = sum;
+    });
+    count[i] = cnt;
+}
+
+// Pass 2 of the direct path (every row of A on the merge path): each warp
+// stages its 32 rows' entries -- a contiguous range of C -- in shared memory
+// and writes that range with coalesced stores.  `stage` entries per warp
+// (at least the largest range, so every warp fits).
+template <typename VT>
+__global__ void __launch_bounds__(kMergeWriteThreads) gustavson_merge_write(
+    int64_t n, int stage, const int *__restrict__ arp, const int *__restrict__ acol, const VT *__restrict__ aval,
+    const int *__restrict__ brp, const int *__restrict__ bcol, const VT *__restrict__ bval,
+    const unsigned long long *__restrict__ masks, const int *__restrict__ crp, int *__restrict__ ccol,
+    VT *__restrict__ cval) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    VT *sval = reinterpret_cast<VT *>(smem) + (int64_t)warp * stage;
+    int *scol = reinterpret_cast<int *>(reinterpret_cast<VT *>(smem) + (int64_t)(blockDim.x >> 5) * stage) +
+                (int64_t)warp * stage;
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t w0 = r - lane;  // the warp's first row
+    if (w0 >= n) return;          // the whole warp
+    const int64_t w1 = w0 + 32 < n ? w0 + 32 : n;
+    const long long base = crp[w0];
+    const int total = (int)(crp[w1] - base);
+    if (r < n) {
+        const int i = (int)r;
+        const unsigned long long mask = masks[i];
+        MergeLists<VT> L;
+        merge_lists<VT>(i, arp, acol, aval, brp, L);
+        const int at = (int)(crp[i] - base);
+        merge_walk<true>(L, bcol, bval, [&](int m, int fp, VT sum) {
+            const int pos = at + first_touch_rank(mask, fp);
+            if (pos < total) {  // always: the row's ranks are below its count
+                scol[pos] = m;
+                sval[pos] = sum;
+            }
+        });
     }
-    if (MODE == 0) count[i] = __popcll(mask);
+    __syncwarp();
+    for (int t = lane; t < total; t += 32) {
+        ccol[base + t] = scol[t];
+        cval[base + t] = sval[t];
+    }
 }
 
 template <typename VT>
@@ -503,11 +562,11 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     w.P.ensure(sizeof(long long) * (n ? n : 1));
     w.Poff.ensure(sizeof(long long) * (n + 1));
     w.lists.ensure(sizeof(int) * kBins * (n ? n : 1));
-    w.counts.ensure(sizeof(int) * (kBins + 1));  // the bin counts, then the b_sorted flag
+    w.counts.ensure(sizeof(int) * (kBins + 2));  // the bin counts, the b_sorted flag, the merge warp maximum
     w.count.ensure(sizeof(int) * (n ? n : 1));
     long long *P = w.P.as<long long>(), *Poff = w.Poff.as<long long>();
-    SMAX_CUDA(cudaMemsetAsync(w.counts.p, 0, sizeof(int) * kBins, st));
-    int *b_sorted = w.counts.as<int>() + kBins;
+    SMAX_CUDA(cudaMemsetAsync(w.counts.p, 0, sizeof(int) * (kBins + 2), st));
+    int *b_sorted = w.counts.as<int>() + kBins, *warp_max = b_sorted + 1;
     const int one = 1;
     SMAX_CUDA(cudaMemcpyAsync(b_sorted, &one, sizeof(int), cudaMemcpyHostToDevice, st));
     if (n > 0) {
@@ -559,7 +618,7 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
         w.masks.ensure(sizeof(unsigned long long) * n);
         gustavson_merge<VT, 1><<<ceil_div_u(n, 256), 256, 0, st>>>(
             nullptr, n, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), nullptr, nullptr, count,
-            w.masks.as<unsigned long long>(), nullptr);
+            w.masks.as<unsigned long long>(), warp_max);
     } else if (nm > 0) {
         gustavson_merge<VT, 0><<<ceil_div_u(nm, 256), 256, 0, st>>>(
             rm, nm, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), pcol, pval, count, nullptr,
@@ -597,17 +656,29 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     SMAX_CUDA(cudaEventRecord(ev[2], st));
     // --- C's row pointer and arrays
     excl_scan<int>(count, C.row_ptr.as<int>(), n, w.scan_tmp, st);
-    int nnz = 0;
+    int nnz = 0, stage = 0;
     SMAX_CUDA(cudaMemcpyAsync(&nnz, C.row_ptr.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (direct) SMAX_CUDA(cudaMemcpyAsync(&stage, warp_max, sizeof(int), cudaMemcpyDeviceToHost, st));
     SMAX_CUDA(cudaStreamSynchronize(st));
     C.nnz = nnz;
     C.col.ensure(sizeof(int) * (nnz ? nnz : 1));
     C.val.ensure(sizeof(VT) * (nnz ? nnz : 1));
     SMAX_CUDA(cudaEventRecord(ev[3], st));
     if (direct) {
-        gustavson_merge<VT, 2><<<ceil_div_u(n, 256), 256, 0, st>>>(
-            nullptr, n, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), C.col.as<int>(),
-            C.val.as<VT>(), count, w.masks.as<unsigned long long>(), C.rp());
+        // a warp's 32 rows hold at most 32 * kSmallP entries
+        stage = std::max(8, (stage + 7) / 8 * 8);
+        if (stage > 32 * kSmallP) fail(SMAX_ERR_STATE, "SpGEMM merge path: staging size out of range");
+        constexpr int kMaxSmem = kMergeWriteThreads / 32 * 32 * kSmallP * (int)(sizeof(VT) + sizeof(int));
+        static bool attr_set[2] = {false, false};
+        if (!attr_set[sizeof(VT) == 8]) {
+            SMAX_CUDA(cudaFuncSetAttribute(gustavson_merge_write<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kMaxSmem));
+            attr_set[sizeof(VT) == 8] = true;
+        }
+        const size_t smem = (size_t)kMergeWriteThreads / 32 * stage * (sizeof(VT) + sizeof(int));
+        gustavson_merge_write<VT><<<ceil_div_u(n, kMergeWriteThreads), kMergeWriteThreads, smem, st>>>(
+            n, stage, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(),
+            w.masks.as<unsigned long long>(), C.rp(), C.col.as<int>(), C.val.as<VT>());
         SMAX_CUDA(cudaGetLastError());
     } else if (n > 0) {
         compact_kernel<VT><<<ceil_div_u((uint64_t)n * kRowGroup, 256), 256, 0, st>>>(C.rp(), Poff, n, pcol, pval,

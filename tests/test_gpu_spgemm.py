@@ -141,3 +141,48 @@ def test_spgemm_merge_path_rectangular():
     np.testing.assert_array_equal(rp, orp)
     np.testing.assert_array_equal(col, ocol)
     assert normwise(val, oval) <= 1e-12
+
+
+@pytest.mark.parametrize("case", ["disjoint64", "overlapping"])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_spgemm_direct_merge_path(case, dtype):
+    """Every row of A on the merge path, so C is written straight from the
+    second merge pass, one warp staging its 32 rows in shared memory.
+    "disjoint64": every non-empty row of A selects 8 B rows with disjoint
+    columns, 64 distinct entries per row of C -- the largest staging size.
+    "overlapping": random rows of at most 8 entries over short sorted B rows.
+    Both have empty rows and a row count that ends in a partial warp."""
+    rng = np.random.default_rng(124 if case == "disjoint64" else 125)
+    n = 32 * 37 + 19
+    if case == "disjoint64":
+        nb = 700
+        brp = np.arange(nb + 1, dtype=np.int32) * 8
+        bcol = (np.arange(nb)[:, None] * 8 + np.arange(8)[None, :]).reshape(-1).astype(np.int32)
+        b_n_cols = 8 * nb
+        lens = np.full(n, 8)
+        lens[::9] = 0
+        rows = [rng.choice(nb, 8, replace=False) if l else np.zeros(0, int) for l in lens]
+    else:
+        nb = 900
+        blens = rng.integers(0, 9, nb)
+        blens[::17] = 0
+        brp = np.zeros(nb + 1, np.int32)
+        brp[1:] = np.cumsum(blens)
+        bcol = np.concatenate([np.sort(rng.choice(nb, int(l), replace=False)) for l in blens]).astype(np.int32)
+        b_n_cols = nb
+        lens = rng.integers(0, 9, n)
+        lens[::5] = 0
+        rows = [rng.choice(nb, int(l), replace=False) for l in lens]
+    bval = rng.uniform(-1, 1, len(bcol)).astype(dtype)
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    col = np.concatenate(rows).astype(np.int32)
+    A = (rp, col, rng.uniform(-1, 1, len(col)).astype(dtype))
+    B = (brp, bcol, bval)
+    n_rows, n_cols, nnz, crp, ccol, cval = gpu_spgemm(A, B, nb, b_n_cols)
+    orp, ocol, oval = O.spgemm(*A, *B, b_n_cols)
+    if case == "disjoint64":
+        assert np.diff(orp).max() == 64
+    np.testing.assert_array_equal(crp, orp)
+    np.testing.assert_array_equal(ccol, ocol)
+    assert normwise(cval, oval) <= tol(dtype)
