@@ -263,20 +263,21 @@ template <int CS> __device__ __forceinline__ void run_barrier() {
     else cooperative_groups::this_cluster().sync();  // barrier.cluster arrive.release / wait.acquire
 }
 
-// One level s of a run: loads level s+1's rows into `nxt` (and prefetches
-// level s+2 into L2) while it solves level s from `cur`, then the run's
-// barrier.  Returns level s+2's descriptor.
+// One level s of a run: loads level fill_s's rows (described by Ln) into
+// `nxt` and prefetches level s+kL2Ahead into L2 while it solves level s from
+// `cur`, then the run's barrier.  Returns level ret_s's descriptor.  With two
+// register sets fill_s = s+1 and ret_s = s+2; with three, s+2 and s+3.
 template <typename VT, int T, int CS, int NR>
 __device__ __forceinline__ Level sweep_level(const Level *__restrict__ lv, int s, int s1, const Level &Lc,
-                                             const Level &Ln, const int *__restrict__ psrc,
+                                             const Level &Ln, int fill_s, int ret_s, const int *__restrict__ psrc,
                                              const VT *__restrict__ pval, const VT *__restrict__ pinv,
                                              const VT *__restrict__ bp, VT *xp, VT *ring, int g, int warp0,
                                              unsigned rank, RowRegs<VT> (&cur)[NR], RowRegs<VT> (&nxt)[NR]) {
     constexpr int G = T * CS;
-    const Level Lnn = load_level(lv, s + 2 < s1 ? s + 2 : s);
-    if (s + 1 < s1 && warp0 < Ln.m) load_rows<VT, T, CS, NR>(Ln, g, psrc, pval, pinv, bp, nxt);
+    const Level Lnn = load_level(lv, ret_s < s1 ? ret_s : s);
+    if (fill_s < s1 && warp0 < Ln.m) load_rows<VT, T, CS, NR>(Ln, g, psrc, pval, pinv, bp, nxt);
     if (s + kL2Ahead < s1)
-        prefetch_level_l2<VT>(kL2Ahead == 2 ? Lnn : load_level(lv, s + kL2Ahead), g, psrc, pval, pinv, bp);
+        prefetch_level_l2<VT>(load_level(lv, s + kL2Ahead), g, psrc, pval, pinv, bp);
     if (warp0 < Lc.m) {
 #pragma unroll
         for (int k = 0; k < NR; ++k) {
@@ -326,10 +327,12 @@ __device__ __forceinline__ Level sweep_level(const Level *__restrict__ lv, int s
 
 // Sweeps steps [s0, s1) of the pack with CS CTAs of T threads (one CTA or one
 // cluster); thread g of the run solves rows g, g + T*CS, ... of every level,
-// the first NR of them from registers loaded one level ahead.  Two register
-// sets alternate between "this level" and "the next", two levels per turn,
-// so no set is copied into the other.
-template <typename VT, int T, int CS, int NR = kRowsPerThread>
+// the first NR of them from registers loaded ahead.  Register sets rotate
+// between "this level" and the ones after it, so no set is copied into
+// another: two sets (loaded one level ahead), or with THREE three sets
+// (two levels ahead; the batched sweep's 512-thread CTAs: 1.265 -> 1.199 ms
+// for 64 matrices, while the single solve's sweeps were 3 % slower with it).
+template <typename VT, int T, int CS, int NR = kRowsPerThread, bool THREE = false>
 __device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const int *__restrict__ psrc,
                           const VT *__restrict__ pval, const VT *__restrict__ pinv, const VT *__restrict__ bp, VT *xp,
                           VT *ring) {
@@ -338,18 +341,40 @@ __device__ void sweep_run(const Level *__restrict__ lv, int s0, int s1, const in
     if constexpr (CS > 1) rank = cooperative_groups::this_cluster().block_rank();
     const int g = (int)rank * T + (int)threadIdx.x;
     const int warp0 = g & ~31;
-    RowRegs<VT> ra[NR], rb[NR];
-    Level La = load_level(lv, s0);
-    Level Lb = load_level(lv, s0 + 1 < s1 ? s0 + 1 : s0);
-    load_rows<VT, T, CS, NR>(La, g, psrc, pval, pinv, bp, ra);
-    for (int s = s0; s < s1; s += 2) {
-        const Level L2 =
-            sweep_level<VT, T, CS, NR>(lv, s, s1, La, Lb, psrc, pval, pinv, bp, xp, ring, g, warp0, rank, ra, rb);
-        if (s + 1 >= s1) break;
-        const Level L3 = sweep_level<VT, T, CS, NR>(lv, s + 1, s1, Lb, L2, psrc, pval, pinv, bp, xp, ring, g, warp0,
-                                                    rank, rb, ra);
-        La = L2;
-        Lb = L3;
+    if constexpr (THREE && T * NR <= 1024) {  // 1024-thread CTAs keep two sets (64 registers a thread)
+        RowRegs<VT> ra[NR], rb[NR], rc[NR];
+        Level La = load_level(lv, s0);
+        Level Lb = load_level(lv, s0 + 1 < s1 ? s0 + 1 : s0);
+        Level Lc = load_level(lv, s0 + 2 < s1 ? s0 + 2 : s0);
+        load_rows<VT, T, CS, NR>(La, g, psrc, pval, pinv, bp, ra);
+        if (s0 + 1 < s1) load_rows<VT, T, CS, NR>(Lb, g, psrc, pval, pinv, bp, rb);
+        for (int s = s0; s < s1; s += 3) {
+            const Level Ld = sweep_level<VT, T, CS, NR>(lv, s, s1, La, Lc, s + 2, s + 3, psrc, pval, pinv, bp, xp,
+                                                        ring, g, warp0, rank, ra, rc);
+            if (s + 1 >= s1) break;
+            const Level Le = sweep_level<VT, T, CS, NR>(lv, s + 1, s1, Lb, Ld, s + 3, s + 4, psrc, pval, pinv, bp,
+                                                        xp, ring, g, warp0, rank, rb, ra);
+            if (s + 2 >= s1) break;
+            const Level Lf = sweep_level<VT, T, CS, NR>(lv, s + 2, s1, Lc, Le, s + 4, s + 5, psrc, pval, pinv, bp,
+                                                        xp, ring, g, warp0, rank, rc, rb);
+            La = Ld;
+            Lb = Le;
+            Lc = Lf;
+        }
+    } else {
+        RowRegs<VT> ra[NR], rb[NR];
+        Level La = load_level(lv, s0);
+        Level Lb = load_level(lv, s0 + 1 < s1 ? s0 + 1 : s0);
+        load_rows<VT, T, CS, NR>(La, g, psrc, pval, pinv, bp, ra);
+        for (int s = s0; s < s1; s += 2) {
+            const Level L2 = sweep_level<VT, T, CS, NR>(lv, s, s1, La, Lb, s + 1, s + 2, psrc, pval, pinv, bp, xp,
+                                                        ring, g, warp0, rank, ra, rb);
+            if (s + 1 >= s1) break;
+            const Level L3 = sweep_level<VT, T, CS, NR>(lv, s + 1, s1, Lb, L2, s + 2, s + 3, psrc, pval, pinv, bp,
+                                                        xp, ring, g, warp0, rank, rb, ra);
+            La = L2;
+            Lb = L3;
+        }
     }
 }
 
@@ -386,7 +411,7 @@ __global__ void __launch_bounds__(T, 1)
         __syncthreads();  // m_sh is rewritten on the next turn
         if (q >= n_mats) return;
         const int m = queue_order[q];
-        sweep_run<VT, T, 1>(lv, mat_steps[m], mat_steps[m + 1], psrc, pval, pinv, bp, xp,
+        sweep_run<VT, T, 1, kRowsPerThread, true>(lv, mat_steps[m], mat_steps[m + 1], psrc, pval, pinv, bp, xp,
                             reinterpret_cast<VT *>(smem));
     }
 }

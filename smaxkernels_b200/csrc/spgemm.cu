@@ -334,10 +334,12 @@ struct MergeLists {  // list j: B entries [kb, ke); its products start at index 
     VT av[kMergeLists];
 };
 
+// Fills the lists of row i from its first kMergeLists entries; returns the
+// products of those entries.
 template <typename VT>
-__device__ __forceinline__ void merge_lists(int i, const int *__restrict__ arp, const int *__restrict__ acol,
-                                            const VT *__restrict__ aval, const int *__restrict__ brp,
-                                            MergeLists<VT> &L) {
+__device__ __forceinline__ int merge_lists(int i, const int *__restrict__ arp, const int *__restrict__ acol,
+                                           const VT *__restrict__ aval, const int *__restrict__ brp,
+                                           MergeLists<VT> &L) {
     const int a0 = arp[i], la = arp[i + 1] - a0;
     int o = 0;
 #pragma unroll
@@ -353,14 +355,17 @@ __device__ __forceinline__ void merge_lists(int i, const int *__restrict__ arp, 
             o += L.ke[j] - L.kb[j];
         }
     }
+    return o;
 }
 
 // Visits the union of the lists in ascending column order: f(col, p, sum)
 // with p the column's first product index and (SUM) its products summed in
-// list order.
+// list order.  Returns false if some list does not strictly increase (the
+// walk then still ends, and every p stays below the row's product count).
 template <bool SUM, typename VT, typename F>
-__device__ __forceinline__ void merge_walk(const MergeLists<VT> &L, const int *__restrict__ bcol,
+__device__ __forceinline__ bool merge_walk(const MergeLists<VT> &L, const int *__restrict__ bcol,
                                            const VT *__restrict__ bval, F f) {
+    bool increasing = true;
     constexpr int K = kMergeLists;
     constexpr int INF = 0x7fffffff;
     int k[K], h[K];
@@ -383,9 +388,11 @@ __device__ __forceinline__ void merge_walk(const MergeLists<VT> &L, const int *_
                 if (SUM) sum += L.av[j] * bval[k[j]];
                 ++k[j];
                 h[j] = k[j] < L.ke[j] ? bcol[k[j]] : INF;
+                increasing &= h[j] > m;
             }
         f(m, fp, sum);
     }
+    return increasing;
 }
 
 __device__ __forceinline__ int first_touch_rank(unsigned long long mask, int p) {
@@ -394,14 +401,18 @@ __device__ __forceinline__ int first_touch_rank(unsigned long long mask, int p) 
 
 // MODE 0: both passes for the rows of a bin list, written at each row's
 // product offset.  MODE 1: pass 1 for every row of A in order; stores the
-// mask and the count, and raises *warp_max to the largest number of C
-// entries that one warp's 32 rows hold (the staging size of the write pass).
+// mask and the count, raises *warp_max to the largest number of C entries
+// that one warp's 32 rows hold (the staging size of the write pass), and
+// sets *off_path if a row does not qualify for the merge path (more than
+// kMergeLists entries, more than kSmallP products, or a B list that does
+// not strictly increase) -- then the masks are not used.
 template <typename VT, int MODE>
 __global__ void __launch_bounds__(256) gustavson_merge(
     const int *__restrict__ rows, int64_t n_rows_bin, const long long *__restrict__ Poff, const int *__restrict__ arp,
     const int *__restrict__ acol, const VT *__restrict__ aval, const int *__restrict__ brp,
     const int *__restrict__ bcol, const VT *__restrict__ bval, int *__restrict__ pcol, VT *__restrict__ pval,
-    int *__restrict__ count, unsigned long long *__restrict__ masks, int *__restrict__ warp_max) {
+    int *__restrict__ count, unsigned long long *__restrict__ masks, int *__restrict__ warp_max,
+    int *__restrict__ off_path) {
     const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (MODE == 0 && r >= n_rows_bin) return;
     const bool valid = r < n_rows_bin;
@@ -409,8 +420,13 @@ __global__ void __launch_bounds__(256) gustavson_merge(
     unsigned long long mask = 0ull;
     MergeLists<VT> L;
     if (valid) {
-        merge_lists<VT>(i, arp, acol, aval, brp, L);
-        merge_walk<false>(L, bcol, bval, [&](int, int fp, VT) { mask |= 1ull << fp; });
+        const int o = merge_lists<VT>(i, arp, acol, aval, brp, L);
+        if (MODE == 1 && (arp[i + 1] - arp[i] > kMergeLists || o > kSmallP)) {
+            *off_path = 1;
+        } else {
+            const bool inc = merge_walk<false>(L, bcol, bval, [&](int, int fp, VT) { mask |= 1ull << fp; });
+            if (MODE == 1 && !inc) *off_path = 1;
+        }
     }
     const int cnt = __popcll(mask);
     if (MODE == 1) {
@@ -542,6 +558,45 @@ template <typename T> void excl_scan(const T *in, T *out, int64_t n, DevBuf &tmp
 
 }  // namespace
 
+namespace {
+
+void record_times(cudaEvent_t *ev, SpgemmTimes *times) {
+    if (!times) return;
+    float a = 0, b = 0, c = 0, d = 0;
+    cudaEventElapsedTime(&a, ev[0], ev[1]);
+    cudaEventElapsedTime(&b, ev[1], ev[2]);
+    cudaEventElapsedTime(&c, ev[2], ev[3]);
+    cudaEventElapsedTime(&d, ev[3], ev[4]);
+    times->setup = a * 1e-3;
+    times->fused = b * 1e-3;
+    times->alloc = c * 1e-3;
+    times->compress = d * 1e-3;
+}
+
+// Pass 2 of the direct merge path into C (C's row pointer and arrays ready;
+// `stage` the largest number of C entries of one warp's 32 rows).
+template <typename VT>
+void merge_write(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, int stage, cudaStream_t st) {
+    const int64_t n = A.n_rows;
+    // a warp's 32 rows hold at most 32 * kSmallP entries
+    stage = std::max(8, (stage + 7) / 8 * 8);
+    if (stage > 32 * kSmallP) fail(SMAX_ERR_STATE, "SpGEMM merge path: staging size out of range");
+    constexpr int kMaxSmem = kMergeWriteThreads / 32 * 32 * kSmallP * (int)(sizeof(VT) + sizeof(int));
+    static bool attr_set = false;
+    if (!attr_set) {
+        SMAX_CUDA(cudaFuncSetAttribute(gustavson_merge_write<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kMaxSmem));
+        attr_set = true;
+    }
+    const size_t smem = (size_t)kMergeWriteThreads / 32 * stage * (sizeof(VT) + sizeof(int));
+    gustavson_merge_write<VT><<<ceil_div_u(n, kMergeWriteThreads), kMergeWriteThreads, smem, st>>>(
+        n, stage, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), w.masks.as<unsigned long long>(),
+        C.rp(), C.col.as<int>(), C.val.as<VT>());
+    SMAX_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
 template <typename VT>
 void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTimes *times, cudaStream_t st) {
     if (A.n_cols != B.n_rows) fail(SMAX_ERR_BAD_ARG, "A.n_cols must equal B.n_rows");
@@ -558,15 +613,48 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
         }
     } destroy{ev};
     SMAX_CUDA(cudaEventRecord(ev[0], st));
+    // The last apply took the direct merge path: try it first.  Pass 1
+    // checks every row (off_path); only if one fails are the rows classified.
+    if (w.direct_hint && n > 0) {
+        w.counts.ensure(sizeof(int) * (kBins + 3));
+        w.count.ensure(sizeof(int) * n);
+        w.masks.ensure(sizeof(unsigned long long) * n);
+        int *flags = w.counts.as<int>() + kBins;  // b_sorted (unused here), warp_max, off_path
+        SMAX_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * 3, st));
+        SMAX_CUDA(cudaEventRecord(ev[1], st));
+        gustavson_merge<VT, 1><<<ceil_div_u(n, 256), 256, 0, st>>>(
+            nullptr, n, nullptr, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), nullptr, nullptr,
+            w.count.as<int>(), w.masks.as<unsigned long long>(), flags + 1, flags + 2);
+        SMAX_CUDA(cudaGetLastError());
+        SMAX_CUDA(cudaEventRecord(ev[2], st));
+        excl_scan<int>(w.count.as<int>(), C.row_ptr.as<int>(), n, w.scan_tmp, st);
+        int nnz = 0, hf[2] = {0, 0};
+        SMAX_CUDA(cudaMemcpyAsync(&nnz, C.row_ptr.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SMAX_CUDA(cudaMemcpyAsync(hf, flags + 1, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
+        SMAX_CUDA(cudaStreamSynchronize(st));
+        if (hf[1] == 0) {
+            C.nnz = nnz;
+            C.col.ensure(sizeof(int) * (nnz ? nnz : 1));
+            C.val.ensure(sizeof(VT) * (nnz ? nnz : 1));
+            SMAX_CUDA(cudaEventRecord(ev[3], st));
+            merge_write<VT>(A, B, C, w, hf[0], st);
+            SMAX_CUDA(cudaEventRecord(ev[4], st));
+            SMAX_CUDA(cudaStreamSynchronize(st));
+            record_times(ev, times);
+            return;
+        }
+        w.direct_hint = false;  // a row left the merge path: classify them all
+        SMAX_CUDA(cudaEventRecord(ev[0], st));
+    }
     // --- setup: product counts, their offsets, row bins
     w.P.ensure(sizeof(long long) * (n ? n : 1));
     w.Poff.ensure(sizeof(long long) * (n + 1));
     w.lists.ensure(sizeof(int) * kBins * (n ? n : 1));
-    w.counts.ensure(sizeof(int) * (kBins + 2));  // the bin counts, the b_sorted flag, the merge warp maximum
+    w.counts.ensure(sizeof(int) * (kBins + 3));  // the bin counts, then b_sorted, warp_max, off_path
     w.count.ensure(sizeof(int) * (n ? n : 1));
     long long *P = w.P.as<long long>(), *Poff = w.Poff.as<long long>();
-    SMAX_CUDA(cudaMemsetAsync(w.counts.p, 0, sizeof(int) * (kBins + 2), st));
-    int *b_sorted = w.counts.as<int>() + kBins, *warp_max = b_sorted + 1;
+    SMAX_CUDA(cudaMemsetAsync(w.counts.p, 0, sizeof(int) * (kBins + 3), st));
+    int *b_sorted = w.counts.as<int>() + kBins, *warp_max = b_sorted + 1, *off_path = b_sorted + 2;
     const int one = 1;
     SMAX_CUDA(cudaMemcpyAsync(b_sorted, &one, sizeof(int), cudaMemcpyHostToDevice, st));
     if (n > 0) {
@@ -618,11 +706,11 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
         w.masks.ensure(sizeof(unsigned long long) * n);
         gustavson_merge<VT, 1><<<ceil_div_u(n, 256), 256, 0, st>>>(
             nullptr, n, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), nullptr, nullptr, count,
-            w.masks.as<unsigned long long>(), warp_max);
+            w.masks.as<unsigned long long>(), warp_max, off_path);
     } else if (nm > 0) {
         gustavson_merge<VT, 0><<<ceil_div_u(nm, 256), 256, 0, st>>>(
             rm, nm, Poff, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), pcol, pval, count, nullptr,
-            nullptr);
+            nullptr, nullptr);
     }
     if (nw > 0)
         gustavson_warp<VT, kWarpP, kWarpTS, kWarpsPerCta, 32><<<ceil_div_u(nw, kWarpsPerCta), kWarpsPerCta * 32, 0, st>>>(
@@ -665,21 +753,7 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     C.val.ensure(sizeof(VT) * (nnz ? nnz : 1));
     SMAX_CUDA(cudaEventRecord(ev[3], st));
     if (direct) {
-        // a warp's 32 rows hold at most 32 * kSmallP entries
-        stage = std::max(8, (stage + 7) / 8 * 8);
-        if (stage > 32 * kSmallP) fail(SMAX_ERR_STATE, "SpGEMM merge path: staging size out of range");
-        constexpr int kMaxSmem = kMergeWriteThreads / 32 * 32 * kSmallP * (int)(sizeof(VT) + sizeof(int));
-        static bool attr_set[2] = {false, false};
-        if (!attr_set[sizeof(VT) == 8]) {
-            SMAX_CUDA(cudaFuncSetAttribute(gustavson_merge_write<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           kMaxSmem));
-            attr_set[sizeof(VT) == 8] = true;
-        }
-        const size_t smem = (size_t)kMergeWriteThreads / 32 * stage * (sizeof(VT) + sizeof(int));
-        gustavson_merge_write<VT><<<ceil_div_u(n, kMergeWriteThreads), kMergeWriteThreads, smem, st>>>(
-            n, stage, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(),
-            w.masks.as<unsigned long long>(), C.rp(), C.col.as<int>(), C.val.as<VT>());
-        SMAX_CUDA(cudaGetLastError());
+        merge_write<VT>(A, B, C, w, stage, st);
     } else if (n > 0) {
         compact_kernel<VT><<<ceil_div_u((uint64_t)n * kRowGroup, 256), 256, 0, st>>>(C.rp(), Poff, n, pcol, pval,
                                                                               C.col.as<int>(), C.val.as<VT>());
@@ -687,18 +761,8 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     }
     SMAX_CUDA(cudaEventRecord(ev[4], st));
     SMAX_CUDA(cudaStreamSynchronize(st));
-    if (times) {
-        float a = 0, b = 0, c = 0, d = 0;
-        cudaEventElapsedTime(&a, ev[0], ev[1]);
-        cudaEventElapsedTime(&b, ev[1], ev[2]);
-        cudaEventElapsedTime(&c, ev[2], ev[3]);
-        cudaEventElapsedTime(&d, ev[3], ev[4]);
-        times->setup = a * 1e-3;
-        times->fused = b * 1e-3;
-        times->alloc = c * 1e-3;
-        times->compress = d * 1e-3;
-        times->products = total_p;
-    }
+    w.direct_hint = direct;
+    record_times(ev, times);
 }
 
 template void spgemm<double>(const DevCRS &, const DevCRS &, DevCRS &, SpgemmWork &, SpgemmTimes *, cudaStream_t);

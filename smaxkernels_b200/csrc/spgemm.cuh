@@ -7,7 +7,6 @@ namespace smax {
 
 struct SpgemmTimes {
     double setup = 0, fused = 0, alloc = 0, compress = 0;  // seconds, CUDA events
-    long long products = 0;                                // sum over rows of the product counts
 };
 
 // Device workspace of the multiply, kept by the caller across applies: every
@@ -16,7 +15,8 @@ struct SpgemmTimes {
 struct SpgemmWork {
     DevBuf P, Poff, lists, counts, count, pcol, pval, scan_tmp;
     DevBuf wts, wsz, woff, wkeys, wfirst, wvals, wpos;
-    DevBuf masks;  // merge path: each row's first-touch mask
+    DevBuf masks;              // merge path: each row's first-touch mask
+    bool direct_hint = false;  // the last apply took the direct merge path
 };
 
 // C's columns per row are in first-touch order and its values are summed in

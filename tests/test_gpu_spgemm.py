@@ -186,3 +186,45 @@ def test_spgemm_direct_merge_path(case, dtype):
     np.testing.assert_array_equal(crp, orp)
     np.testing.assert_array_equal(ccol, ocol)
     assert normwise(cval, oval) <= tol(dtype)
+
+
+def test_spgemm_direct_hint_falls_back_to_classified_rows():
+    """After an apply on the direct merge path, the kernel object's next apply
+    tries that path first, and its pass 1 checks every row.  Four runs on one
+    kernel object, with operands of unchanged sizes:
+    - B sorted: the direct path;
+    - B's rows shuffled: no row may merge, so the rows are classified again;
+    - B sorted again: the direct path once more;
+    - one row of A given 9 entries: classified again.
+    Every run matches the oracle."""
+    from smaxkernels_b200 import FloatType, Interface, IntType, KernelType, PlatformType
+    rng = np.random.default_rng(126)
+    n = 2000
+    lens = rng.integers(0, 9, n)
+    rows = [rng.choice(n, int(l), replace=False) for l in lens]
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum(lens)
+    A = (rp, np.concatenate(rows).astype(np.int32), rng.uniform(-1, 1, int(lens.sum())))
+    blens = rng.integers(0, 9, n)
+    brp = np.zeros(n + 1, np.int32)
+    brp[1:] = np.cumsum(blens)
+    bcol = np.concatenate([np.sort(rng.choice(n, int(l), replace=False)) for l in blens]).astype(np.int32)
+    B = (brp, bcol, rng.uniform(-1, 1, len(bcol)))
+    A9 = (np.concatenate([[0], np.cumsum(np.where(np.arange(n) == 5, 9, lens))]).astype(np.int32),
+          np.concatenate([rng.choice(n, 9, replace=False) if r == 5 else rows[r] for r in range(n)]).astype(np.int32),
+          None)
+    A9 = (A9[0], A9[1], rng.uniform(-1, 1, len(A9[1])))
+    smax = Interface()
+    smax.register_kernel("g", KernelType.SPGEMM, PlatformType.CUDA, IntType.INT32, FloatType.FLOAT64)
+    k = smax.kernel("g")
+    for a, b in ((A, B), (A, _shuffle_rows(*B, seed=127)), (A, B), (A9, B)):
+        k.register_A(n, n, len(a[1]), a[1], a[0], a[2])
+        k.register_B(n, n, len(b[1]), b[1], b[0], b[2])
+        k.register_C()
+        k.run()
+        _, _, _, crp, ccol, cval = k.result()
+        orp, ocol, oval = O.spgemm(*a, *b, n)
+        np.testing.assert_array_equal(crp, orp)
+        np.testing.assert_array_equal(ccol, ocol)
+        assert normwise(cval, oval) <= 1e-12
+    smax.close()
