@@ -610,15 +610,23 @@ def wl_spgemm(b: Bench):
     products = int(lens[col].sum())  # sum over A's entries of the length of B's row
     a_bytes = 12 * nnz + 4 * (n + 1)
     nbytes = 2 * a_bytes + 2 * a_bytes + 12 * nnz_c + 4 * (n + 1)
+    # the kernel's phase timers (CUDA events): on the direct merge path
+    # Fused_Gustavson is pass 1, Alloc_C the scan of C's counts and the
+    # read-back of nnz(C), Compress the write pass
+    phases = ("Symbolic_Setup", "Fused_Gustavson", "Alloc_C", "Compress")
+    t0 = {nm: k.timer(nm) for nm in phases}
     with b.clocks() as clk:
         t, reps = b.time(k.apply, budget_s=2.0, max_reps=200)
+    calls = reps + 4  # b.time's three warm-up calls and its first timed call
+    phase_ms = {nm: round((k.timer(nm) - t0[nm]) / calls * 1e3, 4) for nm in phases}
     cpu = b.cpu(lambda: b.ref.time_spgemm(rp, col, val, reps=3), nbytes,
                 "3 applies (reference OpenMP symbolic + numeric phases)")
     b.emit("spgemm_f64_laplace3d_96", "SpGEMM GB/s (2A + 2B + C bytes)", nbytes / t / 1e9, "GB/s", t, reps, "f64",
            {"n_rows": n, "nnz_a": nnz, "nnz_c": nnz_c, "products": products,
             "l2": "A, B (77 MB) L2-resident across the fused pass"},
-           clk.summary(), b.hbm(nbytes, t, "gustavson_merge"), cpu, launches=None,
-           gflops=round(2 * products / t / 1e9, 3), reference_gflops_2nnzC=round(2 * nnz_c / t / 1e9, 3))
+           clk.summary(), b.hbm(nbytes, t, "gustavson_merge_write", "spgemm_f64_laplace3d_96"), cpu, launches=None,
+           gflops=round(2 * products / t / 1e9, 3), reference_gflops_2nnzC=round(2 * nnz_c / t / 1e9, 3),
+           phase_ms=phase_ms)
     smax.close()
 
 
