@@ -117,6 +117,7 @@ inline unsigned ceil_div_u(uint64_t a, uint64_t b) { return (unsigned)((a + b - 
 
 // number of SMs of the current device (148 on B200), cached per device
 int sm_count();
+int64_t l2_bytes();  // L2 capacity of the current device
 
 // The legacy default stream (NULL / cudaStreamLegacy) and the per-thread
 // default stream cannot be captured into a CUDA graph.

@@ -45,6 +45,17 @@ int sm_count() {
     return n;
 }
 
+int64_t l2_bytes() {
+    static int cached[64] = {0};
+    int dev = 0;
+    SMAX_CUDA(cudaGetDevice(&dev));
+    if (dev < 64 && cached[dev]) return cached[dev];
+    int n = 0;
+    SMAX_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrL2CacheSize, dev));
+    if (dev < 64) cached[dev] = n;
+    return n;
+}
+
 namespace {
 // One pass over an uploaded CRS matrix: row_ptr[0] == 0, row_ptr[n] == nnz,
 // row_ptr non-decreasing, every column in [0, n_cols).  Hot kernels trust the

@@ -38,13 +38,17 @@ template <typename VT> struct V16;
 template <> struct V16<double> { using T = double2; static constexpr int N = 2; };
 template <> struct V16<float> { using T = float4; static constexpr int N = 4; };
 
-template <typename VT, int VEC>
+// Block values: evict-first (streamed once), or with KEEP the default
+// policy, so that a matrix whose values fit in L2 stays there across products.
+template <typename VT, int VEC, bool KEEP = false>
 __device__ __forceinline__ void load16(const VT *p, VT *o) {
     if constexpr (VEC == 2) {
-        double2 v = __ldcs(reinterpret_cast<const double2 *>(p));
+        const double2 *q = reinterpret_cast<const double2 *>(p);
+        const double2 v = KEEP ? __ldg(q) : __ldcs(q);
         o[0] = v.x; o[1] = v.y;
     } else {
-        float4 v = __ldcs(reinterpret_cast<const float4 *>(p));
+        const float4 *q = reinterpret_cast<const float4 *>(p);
+        const float4 v = KEEP ? __ldg(q) : __ldcs(q);
         o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
     }
 }
@@ -143,7 +147,7 @@ __global__ void __launch_bounds__(256) bcrs_stream_kernel(const int *__restrict_
 // keeps the same VEC in-block positions for the whole row, so the bs sums
 // are complete without shuffles and are folded into the bh outputs through
 // the group's shared-memory tile (fixed order).
-template <typename VT>
+template <typename VT, bool KEEP>
 __global__ void __launch_bounds__(256) bcrs_group_kernel(const int *__restrict__ row_ptr,
                                                          const int *__restrict__ col, const VT *__restrict__ val,
                                                          int64_t n_brows, int bh, int bw, int hpad, int wpad,
@@ -173,8 +177,8 @@ __global__ void __launch_bounds__(256) bcrs_group_kernel(const int *__restrict__
         int j = row_ptr[br];
         for (; j + 1 < b1; j += 2) {
             VT v0[VEC], v1[VEC];
-            load16<VT, VEC>(val + (int64_t)j * bs + o, v0);
-            load16<VT, VEC>(val + (int64_t)(j + 1) * bs + o, v1);
+            load16<VT, VEC, KEEP>(val + (int64_t)j * bs + o, v0);
+            load16<VT, VEC, KEEP>(val + (int64_t)(j + 1) * bs + o, v1);
             const int64_t c0 = (int64_t)col[j] * wpad, c1 = (int64_t)col[j + 1] * wpad;
             VT x0[VEC], x1[VEC];
 #pragma unroll
@@ -191,7 +195,7 @@ __global__ void __launch_bounds__(256) bcrs_group_kernel(const int *__restrict__
         }
         if (j < b1) {
             VT v[VEC];
-            load16<VT, VEC>(val + (int64_t)j * bs + o, v);
+            load16<VT, VEC, KEEP>(val + (int64_t)j * bs + o, v);
             const int64_t c = (int64_t)col[j] * wpad;
 #pragma unroll
             for (int i = 0; i < VEC; ++i)
@@ -304,8 +308,17 @@ void bcrs_spmv(const DevBCRS &m, const VT *x, VT *y, cudaStream_t st) {
         const double steps = (double)m.n_blocks * (double)(m.hpad * m.wpad) /
                              ((double)m.n_rows * 32.0 * (16.0 / sizeof(VT)));
         const int64_t group = m.hpad * m.wpad / (16 / (int64_t)sizeof(VT));
-        if (steps < 2.0)
-            bcrs_group_kernel<VT><<<ceil_div_u((uint64_t)m.n_rows * group, 256), 256, 0, st>>>(
+        // values that fit in half of L2 are loaded with the default policy and
+        // stay resident across repeated products (4x4 blocks of the 7-point
+        // 64^3 Laplacian, 59 MB of values, in a loop of products: see the
+        // BCRS notes); larger ones stream evict-first
+        const bool keep = (double)m.n_blocks * (double)(m.hpad * m.wpad) * sizeof(VT) <= 0.5 * (double)l2_bytes();
+        if (steps < 2.0 && keep)
+            bcrs_group_kernel<VT, true><<<ceil_div_u((uint64_t)m.n_rows * group, 256), 256, 0, st>>>(
+                m.row_ptr.as<int>(), m.col.as<int>(), m.val.as<VT>(), m.n_rows, (int)m.bh, (int)m.bw, (int)m.hpad,
+                (int)m.wpad, m.col_major ? 1 : 0, x, y);
+        else if (steps < 2.0)
+            bcrs_group_kernel<VT, false><<<ceil_div_u((uint64_t)m.n_rows * group, 256), 256, 0, st>>>(
                 m.row_ptr.as<int>(), m.col.as<int>(), m.val.as<VT>(), m.n_rows, (int)m.bh, (int)m.bw, (int)m.hpad,
                 (int)m.wpad, m.col_major ? 1 : 0, x, y);
         else if (steps >= 3.0)
