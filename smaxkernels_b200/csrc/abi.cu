@@ -352,7 +352,11 @@ uint64_t out_count(const smax_kernel_s *k) {
 // CRS SpMV with the warp-stream kernel in host mode, large enough that the
 // kernel time is worth hiding under the download of y: builds (once per
 // upload) row blocks starting at entries that are multiples of 4 (the
-// kernel's 16-byte loads), each with its own plan over the shared device copy
+// kernel's 16-byte loads), each with its own plan over the shared device copy.
+// Block b holds about 2^b / (2^B - 1) of the entries: the first block is small,
+// so y's download starts early, and each block computes in about the time
+// the previous block's y takes to download (the kernel produces y about
+// twice as fast as the host link takes it), so the link stays busy.
 bool pipe_ready(smax_kernel_s *k) {
     if (k->ktype != SMAX_KERNEL_SPMV || k->f_scs || k->f_bcrs || k->spmv_variant == 2) return false;
     if (k->pipe_blocks < 2 || k->dA.n_rows < (1 << 18)) return false;
@@ -371,8 +375,10 @@ bool pipe_ready(smax_kernel_s *k) {
     const int64_t n = k->dA.n_rows, nnz = k->dA.nnz;
     const int *rp = static_cast<const int *>(k->A.row_ptr);  // the registered host row pointer
     std::vector<int64_t> r0{0}, e0{0};
-    for (int b = 1; b < k->pipe_blocks; ++b) {
-        const int64_t target = nnz * b / k->pipe_blocks;
+    const int nbk = std::min(k->pipe_blocks, 16);
+    const double whole = (double)((1ll << nbk) - 1);
+    for (int b = 1; b < nbk; ++b) {
+        const int64_t target = (int64_t)((double)nnz * (double)((1ll << b) - 1) / whole);
         int64_t r = std::lower_bound(rp, rp + n + 1, (int)target) - rp;
         int64_t limit = std::min<int64_t>(n, r + 4096);
         while (r < limit && (rp[r] % 4) != 0) ++r;
@@ -415,7 +421,10 @@ void apply_pipelined(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
     else apply_pipe_t<float>(k, static_cast<const float *>(b), static_cast<float *>(c), c_off);
 }
 
-void do_initialize(smax_kernel_s *k) {
+// wait: return only when x (and b) are on the device, as the reference's
+// initialize does; run() does not wait, since its apply is ordered after the
+// copies on the same stream and its finalize waits for the results
+void do_initialize(smax_kernel_s *k, bool wait = true) {
     double t0 = wall_s();
     if (k->ktype == SMAX_KERNEL_SPGEMM) {
         require(k->Cref.set, SMAX_ERR_STATE, "register_C before initialize");
@@ -452,7 +461,7 @@ void do_initialize(smax_kernel_s *k) {
             SMAX_CUDA(cudaMemcpyAsync(k->dC.p, k->C.val, cb, cudaMemcpyHostToDevice, k->stream));
         if (bb) SMAX_CUDA(cudaMemcpyAsync(k->dB.p, k->B.val, bb, cudaMemcpyHostToDevice, k->stream));
     }
-    SMAX_CUDA(cudaStreamSynchronize(k->stream));
+    if (wait) SMAX_CUDA(cudaStreamSynchronize(k->stream));
     k->timers["initialize"] += wall_s() - t0;
 }
 
@@ -794,7 +803,7 @@ smax_status smax_kernel_run(smax_kernel k, uint64_t A_offset, uint64_t B_offset,
     (void)A_offset;
     return guarded([&] {
         smax_kernel_s *kk = K(k);
-        do_initialize(kk);
+        do_initialize(kk, false);
         do_apply(kk, B_offset, C_offset);
         do_finalize(kk);
     });

@@ -199,7 +199,7 @@ struct smax_kernel_s {
         std::vector<smax::DevBuf> rps;         // rebased row pointers
         int blocks() const { return (int)plans.size(); }
     } pipe;
-    int pipe_blocks = 4;                        // SMAX_FLAG_SPMV_PIPELINE (0: off)
+    int pipe_blocks = 6;                        // SMAX_FLAG_SPMV_PIPELINE (0: off)
 
     // stopwatches
     std::map<std::string, double> timers;

@@ -232,7 +232,8 @@ class Kernel:
 
     def set_spmv_pipeline(self, blocks: int):
         """CRS SpMV with host operands: row blocks whose part of y is downloaded
-        while later blocks compute (default 4; 0 or 1: off)."""
+        while later blocks compute; block b holds 2^b / (2^B - 1) of the entries
+        (default 6, at most 16 used; 0 or 1: off)."""
         return self._flag("spmv_pipeline", blocks)
 
     def set_solve_mode(self, mode: int):

@@ -24,18 +24,22 @@ def _spmv_kernel(vt, pipeline=None):
 
 
 @pytest.mark.parametrize("vt", [np.float64, np.float32])
-@pytest.mark.parametrize("pipeline", [0, 4, 7])
+@pytest.mark.parametrize("pipeline", [0, 4, 7, 16, None])
 def test_pipelined_spmv_matches_oracle(vt, pipeline):
+    """Geometric row blocks (None: the default count); x changes between
+    runs, which upload it without waiting before the apply."""
     n = 300_000
     rp, col, val = rand_crs(n, 12, 77, vt=vt, empty_frac=0.05, long_rows=(40000, 9000, 5000))
-    x = np.random.default_rng(78).uniform(-1, 1, n).astype(vt)
-    y_ref = O.spmv_crs(rp, col, val, x)
+    rng = np.random.default_rng(78)
+    x = rng.uniform(-1, 1, n).astype(vt)
     smax, k = _spmv_kernel(vt, pipeline)
     y = np.zeros(n, vt)
     k.register_A(n, n, len(col), col, rp, val)
     k.register_B(n, x)
     k.register_C(n, y)
     for _ in range(3):  # plans built on the first apply, reused after
+        x[:] = rng.uniform(-1, 1, n).astype(vt)
+        y_ref = O.spmv_crs(rp, col, val, x)
         y[:] = 7.0
         k.run()
         assert normwise(y, y_ref) <= tol(vt)
