@@ -216,25 +216,31 @@ def test_spmm_config2_vs_reference(vt, k_):
 
 # ---------------------------------------------------------------- SpGEMM ----
 @pytest.mark.slow
-def test_spgemm_config2_vs_reference():
-    from smaxkernels_b200 import FloatType, IntType, KernelType, PlatformType
+@pytest.mark.parametrize("vt", [np.float64, np.float32])
+def test_spgemm_config2_vs_reference(vt):
+    """Two runs on one kernel object: the first classifies the rows, the
+    second takes the direct merge path at once.  Both equal the reference."""
+    from smaxkernels_b200 import IntType, KernelType, PlatformType
     M = _M()
-    rp, col, val = M.laplace3d_7pt(96)
+    rp, col, val64 = M.laplace3d_7pt(96)
+    val = val64.astype(vt)
     n = len(rp) - 1
+    orp, ocol, oval, onr, onc = R().spgemm(rp, col, val, rp, col, val, n, n)
+    ref64 = R().spgemm(rp, col, val64, rp, col, val64, n, n)[2] if vt == np.float32 else None
     smax = _iface()
-    smax.register_kernel("g", KernelType.SPGEMM, PlatformType.CUDA, IntType.INT32, FloatType.FLOAT64)
+    smax.register_kernel("g", KernelType.SPGEMM, PlatformType.CUDA, IntType.INT32, _ft(vt))
     k = smax.kernel("g")
     k.register_A(n, n, len(col), col, rp, val)
     k.register_B(n, n, len(col), col, rp, val)
-    k.register_C()
-    k.run()
-    n_rows, n_cols, nnz, crp, ccol, cval = k.result()
+    for run in range(2):
+        k.register_C()
+        k.run()
+        n_rows, n_cols, nnz, crp, ccol, cval = k.result()
+        assert (n_rows, n_cols, nnz) == (onr, onc, len(ocol)) and nnz == 21_732_480
+        np.testing.assert_array_equal(crp, orp)
+        np.testing.assert_array_equal(ccol, ocol)  # first-touch order inside every row
+        _check_fp(cval, oval, vt, ref64, f"SpGEMM values, run {run}")
     smax.close()
-    orp, ocol, oval, onr, onc = R().spgemm(rp, col, val, rp, col, val, n, n)
-    assert (n_rows, n_cols, nnz) == (onr, onc, len(ocol)) and nnz == 21_732_480
-    np.testing.assert_array_equal(crp, orp)
-    np.testing.assert_array_equal(ccol, ocol)  # first-touch order inside every row
-    _check_fp(cval, oval, np.float64, None, "SpGEMM values")
 
 
 # ------------------------------------------------------ SpTRSV / SpTRSM ----
