@@ -466,13 +466,22 @@ def wl_spmv_laplace64(b: Bench):
     with b.clocks() as clk:
         t_fl, reps = b.time(k.apply, flush=True, budget_s=1.0, max_reps=200)
         t_hot, _ = b.time(k.apply)
+        # the same without the per-apply CUDA-event stopwatch (SMAX_FLAG_TIMERS
+        # = 0): at this size the event pair is a third of an apply
+        k.set_timers(False)
+        t_fl_off, _ = b.time(k.apply, flush=True, budget_s=1.0, max_reps=200)
+        t_hot_off, _ = b.time(k.apply)
+        k.set_timers(True)
     cpu = b.cpu(lambda: b.ref.time_spmv_crs(rp, col, val, x, warm=3, reps=100)[0], nbytes,
                 "100 applies after 3 warm-ups (reference OpenMP CRS kernel)")
     b.emit("crs_spmv_f64_laplace3d_64", "CRS SpMV GB/s (L2-flushed)", nbytes / t_fl / 1e9, "GB/s", t_fl, reps,
            "f64", {"n_rows": n, "nnz": nnz, "l2": "flushed (256 MB write) before every timed launch"},
-           clk.summary(), b.hbm(nbytes, t_fl, "crs_stream_kernel"), cpu, launches=2 * reps,
+           clk.summary(), b.hbm(nbytes, t_fl, "crs_stream_kernel"), cpu, launches=reps,
            hot={"value": round(nbytes / t_hot / 1e9, 3), "ms_per_step": round(t_hot * 1e3, 5),
-                "l2": "hot (repeated launches, matrix L2-resident)"})
+                "l2": "hot (repeated launches, matrix L2-resident)"},
+           timers_off={"value": round(nbytes / t_fl_off / 1e9, 3), "ms_per_step": round(t_fl_off * 1e3, 5),
+                       "hot_value": round(nbytes / t_hot_off / 1e9, 3),
+                       "hot_ms_per_step": round(t_hot_off * 1e3, 5)})
     smax.close()
 
 
@@ -1044,11 +1053,23 @@ def wl_cusparse(b: Bench):
         return torch.sparse_csr_tensor(b.dev(rp.astype(np.int32)), b.dev(col.astype(np.int32)), b.dev(val),
                                        size=(len(rp) - 1, n_cols))
 
+    def ours(k, **kw):
+        """This platform's time per apply with its default stopwatches (a
+        CUDA-event pair per apply), then with them off (SMAX_FLAG_TIMERS = 0),
+        as torch.sparse records none."""
+        t_on, _ = b.time(k.apply, **kw)
+        k.set_timers(False)
+        t_off, _ = b.time(k.apply, **kw)
+        k.set_timers(True)
+        return t_on, t_off
+
     def line(name, what, nbytes, t_lib, t_ours, reps, config, clk, kern_lib, extra=None):
+        t_on, t_off = t_ours
         b.emit(name, f"cuSPARSE {what} GB/s (through torch.sparse)", nbytes / t_lib / 1e9, "GB/s", t_lib, reps,
                "f64", config, clk, b.hbm(nbytes, t_lib, kern_lib), None,
-               ours_ms=round(t_ours * 1e3, 5), cusparse_ms=round(t_lib * 1e3, 5),
-               ours_over_cusparse=round(t_lib / t_ours, 3), **(extra or {}))
+               ours_ms=round(t_on * 1e3, 5), cusparse_ms=round(t_lib * 1e3, 5),
+               ours_over_cusparse=round(t_lib / t_on, 3), ours_ms_timers_off=round(t_off * 1e3, 5),
+               ours_over_cusparse_timers_off=round(t_lib / t_off, 3), **(extra or {}))
 
     # CSR SpMV: the headline matrix and the 7-point 64^3 Laplacian
     for name, (rp, col, val), x in (
@@ -1067,7 +1088,7 @@ def wl_cusparse(b: Bench):
         k.initialize()
         with b.clocks() as clk:
             t_lib, reps = b.time(lambda: torch.mv(A, xd, out=yd))
-            t_ours, _ = b.time(k.apply)
+            t_ours = ours(k)
         err = float(torch.linalg.norm(yd - y2) / torch.linalg.norm(y2))
         line(f"cusparse_csr_spmv_f64_{name}", "CSR SpMV", crs_bytes(n, nnz, n, 8), t_lib, t_ours, reps,
              {"n_rows": n, "nnz": nnz, "library_call": "torch.mv(sparse_csr, x)"}, clk.summary(),
@@ -1093,7 +1114,7 @@ def wl_cusparse(b: Bench):
     X2 = X.view(n, kv)
     with b.clocks() as clk:
         t_lib, reps = b.time(lambda: torch.mm(A, X2, out=Y))
-        t_ours, _ = b.time(k.apply)
+        t_ours = ours(k)
     err = float(torch.linalg.norm(Y.reshape(-1) - Y2) / torch.linalg.norm(Y2))
     line("cusparse_csr_spmm_k16_f64_stencil27_128", "CSR SpMM", (8 + 4) * nnz + 4 * (n + 1) + 2 * 8 * n * kv,
          t_lib, t_ours, reps, {"n_rows": n, "nnz": nnz, "k": kv, "library_call": "torch.mm(sparse_csr, X)"},
@@ -1119,7 +1140,7 @@ def wl_cusparse(b: Bench):
     nbytes = 4 * a_bytes + 12 * nnz_c + 4 * (n + 1)
     with b.clocks() as clk:
         t_lib, reps = b.time(lambda: torch.mm(A, A), budget_s=2.0, max_reps=100)
-        t_ours, _ = b.time(k.apply, budget_s=2.0, max_reps=100)
+        t_ours = ours(k, budget_s=2.0, max_reps=100)
     C = torch.mm(A, A)
     line("cusparse_spgemm_f64_laplace3d_96", "SpGEMM", nbytes, t_lib, t_ours, reps,
          {"n_rows": n, "nnz_a": nnz, "nnz_c": nnz_c, "library_call": "torch.mm(sparse_csr, sparse_csr)"},
@@ -1146,7 +1167,7 @@ def wl_cusparse(b: Bench):
                                      size=(n, n))
         with b.clocks() as clk:
             t_lib, reps = b.time(lambda: torch.mv(Ab, xd, out=yd))
-            t_ours, _ = b.time(k.apply)
+            t_ours = ours(k)
         err = float(torch.linalg.norm(yd - y2) / torch.linalg.norm(y2))
         line("cusparse_bsr4x4_spmv_f64_laplace3d_64", "BSR SpMV", (16 * 8 + 4) * nb + 4 * (n // 4 + 1) + 16 * n,
              t_lib, t_ours, reps, {"n_rows": n, "n_blocks": nb, "library_call": "torch.mv(sparse_bsr, x)"},

@@ -99,6 +99,7 @@ typedef int smax_status;
 #define SMAX_FLAG_REFINE_TOL 16        /* stop refining once max|dx| <= 10^-value * max|x| (host check per step; 0: run all) */
 #define SMAX_FLAG_SWEEP_CLUSTER 17     /* SpTRSV: runs with levels wider than 1024 rows on a thread-block cluster (0: one CTA) */
 #define SMAX_FLAG_SPMV_PIPELINE 18     /* CRS SpMV with host pointers: B row blocks, block b with 2^b/(2^B-1) of the entries, whose y is downloaded while later blocks compute (default 6, at most 16 used; 0/1: off) */
+#define SMAX_FLAG_TIMERS 19            /* 1 (default): time every apply with a pair of CUDA events (timer "apply", SpGEMM's phases); 0: no events, those timers stay 0.  A timing event between launches costs about 2.5 us of device time */
 
 /* SpTRSV / SpTRSM launch schemes (SMAX_FLAG_SOLVE_MODE) */
 #define SMAX_SOLVE_AUTO 0        /* the default: SMAX_SOLVE_SYNCFREE for one right-hand side and few wide

@@ -137,6 +137,7 @@ class Kernel {
     int set_level_merge(int rows) { return flag(SMAX_FLAG_LEVEL_MERGE, rows); }
     int set_sweep_cluster(bool v) { return flag(SMAX_FLAG_SWEEP_CLUSTER, v); }
     int set_spmv_pipeline(int blocks) { return flag(SMAX_FLAG_SPMV_PIPELINE, blocks); }
+    int set_timers(bool on) { return flag(SMAX_FLAG_TIMERS, on ? 1 : 0); }
     int set_spin_limit(int kilo_polls) { return flag(SMAX_FLAG_SPIN_LIMIT, kilo_polls); }
     int set_refine(int steps, int tol_exp = 0) {
         return flag(SMAX_FLAG_REFINE, steps) || flag(SMAX_FLAG_REFINE_TOL, tol_exp);

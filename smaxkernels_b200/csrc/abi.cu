@@ -5,6 +5,7 @@
 // spmm.hpp:68-100): the kernel type and the flags pick the format and kernel.
 #include <algorithm>
 #include <cstring>
+#include <optional>
 
 #include "abi_internal.cuh"
 #include "sptrsv_batch.cuh"
@@ -465,35 +466,50 @@ void do_initialize(smax_kernel_s *k, bool wait = true) {
     k->timers["initialize"] += wall_s() - t0;
 }
 
+// The "apply" stopwatch: a pair of CUDA events around one apply, unless the
+// kernel's timers are off (SMAX_FLAG_TIMERS).
+struct ApplyStopwatch {
+    std::optional<EventInterval> iv;
+    explicit ApplyStopwatch(smax_kernel_s *k) {
+        if (!k->timers_on) return;
+        k->timers["apply"] += k->apply_events.trim(512);
+        iv.emplace(k->apply_events, k->stream);
+    }
+    void close() {
+        if (iv) iv->close();
+    }
+};
+
 void do_apply(smax_kernel_s *k, uint64_t b_off, uint64_t c_off) {
     require(!k->a_dirty, SMAX_ERR_STATE, "initialize before apply");
     if (k->ktype == SMAX_KERNEL_SPGEMM) {
         // offsets are ignored, as in the reference (src/kernels/spgemm.hpp:108-130)
-        k->timers["apply"] += k->apply_events.trim(512);
-        EventInterval iv(k->apply_events, k->stream);
-        if (k->vbytes == 8) spgemm<double>(k->dA, k->dBm, k->dCm, k->spgemm_work, &k->spgemm_times, k->stream);
-        else spgemm<float>(k->dA, k->dBm, k->dCm, k->spgemm_work, &k->spgemm_times, k->stream);
-        iv.close();
-        const SpgemmTimes &t = k->spgemm_times;
-        k->timers["Symbolic_Setup"] += t.setup;
-        k->timers["Fused_Gustavson"] += t.fused;
-        k->timers["Alloc_C"] += t.alloc;
-        k->timers["Compress"] += t.compress;
-        k->timers["symbolic_phase"] += t.setup + t.alloc;
-        k->timers["numerical_phase"] += t.fused + t.compress;
+        ApplyStopwatch sw(k);
+        SpgemmTimes *times = k->timers_on ? &k->spgemm_times : nullptr;
+        if (k->vbytes == 8) spgemm<double>(k->dA, k->dBm, k->dCm, k->spgemm_work, times, k->stream);
+        else spgemm<float>(k->dA, k->dBm, k->dCm, k->spgemm_work, times, k->stream);
+        sw.close();
+        if (times) {
+            const SpgemmTimes &t = *times;
+            k->timers["Symbolic_Setup"] += t.setup;
+            k->timers["Fused_Gustavson"] += t.fused;
+            k->timers["Alloc_C"] += t.alloc;
+            k->timers["Compress"] += t.compress;
+            k->timers["symbolic_phase"] += t.setup + t.alloc;
+            k->timers["numerical_phase"] += t.fused + t.compress;
+        }
         k->spgemm_done = true;
         return;
     }
     check_extents(k, b_off, c_off);
-    k->timers["apply"] += k->apply_events.trim(512);
-    EventInterval iv(k->apply_events, k->stream);
+    ApplyStopwatch sw(k);
     if (!k->f_device && pipe_ready(k)) {
         apply_pipelined(k, b_off, c_off);  // records one output range per row block
     } else {
         apply_core(k, b_off, c_off);
         if (!k->f_device) record_out(k, out_offset(k, b_off, c_off), out_count(k));
     }
-    iv.close();
+    sw.close();
 }
 
 }  // namespace
@@ -705,6 +721,7 @@ smax_status smax_kernel_set_flag(smax_kernel k, int flag, int value) {
             kk->refine_tol = value;
             break;
         case SMAX_FLAG_SWEEP_CLUSTER: kk->sweep_cluster = v; break;
+        case SMAX_FLAG_TIMERS: kk->timers_on = v; break;
         case SMAX_FLAG_SPMV_PIPELINE:
             require(value >= 0 && value <= 64, SMAX_ERR_BAD_ARG, "pipeline blocks must be in [0, 64]");
             kk->pipe_blocks = value;

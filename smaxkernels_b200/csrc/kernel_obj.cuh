@@ -177,6 +177,7 @@ struct smax_kernel_s {
     // FP32 solve + FP64 residual refinement (refine.cu); 0 steps = off
     int refine_steps = 0, refine_tol = 0;
     bool sweep_cluster = false;     // allow cluster runs in the level-pack solves
+    bool timers_on = true;          // SMAX_FLAG_TIMERS: CUDA-event stopwatches around every apply
     smax::RefineState refine;
 
     // host-pointer mode: output ranges written by apply() since the last

@@ -604,15 +604,23 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     C.n_rows = n;
     C.n_cols = B.n_cols;
     C.row_ptr.ensure(sizeof(int) * (n + 1));
-    cudaEvent_t ev[5];
-    for (auto &e : ev) SMAX_CUDA(cudaEventCreate(&e));
-    struct Destroy {
-        cudaEvent_t *ev;
-        ~Destroy() {
-            for (int i = 0; i < 5; ++i) cudaEventDestroy(ev[i]);
+    // phase boundaries for the timers, only when they are wanted
+    struct PhaseEvents {
+        cudaEvent_t ev[5] = {};
+        explicit PhaseEvents(bool on) {
+            if (on)
+                for (auto &e : ev) SMAX_CUDA(cudaEventCreate(&e));
         }
-    } destroy{ev};
-    SMAX_CUDA(cudaEventRecord(ev[0], st));
+        void mark(int i, cudaStream_t s) {
+            if (ev[i]) SMAX_CUDA(cudaEventRecord(ev[i], s));
+        }
+        ~PhaseEvents() {
+            for (auto &e : ev)
+                if (e) cudaEventDestroy(e);
+        }
+    } pe(times != nullptr);
+    cudaEvent_t *ev = pe.ev;
+    pe.mark(0, st);
     // The last apply took the direct merge path: try it first.  Pass 1
     // checks every row (off_path); only if one fails are the rows classified.
     if (w.direct_hint && n > 0) {
@@ -621,12 +629,12 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
         w.masks.ensure(sizeof(unsigned long long) * n);
         int *flags = w.counts.as<int>() + kBins;  // b_sorted (unused here), warp_max, off_path
         SMAX_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * 3, st));
-        SMAX_CUDA(cudaEventRecord(ev[1], st));
+        pe.mark(1, st);
         gustavson_merge<VT, 1><<<ceil_div_u(n, 256), 256, 0, st>>>(
             nullptr, n, nullptr, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), nullptr, nullptr,
             w.count.as<int>(), w.masks.as<unsigned long long>(), flags + 1, flags + 2);
         SMAX_CUDA(cudaGetLastError());
-        SMAX_CUDA(cudaEventRecord(ev[2], st));
+        pe.mark(2, st);
         excl_scan<int>(w.count.as<int>(), C.row_ptr.as<int>(), n, w.scan_tmp, st);
         int nnz = 0, hf[2] = {0, 0};
         SMAX_CUDA(cudaMemcpyAsync(&nnz, C.row_ptr.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -636,15 +644,15 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
             C.nnz = nnz;
             C.col.ensure(sizeof(int) * (nnz ? nnz : 1));
             C.val.ensure(sizeof(VT) * (nnz ? nnz : 1));
-            SMAX_CUDA(cudaEventRecord(ev[3], st));
+            pe.mark(3, st);
             merge_write<VT>(A, B, C, w, hf[0], st);
-            SMAX_CUDA(cudaEventRecord(ev[4], st));
+            pe.mark(4, st);
             SMAX_CUDA(cudaStreamSynchronize(st));
             record_times(ev, times);
             return;
         }
         w.direct_hint = false;  // a row left the merge path: classify them all
-        SMAX_CUDA(cudaEventRecord(ev[0], st));
+        pe.mark(0, st);
     }
     // --- setup: product counts, their offsets, row bins
     w.P.ensure(sizeof(long long) * (n ? n : 1));
@@ -676,7 +684,7 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     const long long total_p = h.total_p;
     const int ns = h.counts[0], nw = h.counts[1], nc = h.counts[2], ng = h.counts[3], nm = h.counts[4];
     const int *rs = w.lists.as<int>(), *rw = rs + n, *rc = rs + 2 * n, *rg = rs + 3 * n, *rm = rs + 4 * n;
-    SMAX_CUDA(cudaEventRecord(ev[1], st));
+    pe.mark(1, st);
     // --- fused Gustavson pass into product-offset (padded) buffers
     if (nm != n || n == 0) {  // the direct merge path writes C itself
         w.pcol.ensure(sizeof(int) * (total_p ? total_p : 1));
@@ -741,7 +749,7 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
                                                          w.wfirst.as<int>(), w.wvals.as<VT>(), w.wpos.as<int>());
     }
     SMAX_CUDA(cudaGetLastError());
-    SMAX_CUDA(cudaEventRecord(ev[2], st));
+    pe.mark(2, st);
     // --- C's row pointer and arrays
     excl_scan<int>(count, C.row_ptr.as<int>(), n, w.scan_tmp, st);
     int nnz = 0, stage = 0;
@@ -751,7 +759,7 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
     C.nnz = nnz;
     C.col.ensure(sizeof(int) * (nnz ? nnz : 1));
     C.val.ensure(sizeof(VT) * (nnz ? nnz : 1));
-    SMAX_CUDA(cudaEventRecord(ev[3], st));
+    pe.mark(3, st);
     if (direct) {
         merge_write<VT>(A, B, C, w, stage, st);
     } else if (n > 0) {
@@ -759,7 +767,7 @@ void spgemm(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, SpgemmTi
                                                                               C.col.as<int>(), C.val.as<VT>());
         SMAX_CUDA(cudaGetLastError());
     }
-    SMAX_CUDA(cudaEventRecord(ev[4], st));
+    pe.mark(4, st);
     SMAX_CUDA(cudaStreamSynchronize(st));
     w.direct_hint = direct;
     record_times(ev, times);

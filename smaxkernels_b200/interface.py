@@ -65,7 +65,7 @@ class SpMVType(enum.IntEnum):
 FLAG = dict(mat_perm=0, mat_upper_triang=1, mat_lower_triang=2, vec_row_major=3, mat_scs=4, mat_bcrs=5,
             block_column_major=6, kernel_impl=7, device_pointers=8, a_dirty=9,
             spmv_variant=10, solve_mode=11, level_merge=12, spin_limit=13, test_force_timeout=14,
-            refine=15, refine_tol=16, sweep_cluster=17, spmv_pipeline=18)
+            refine=15, refine_tol=16, sweep_cluster=17, spmv_pipeline=18, timers=19)
 
 SOLVE_AUTO, SOLVE_PER_LEVEL, SOLVE_MERGED, SOLVE_GRAPH, SOLVE_PERSISTENT, SOLVE_SYNCFREE = 0, 1, 2, 3, 4, 5
 
@@ -229,6 +229,13 @@ class Kernel:
         """CRS SpMV kernel: 0 auto, 1 warp-stream, 2 row-tile.  Row-major SpMM:
         0 auto, 1 a grid of all rows, 2 one CTA per SM walking a row range."""
         return self._flag("spmv_variant", v)
+
+    def set_timers(self, on: bool):
+        """CUDA-event stopwatches around every apply (the "apply" timer and
+        SpGEMM's phases; default on).  Off, applies record no events: a
+        timing event between launches costs about 2.5 us of device time,
+        which matters for small matrices in a loop."""
+        return self._flag("timers", int(bool(on)))
 
     def set_spmv_pipeline(self, blocks: int):
         """CRS SpMV with host operands: row blocks whose part of y is downloaded

@@ -96,3 +96,11 @@ def test_ctx_set_levels_validates_and_stores():
     assert _lib.lib.smax_ctx_set_levels(ctx, 1, bad0) == _lib.ERR_BAD_ARG
     assert _lib.lib.smax_ctx_get_n_levels(ctx) == 3  # unchanged by the rejected calls
     assert _lib.lib.smax_ctx_destroy(ctx) == 0
+
+
+def test_python_flag_table_matches_header():
+    """interface.FLAG names every SMAX_FLAG_* of the header with its value."""
+    from smaxkernels_b200.interface import FLAG
+    src = open(os.path.join(REPO, "include", "smax_b200.h")).read()
+    header = {m.group(1).lower(): int(m.group(2)) for m in re.finditer(r"#define SMAX_FLAG_(\w+) (\d+)", src)}
+    assert header == FLAG

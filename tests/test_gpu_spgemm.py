@@ -228,3 +228,28 @@ def test_spgemm_direct_hint_falls_back_to_classified_rows():
         np.testing.assert_array_equal(ccol, ocol)
         assert normwise(cval, oval) <= 1e-12
     smax.close()
+
+
+def test_spgemm_timers_off():
+    """With the timers off SpGEMM records no phase events: its phase timers
+    stay 0 and C is unchanged."""
+    from smaxkernels_b200 import FloatType, Interface, IntType, KernelType, PlatformType
+    A = rand_crs(1500, 8, 128)
+    smax = Interface()
+    smax.register_kernel("g", KernelType.SPGEMM, PlatformType.CUDA, IntType.INT32, FloatType.FLOAT64)
+    k = smax.kernel("g")
+    k.set_timers(False)
+    rp, col, val = A
+    k.register_A(1500, 1500, len(col), col, rp, val)
+    k.register_B(1500, 1500, len(col), col, rp, val)
+    for _ in range(2):
+        k.register_C()
+        k.run()
+        _, _, _, crp, ccol, cval = k.result()
+        orp, ocol, oval = O.spgemm(*A, *A, 1500)
+        np.testing.assert_array_equal(crp, orp)
+        np.testing.assert_array_equal(ccol, ocol)
+        assert normwise(cval, oval) <= 1e-12
+    for name in ("apply", "Symbolic_Setup", "Fused_Gustavson", "Alloc_C", "Compress"):
+        assert k.timer(name) == 0.0, name
+    smax.close()

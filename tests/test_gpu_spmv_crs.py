@@ -175,3 +175,29 @@ def test_operand_too_small_is_rejected():
     with pytest.raises(SmaxError):
         k.run()
     smax.close()
+
+
+def test_timers_off_records_no_apply_time():
+    """SMAX_FLAG_TIMERS = 0: applies record no CUDA events and the apply
+    timer stays 0; the results are unchanged.  Switched back on, the timer
+    counts again."""
+    from smaxkernels_b200 import FloatType, Interface, IntType, KernelType, PlatformType
+    rp, col, val = rand_crs(3000, 20, 6)
+    n = 3000
+    x = np.random.default_rng(2).uniform(-1, 1, n)
+    y = np.zeros(n)
+    smax = Interface()
+    smax.register_kernel("k", KernelType.SPMV, PlatformType.CUDA, IntType.INT32, FloatType.FLOAT64)
+    k = smax.kernel("k")
+    k.set_timers(False)
+    k.register_A(n, n, len(col), col, rp, val)
+    k.register_B(n, x)
+    k.register_C(n, y)
+    for _ in range(3):
+        k.run()
+    assert normwise(y, O.spmv_crs(rp, col, val, x)) <= 1e-12
+    assert k.timer("apply") == 0.0
+    k.set_timers(True)
+    k.run()
+    assert k.timer("apply") > 0
+    smax.close()
