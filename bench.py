@@ -476,7 +476,7 @@ def wl_spmv_laplace64(b: Bench):
                 "100 applies after 3 warm-ups (reference OpenMP CRS kernel)")
     b.emit("crs_spmv_f64_laplace3d_64", "CRS SpMV GB/s (L2-flushed)", nbytes / t_fl / 1e9, "GB/s", t_fl, reps,
            "f64", {"n_rows": n, "nnz": nnz, "l2": "flushed (256 MB write) before every timed launch"},
-           clk.summary(), b.hbm(nbytes, t_fl, "crs_stream_kernel"), cpu, launches=reps,
+           clk.summary(), b.hbm(nbytes, t_fl, "crs_stream_kernel", "crs_spmv_f64_laplace3d_64"), cpu, launches=reps,
            hot={"value": round(nbytes / t_hot / 1e9, 3), "ms_per_step": round(t_hot * 1e3, 5),
                 "l2": "hot (repeated launches, matrix L2-resident)"},
            timers_off={"value": round(nbytes / t_fl_off / 1e9, 3), "ms_per_step": round(t_fl_off * 1e3, 5),
