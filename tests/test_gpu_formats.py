@@ -266,11 +266,14 @@ def test_bcrs_long_block_rows_vs_oracle(vt, shape, col_major):
 
 @pytest.mark.parametrize("vt", [np.float64, np.float32])
 @pytest.mark.parametrize("col_major", [False, True])
-def test_bcrs_short_block_rows_laplace(vt, col_major):
-    """The 7-point 32^3 Laplacian in 4x4 blocks: under two warp steps per block
-    row, so a lane group per block row (odd and even block counts per row)."""
+@pytest.mark.parametrize("side", [32, 96])
+def test_bcrs_short_block_rows_laplace(vt, col_major, side):
+    """The 7-point Laplacian in 4x4 blocks: under two warp steps per block row,
+    so a lane group per block row (odd and even block counts per row).  At
+    32^3 the block values fit in half of L2 and load with the default cache
+    policy; at 96^3 (99-198 MB of values) they stream evict-first."""
     from smaxkernels_b200 import matrices as M
-    rp, col, val = M.laplace3d_7pt(32, dtype=vt)
+    rp, col, val = M.laplace3d_7pt(side, dtype=vt)
     n = len(rp) - 1
     smax = _iface()
     b = smax.utils.convert_crs_to_bcrs(n, n, len(col), col, rp, val, 4, 4, 4, 4, col_major)
