@@ -55,12 +55,12 @@ __device__ __forceinline__ void load16(const VT *p, VT *o) {
 
 constexpr int kMaxBs = 128;  // largest block size of the stream path
 
+// The stream loop of one block row per warp (the kernels below launch it).
 template <typename VT, bool UNROLL>
-__global__ void __launch_bounds__(256) bcrs_stream_kernel(const int *__restrict__ row_ptr,
-                                                          const int *__restrict__ col, const VT *__restrict__ val,
-                                                          int64_t n_brows, int bh, int bw, int hpad, int wpad,
-                                                          int col_major, const VT *__restrict__ x,
-                                                          VT *__restrict__ y) {
+__device__ __forceinline__ void bcrs_stream_rows(const int *__restrict__ row_ptr, const int *__restrict__ col,
+                                                 const VT *__restrict__ val, int64_t n_brows, int bh, int bw,
+                                                 int hpad, int wpad, int col_major, const VT *__restrict__ x,
+                                                 VT *__restrict__ y) {
     constexpr int VEC = V16<VT>::N;
     __shared__ VT tile[8][kMaxBs];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -140,6 +140,28 @@ __global__ void __launch_bounds__(256) bcrs_stream_kernel(const int *__restrict_
         for (int j = 0; j < bw; ++j) s += tile[warp][col_major ? j * hpad + ix : ix * wpad + j];
         st_stream(y + br * hpad + ix, s);
     }
+}
+
+template <typename VT, bool UNROLL>
+__global__ void __launch_bounds__(256) bcrs_stream_kernel(const int *__restrict__ row_ptr,
+                                                          const int *__restrict__ col, const VT *__restrict__ val,
+                                                          int64_t n_brows, int bh, int bw, int hpad, int wpad,
+                                                          int col_major, const VT *__restrict__ x,
+                                                          VT *__restrict__ y) {
+    bcrs_stream_rows<VT, UNROLL>(row_ptr, col, val, n_brows, bh, bw, hpad, wpad, col_major, x, y);
+}
+
+// FP64: at most 48 registers, five CTAs per SM instead of four (the four-step
+// loop spills 32 bytes; 2^22 lognormal 4x4: 2.30 -> 2.26 ms; a bound of six
+// CTAs spilled 64 bytes and took 2.54 ms).  FP32 keeps the plain kernel: the
+// same bound spilled 88 bytes there.
+template <bool UNROLL>
+__global__ void __launch_bounds__(256, 5) bcrs_stream_kernel_f64(const int *__restrict__ row_ptr,
+                                                                 const int *__restrict__ col,
+                                                                 const double *__restrict__ val, int64_t n_brows,
+                                                                 int bh, int bw, int hpad, int wpad, int col_major,
+                                                                 const double *__restrict__ x, double *__restrict__ y) {
+    bcrs_stream_rows<double, UNROLL>(row_ptr, col, val, n_brows, bh, bw, hpad, wpad, col_major, x, y);
 }
 
 // Short block rows: a group of G = bs / VEC lanes per block row (8 lanes for
@@ -321,6 +343,11 @@ void bcrs_spmv(const DevBCRS &m, const VT *x, VT *y, cudaStream_t st) {
             bcrs_group_kernel<VT, false><<<ceil_div_u((uint64_t)m.n_rows * group, 256), 256, 0, st>>>(
                 m.row_ptr.as<int>(), m.col.as<int>(), m.val.as<VT>(), m.n_rows, (int)m.bh, (int)m.bw, (int)m.hpad,
                 (int)m.wpad, m.col_major ? 1 : 0, x, y);
+        else if (steps >= 3.0 && sizeof(VT) == 8)
+            bcrs_stream_kernel_f64<true><<<ceil_div_u(m.n_rows, 8), 256, 0, st>>>(
+                m.row_ptr.as<int>(), m.col.as<int>(), reinterpret_cast<const double *>(m.val.as<VT>()), m.n_rows,
+                (int)m.bh, (int)m.bw, (int)m.hpad, (int)m.wpad, m.col_major ? 1 : 0,
+                reinterpret_cast<const double *>(x), reinterpret_cast<double *>(y));
         else if (steps >= 3.0)
             bcrs_stream_kernel<VT, true><<<ceil_div_u(m.n_rows, 8), 256, 0, st>>>(
                 m.row_ptr.as<int>(), m.col.as<int>(), m.val.as<VT>(), m.n_rows, (int)m.bh, (int)m.bw, (int)m.hpad,
