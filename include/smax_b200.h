@@ -398,7 +398,8 @@ void smax_free_host(void *p);
  * Limits: n_rows <= SMAX_NOALLOC_MAX_ROWS and nnz <= SMAX_NOALLOC_MAX_NNZ, else
  * SMAX_ERR_BAD_ARG.  Calls share the scratch area: calls that overlap on the
  * GPU race, so issue them on one stream or serialise them.  The first call on
- * a device looks up the scratch address; make it before any stream capture.
+ * a device does the set-up (it looks up the scratch address); make it before
+ * any stream capture.
  * The call validates the matrix (SMAX_ERR_COL_OOB / SMAX_ERR_BAD_ARG) and
  * synchronises `stream` (a cudaStream_t; NULL = legacy default stream). */
 #define SMAX_NOALLOC_MAX_ROWS (1 << 20)

@@ -17,9 +17,9 @@
 //     start at zero (the bit mask, the status word) is cleared by each call;
 //   * calls that overlap on the GPU (two streams, or two host threads) race
 //     on it -- order them on one stream or serialise them;
-//   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//   * the first call on a device does the set-up: it looks up the array's
+//     device address (cudaGetSymbolAddress) with that device current; make
+//     that first call before any stream capture.
 // Limits: n_rows <= SMAX_NOALLOC_MAX_ROWS, nnz <= SMAX_NOALLOC_MAX_NNZ; larger
 // problems are rejected with SMAX_ERR_BAD_ARG before any work is queued.
 #include <mutex>
