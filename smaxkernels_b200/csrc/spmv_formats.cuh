@@ -23,6 +23,9 @@ struct DevSCS {
     // fix-up pass adds in task order
     int64_t n_tasks = 0, n_multi = 0, n_slots = 0;
     DevBuf task_chunk, task_j0, task_slot, multi_chunk, multi_first, multi_count, partial;
+    // per padded row: its entries up to the last one that is not padding
+    // (column 0, value 0); the task kernel skips the rest when x[0] is finite
+    DevBuf row_len;
     int plan_vbytes = 0;
 };
 

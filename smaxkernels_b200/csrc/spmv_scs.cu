@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(256) scs_task_kernel(const int *__restrict__ c
                                                        const int *__restrict__ task_slot, int64_t n_tasks,
                                                        const int *__restrict__ col, const VT *__restrict__ val,
                                                        const VT *__restrict__ x, VT *__restrict__ y,
-                                                       VT *__restrict__ partial) {
+                                                       VT *__restrict__ partial, const int *__restrict__ row_len) {
     constexpr int C = LPC * VEC;
     constexpr int CPI = 32 / LPC;  // chunk columns per warp instruction
     const int lane = threadIdx.x & 31;
@@ -137,15 +137,33 @@ __global__ void __launch_bounds__(256) scs_task_kernel(const int *__restrict__ c
     VT acc[VEC];
 #pragma unroll
     for (int i = 0; i < VEC; ++i) acc[i] = VT(0);
+    // Entries past a row's last stored entry are the layout's padding
+    // (column 0, value 0): their products 0 * x[0] add nothing when x[0] is
+    // finite, so the lane neither loads them nor gathers for them -- the
+    // sectors of a column that hold only padding are not fetched.  With a
+    // non-finite x[0] every stored entry is used, as the reference does.
+    int rl[VEC], rlmax = 0x7fffffff;
+#pragma unroll
+    for (int i = 0; i < VEC; ++i) rl[i] = 0x7fffffff;
+    if (row_len && isfinite(__ldg(x))) {
+        rlmax = 0;
+#pragma unroll
+        for (int i = 0; i < VEC; ++i) {
+            rl[i] = row_len[(int64_t)c * C + sub * VEC + i];
+            rlmax = max(rlmax, rl[i]);
+        }
+    }
     int j = jt + lane / LPC;
     auto step = [&](int jj) {
+        if (jj >= rlmax) return;
         const int64_t idx = cs + (int64_t)jj * C + sub * VEC;
         VT v[VEC];
         load_vals<VT, VEC>(val + idx, v);
         int cc[VEC];
         load_cols<VEC>(col + idx, cc);
 #pragma unroll
-        for (int i = 0; i < VEC; ++i) acc[i] += v[i] * __ldcg(x + cc[i]);
+        for (int i = 0; i < VEC; ++i)
+            if (jj < rl[i]) acc[i] += v[i] * __ldcg(x + cc[i]);
     };
     for (; j + 3 * CPI < jl; j += 4 * CPI) {
         // four columns' loads first, then their products in column order
@@ -155,18 +173,27 @@ __global__ void __launch_bounds__(256) scs_task_kernel(const int *__restrict__ c
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int64_t idx = i0 + (int64_t)u * CPI * C;
-            load_vals<VT, VEC>(val + idx, v[u]);
-            load_cols<VEC>(col + idx, cc[u]);
+            if (j + u * CPI < rlmax) {
+                load_vals<VT, VEC>(val + idx, v[u]);
+                load_cols<VEC>(col + idx, cc[u]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < VEC; ++i) {
+                    v[u][i] = VT(0);
+                    cc[u][i] = 0;
+                }
+            }
         }
         VT xv[4][VEC];
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
-            for (int i = 0; i < VEC; ++i) xv[u][i] = __ldcg(x + cc[u][i]);
+            for (int i = 0; i < VEC; ++i) xv[u][i] = j + u * CPI < rl[i] ? __ldcg(x + cc[u][i]) : VT(0);
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
-            for (int i = 0; i < VEC; ++i) acc[i] += v[u][i] * xv[u][i];
+            for (int i = 0; i < VEC; ++i)
+                if (j + u * CPI < rl[i]) acc[i] += v[u][i] * xv[u][i];
     }
     for (; j < jl; j += CPI) step(j);
 #pragma unroll
@@ -298,6 +325,25 @@ bool scs_vector_path(int64_t C, int vbytes) {
     return C % vec == 0 && C / vec >= 1 && C / vec <= 32 && ((C / vec) & (C / vec - 1)) == 0;
 }
 
+namespace {
+template <typename VT>
+__global__ void scs_row_len_kernel(const int *__restrict__ chunk_ptr, const int *__restrict__ chunk_len,
+                                   const int *__restrict__ col, const VT *__restrict__ val, int64_t C,
+                                   int64_t n_rows_padded, int *__restrict__ row_len) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rows_padded) return;
+    const int64_t c = r / C, l = r % C;
+    const int64_t cs = chunk_ptr[c];
+    int j = chunk_len[c];
+    while (j > 0) {
+        const int64_t idx = cs + (int64_t)(j - 1) * C + l;
+        if (col[idx] != 0 || val[idx] != VT(0)) break;
+        --j;
+    }
+    row_len[r] = j;
+}
+}  // namespace
+
 void scs_plan(DevSCS &m, int vbytes, cudaStream_t st) {
     const int64_t nc = m.n_chunks;
     std::vector<int> len(nc > 0 ? nc : 1);
@@ -334,6 +380,21 @@ void scs_plan(DevSCS &m, int vbytes, cudaStream_t st) {
     m.n_multi = (int64_t)mc.size();
     m.n_slots = slots;
     m.plan_vbytes = vbytes;
+    // each padded row's length up to its last stored entry that is not
+    // padding (column 0 with value 0)
+    m.row_len.alloc(sizeof(int) * (m.n_rows_padded > 0 ? m.n_rows_padded : 1));
+    if (m.n_rows_padded > 0) {
+        const unsigned g = ceil_div_u(m.n_rows_padded, 256);
+        if (vbytes == 8)
+            scs_row_len_kernel<double><<<g, 256, 0, st>>>(m.chunk_ptr.as<int>(), m.chunk_len.as<int>(),
+                                                            m.col.as<int>(), m.val.as<double>(), m.C,
+                                                            m.n_rows_padded, m.row_len.as<int>());
+        else
+            scs_row_len_kernel<float><<<g, 256, 0, st>>>(m.chunk_ptr.as<int>(), m.chunk_len.as<int>(),
+                                                           m.col.as<int>(), m.val.as<float>(), m.C,
+                                                           m.n_rows_padded, m.row_len.as<int>());
+        SMAX_CUDA(cudaGetLastError());
+    }
     SMAX_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -341,14 +402,19 @@ namespace {
 
 template <typename VT, int VEC>
 void launch_task(int64_t lpc, unsigned grid, const int *cp, const int *cl, const int *tc, const int *tj, const int *ts,
-                 int64_t n_tasks, const int *ci, const VT *v, const VT *x, VT *y, VT *part, cudaStream_t st) {
+                 int64_t n_tasks, const int *ci, const VT *v, const VT *x, VT *y, VT *part, const int *rl,
+                 cudaStream_t st) {
     switch (lpc) {
-    case 1: scs_task_kernel<VT, 1, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part); break;
-    case 2: scs_task_kernel<VT, 2, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part); break;
-    case 4: scs_task_kernel<VT, 4, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part); break;
-    case 8: scs_task_kernel<VT, 8, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part); break;
-    case 16: scs_task_kernel<VT, 16, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part); break;
-    case 32: scs_task_kernel<VT, 32, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part); break;
+    case 1: scs_task_kernel<VT, 1, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part, rl); break;
+    case 2: scs_task_kernel<VT, 2, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part, rl); break;
+    case 4: scs_task_kernel<VT, 4, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part, rl); break;
+    case 8: scs_task_kernel<VT, 8, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part, rl); break;
+    case 16:
+        scs_task_kernel<VT, 16, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part, rl);
+        break;
+    case 32:
+        scs_task_kernel<VT, 32, VEC><<<grid, 256, 0, st>>>(cp, cl, tc, tj, ts, n_tasks, ci, v, x, y, part, rl);
+        break;
     default: fail(SMAX_ERR_STATE, "unexpected SELL chunk width");
     }
 }
@@ -381,8 +447,9 @@ void scs_spmv(const DevSCS &m, const VT *x, VT *y, cudaStream_t st) {
         const int *tc = m.task_chunk.as<int>(), *tj = m.task_j0.as<int>(), *ts = m.task_slot.as<int>();
         const VT *v = m.val.as<VT>();
         VT *part = m.partial.as<VT>();
-        if (vec == 1) launch_task<VT, 1>(m.C, grid, cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part, st);
-        else launch_task<VT, 2>(m.C / 2, grid, cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part, st);
+        const int *rl = m.row_len.p ? m.row_len.as<int>() : nullptr;
+        if (vec == 1) launch_task<VT, 1>(m.C, grid, cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part, rl, st);
+        else launch_task<VT, 2>(m.C / 2, grid, cp, cl, tc, tj, ts, m.n_tasks, ci, v, x, y, part, rl, st);
         if (m.n_multi > 0)
             scs_fixup_kernel<VT><<<ceil_div_u(m.n_multi * m.C, 256), 256, 0, st>>>(
                 m.multi_chunk.as<int>(), m.multi_first.as<int>(), m.multi_count.as<int>(), m.n_multi, (int)m.C, part,

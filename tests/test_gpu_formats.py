@@ -342,3 +342,46 @@ def test_spmm_config2_stencil27(vt, k_):
     Y = gpu_spmm(rp, col, val, X, k_, True)
     Y_ref = O.spmm(rp, col, val.astype(np.float64), X.astype(np.float64), k_, row_major=True)
     assert normwise(Y, Y_ref) <= tol(vt)
+
+
+@pytest.mark.parametrize("vt", [np.float64, np.float32])
+@pytest.mark.parametrize("x0", [1.5, np.inf, np.nan])
+def test_scs_padding_skip_matches_reference_semantics(vt, x0):
+    """The SELL task kernel skips each row's padding (column 0, value 0 past its
+    last other stored entry) when x[0] is finite.  With x[0] infinite or NaN it
+    uses every stored entry, as the reference's SELL loop does, so 0 * x[0]
+    makes NaN in every row that holds padding -- the oracle's SELL product
+    (over all stored entries) is the reference here.  Some rows end with an
+    explicit zero in column 0, which the kernel may skip with a finite x[0]."""
+    rng = np.random.default_rng(46)
+    n = 3000
+    lens = rng.integers(1, 40, n)
+    lens[::50] = 300
+    rows = []
+    for r, l in enumerate(lens):
+        c = np.sort(rng.choice(np.arange(1, n), int(l), replace=False)).astype(np.int32)
+        if r % 7 == 0:
+            c = np.concatenate([c[:-1], [0]]).astype(np.int32)  # ends in column 0
+        rows.append(c)
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum(lens)
+    col = np.concatenate(rows).astype(np.int32)
+    val = rng.uniform(-1, 1, len(col)).astype(vt)
+    val[rp[1:][::7] - 1] = 0.0  # those column-0 entries are explicit zeros
+    smax = _iface()
+    s = smax.utils.convert_crs_to_scs(n, n, len(col), col, rp, val, 32, 128)
+    smax.close()
+    x = rng.uniform(-1, 1, n).astype(vt)
+    x[0] = x0
+    y = gpu_scs_spmv(s, x)
+    xx = np.zeros(max(s["n_rows_padded"], n), vt)
+    xx[:n] = x
+    y_ref = O.spmv_scs(32, s["chunk_ptr"], s["chunk_lengths"], s["col"], s["val"], xx, s["n_rows_padded"])
+    y, y_ref = y[: s["n_rows_padded"]], y_ref[: s["n_rows_padded"]]
+    np.testing.assert_array_equal(np.isnan(y), np.isnan(y_ref))
+    if np.isfinite(x0):
+        assert not np.isnan(y).any()
+    else:
+        assert np.isnan(y).any()
+    fin = ~np.isnan(y_ref)
+    assert normwise(y[fin], y_ref[fin]) <= tol(vt)
