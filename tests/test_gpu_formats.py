@@ -385,3 +385,31 @@ def test_scs_padding_skip_matches_reference_semantics(vt, x0):
         assert np.isnan(y).any()
     fin = ~np.isnan(y_ref)
     assert normwise(y[fin], y_ref[fin]) <= tol(vt)
+
+
+def test_scs_split_chunks_repeated_products():
+    """Chunks longer than 32 columns are split over several warps and the
+    chunk's last warp adds their partial sums; its counter must be back at 0
+    for the next product.  Five products on one kernel object, x changing."""
+    from smaxkernels_b200 import IntType, KernelType, PlatformType
+    rp, col, val = rand_crs(4000, 30, 47, empty_frac=0.05, long_rows=(1500, 700, 300))
+    n = len(rp) - 1
+    smax = _iface()
+    s = smax.utils.convert_crs_to_scs(n, n, len(col), col, rp, val, 32, 256)
+    assert max(s["chunk_lengths"]) > 32
+    smax.register_kernel("k", KernelType.SPMV, PlatformType.CUDA, IntType.INT32, _ft(val.dtype))
+    k = smax.kernel("k")
+    k.set_mat_scs(True)
+    vs = max(s["n_rows_padded"], n)
+    xx = np.zeros(vs)
+    y = np.zeros(vs)
+    k.register_A(s["C"], s["sigma"], s["n_rows"], s["n_rows_padded"], n, s["n_chunks"], s["n_elements"],
+                 s["nnz"], s["chunk_ptr"], s["chunk_lengths"], s["col"], s["val"], s["perm"])
+    k.register_B(vs, xx)
+    k.register_C(vs, y)
+    rng = np.random.default_rng(48)
+    for _ in range(5):
+        xx[:n] = rng.uniform(-1, 1, n)
+        k.run()
+        assert normwise(y[s["perm"]], O.spmv_crs(rp, col, val, xx[:n])) <= 1e-12
+    smax.close()
