@@ -129,6 +129,7 @@ void spmv_upload(smax_kernel_s *k) {
         if (nv) SMAX_CUDA(cudaMemcpyAsync(d.val.p, r.val, (size_t)k->vbytes * nv, cudaMemcpyHostToDevice, st));
         validate_bcrs(d, dstatus(k), st);
         read_status(k);
+        bcrs_plan(d, st);
     } else {
         require(k->A.set, SMAX_ERR_STATE, "register_A before initialize");
         upload_crs(k->dA, k->A, k->vbytes, st, crs_stream_pad());

@@ -26,6 +26,7 @@
 // the in-block index of the chosen order; blocks are zero-filled first.
 #include "spmv_formats.cuh"
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_segmented_radix_sort.cuh>
 #include <cub/device/device_select.cuh>
@@ -60,12 +61,13 @@ template <typename VT, bool UNROLL>
 __device__ __forceinline__ void bcrs_stream_rows(const int *__restrict__ row_ptr, const int *__restrict__ col,
                                                  const VT *__restrict__ val, int64_t n_brows, int bh, int bw,
                                                  int hpad, int wpad, int col_major, const VT *__restrict__ x,
-                                                 VT *__restrict__ y) {
+                                                 VT *__restrict__ y, const int *__restrict__ order) {
     constexpr int VEC = V16<VT>::N;
     __shared__ VT tile[8][kMaxBs];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t br = (int64_t)blockIdx.x * 8 + warp;
-    if (br >= n_brows) return;  // uniform per warp
+    const int64_t w = (int64_t)blockIdx.x * 8 + warp;
+    if (w >= n_brows) return;  // uniform per warp
+    const int64_t br = order ? order[w] : w;
     const int bs = hpad * wpad;
     const int o = (lane * VEC) % bs;  // this lane's first in-block position
     int jx[VEC];
@@ -147,8 +149,8 @@ __global__ void __launch_bounds__(256) bcrs_stream_kernel(const int *__restrict_
                                                           const int *__restrict__ col, const VT *__restrict__ val,
                                                           int64_t n_brows, int bh, int bw, int hpad, int wpad,
                                                           int col_major, const VT *__restrict__ x,
-                                                          VT *__restrict__ y) {
-    bcrs_stream_rows<VT, UNROLL>(row_ptr, col, val, n_brows, bh, bw, hpad, wpad, col_major, x, y);
+                                                          VT *__restrict__ y, const int *__restrict__ order) {
+    bcrs_stream_rows<VT, UNROLL>(row_ptr, col, val, n_brows, bh, bw, hpad, wpad, col_major, x, y, order);
 }
 
 // FP64: at most 48 registers, five CTAs per SM instead of four (the four-step
@@ -160,8 +162,9 @@ __global__ void __launch_bounds__(256, 5) bcrs_stream_kernel_f64(const int *__re
                                                                  const int *__restrict__ col,
                                                                  const double *__restrict__ val, int64_t n_brows,
                                                                  int bh, int bw, int hpad, int wpad, int col_major,
-                                                                 const double *__restrict__ x, double *__restrict__ y) {
-    bcrs_stream_rows<double, UNROLL>(row_ptr, col, val, n_brows, bh, bw, hpad, wpad, col_major, x, y);
+                                                                 const double *__restrict__ x, double *__restrict__ y,
+                                                                 const int *__restrict__ order) {
+    bcrs_stream_rows<double, UNROLL>(row_ptr, col, val, n_brows, bh, bw, hpad, wpad, col_major, x, y, order);
 }
 
 // Short block rows: a group of G = bs / VEC lanes per block row (8 lanes for
@@ -324,6 +327,7 @@ bool bcrs_stream_path(int64_t hpad, int64_t wpad, int vbytes) {
 template <typename VT>
 void bcrs_spmv(const DevBCRS &m, const VT *x, VT *y, cudaStream_t st) {
     if (m.n_rows == 0) return;
+    const int *order = m.order.p ? m.order.as<int>() : nullptr;
     if (bcrs_stream_path(m.hpad, m.wpad, sizeof(VT))) {
         // mean warp steps per block row: below two a lane group per block row
         // wastes fewer lanes; the four-step loop pays off from about three
@@ -347,20 +351,47 @@ void bcrs_spmv(const DevBCRS &m, const VT *x, VT *y, cudaStream_t st) {
             bcrs_stream_kernel_f64<true><<<ceil_div_u(m.n_rows, 8), 256, 0, st>>>(
                 m.row_ptr.as<int>(), m.col.as<int>(), reinterpret_cast<const double *>(m.val.as<VT>()), m.n_rows,
                 (int)m.bh, (int)m.bw, (int)m.hpad, (int)m.wpad, m.col_major ? 1 : 0,
-                reinterpret_cast<const double *>(x), reinterpret_cast<double *>(y));
+                reinterpret_cast<const double *>(x), reinterpret_cast<double *>(y), order);
         else if (steps >= 3.0)
             bcrs_stream_kernel<VT, true><<<ceil_div_u(m.n_rows, 8), 256, 0, st>>>(
                 m.row_ptr.as<int>(), m.col.as<int>(), m.val.as<VT>(), m.n_rows, (int)m.bh, (int)m.bw, (int)m.hpad,
-                (int)m.wpad, m.col_major ? 1 : 0, x, y);
+                (int)m.wpad, m.col_major ? 1 : 0, x, y, order);
         else
             bcrs_stream_kernel<VT, false><<<ceil_div_u(m.n_rows, 8), 256, 0, st>>>(
                 m.row_ptr.as<int>(), m.col.as<int>(), m.val.as<VT>(), m.n_rows, (int)m.bh, (int)m.bw, (int)m.hpad,
-                (int)m.wpad, m.col_major ? 1 : 0, x, y);
+                (int)m.wpad, m.col_major ? 1 : 0, x, y, order);
     } else
         bcrs_thread_kernel<VT><<<ceil_div_u(m.n_rows, 128), 128, 0, st>>>(
             m.row_ptr.as<int>(), m.col.as<int>(), m.val.as<VT>(), m.n_rows, (int)m.bh, (int)m.bw, (int)m.hpad,
             (int)m.wpad, m.col_major ? 1 : 0, x, y);
     SMAX_CUDA(cudaGetLastError());
+}
+
+namespace {
+__global__ void bcrs_row_lengths(const int *__restrict__ row_ptr, int64_t n, int *__restrict__ len,
+                                 int *__restrict__ idx) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    len[r] = row_ptr[r + 1] - row_ptr[r];
+    idx[r] = (int)r;
+}
+}  // namespace
+
+void bcrs_plan(DevBCRS &m, cudaStream_t st) {
+    m.order.release();
+    if (m.n_rows < 2) return;
+    const int64_t n = m.n_rows;
+    DevBuf len(sizeof(int) * n), idx(sizeof(int) * n), len_sorted(sizeof(int) * n);
+    m.order.alloc(sizeof(int) * n);
+    bcrs_row_lengths<<<ceil_div_u(n, 256), 256, 0, st>>>(m.row_ptr.as<int>(), n, len.as<int>(), idx.as<int>());
+    SMAX_CUDA(cudaGetLastError());
+    size_t tb = 0;
+    SMAX_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, len.as<int>(), len_sorted.as<int>(),
+                                                        idx.as<int>(), m.order.as<int>(), (int)n, 0, 32, st));
+    DevBuf tmp(tb ? tb : 1);
+    SMAX_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.p, tb, len.as<int>(), len_sorted.as<int>(),
+                                                        idx.as<int>(), m.order.as<int>(), (int)n, 0, 32, st));
+    SMAX_CUDA(cudaStreamSynchronize(st));
 }
 
 template void bcrs_spmv<double>(const DevBCRS &, const double *, double *, cudaStream_t);

@@ -38,7 +38,11 @@ struct DevBCRS {
     int64_t n_rows = 0, n_cols = 0, n_blocks = 0, bh = 0, bw = 0, hpad = 0, wpad = 0;
     bool col_major = false;
     DevBuf row_ptr, col, val;
+    // block rows longest first (bcrs_plan): the warp-per-block-row kernel
+    // starts the long rows first, so none is left running alone at the end
+    DevBuf order;
 };
+void bcrs_plan(DevBCRS &m, cudaStream_t st);
 
 void validate_scs(const DevSCS &m, DevStatus *st, cudaStream_t s);
 void validate_bcrs(const DevBCRS &m, DevStatus *st, cudaStream_t s);
