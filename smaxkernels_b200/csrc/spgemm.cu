@@ -582,12 +582,8 @@ void merge_write(const DevCRS &A, const DevCRS &B, DevCRS &C, SpgemmWork &w, int
     stage = std::max(8, (stage + 7) / 8 * 8);
     if (stage > 32 * kSmallP) fail(SMAX_ERR_STATE, "SpGEMM merge path: staging size out of range");
     constexpr int kMaxSmem = kMergeWriteThreads / 32 * 32 * kSmallP * (int)(sizeof(VT) + sizeof(int));
-    static bool attr_set = false;
-    if (!attr_set) {
-        SMAX_CUDA(cudaFuncSetAttribute(gustavson_merge_write<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       kMaxSmem));
-        attr_set = true;
-    }
+    // set on every call: the attribute belongs to the current device
+    SMAX_CUDA(cudaFuncSetAttribute(gustavson_merge_write<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem));
     const size_t smem = (size_t)kMergeWriteThreads / 32 * stage * (sizeof(VT) + sizeof(int));
     gustavson_merge_write<VT><<<ceil_div_u(n, kMergeWriteThreads), kMergeWriteThreads, smem, st>>>(
         n, stage, A.rp(), A.ci(), A.val.as<VT>(), B.rp(), B.ci(), B.val.as<VT>(), w.masks.as<unsigned long long>(),
