@@ -29,7 +29,7 @@ struct DevSCS {
     int plan_vbytes = 0;
 };
 
-constexpr int kScsTaskCols = 32;
+constexpr int kScsTaskCols = 64;
 // Builds the task plan of a SELL-C-sigma matrix (after upload or conversion).
 void scs_plan(DevSCS &m, int vbytes, cudaStream_t st);
 
