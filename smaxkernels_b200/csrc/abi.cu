@@ -34,16 +34,28 @@ smax_kernel_s *K(smax_kernel k) {
     return k;
 }
 
-void read_status(smax_kernel_s *k) {
-    if (!k->status.p) return;
+namespace {
+// The status word, after the work queued on the kernel's stream.
+DevStatus fetch_status(smax_kernel_s *k) {
     DevStatus st{};
     SMAX_CUDA(cudaMemcpyAsync(&st, k->status.p, sizeof(st), cudaMemcpyDeviceToHost, k->stream));
     SMAX_CUDA(cudaStreamSynchronize(k->stream));
+    return st;
+}
+
+// A recorded device error: clear it and report it.
+void check_status(smax_kernel_s *k, const DevStatus &st) {
     if (st.code != 0) {
         SMAX_CUDA(cudaMemsetAsync(k->status.p, 0, sizeof(DevStatus), k->stream));
         SMAX_CUDA(cudaStreamSynchronize(k->stream));
         fail(st.code, "device reported error " + std::to_string(st.code) + " at index " + std::to_string(st.index));
     }
+}
+}  // namespace
+
+void read_status(smax_kernel_s *k) {
+    if (!k->status.p) return;
+    check_status(k, fetch_status(k));
 }
 
 DevStatus *dstatus(smax_kernel_s *k) { return k->status.as<DevStatus>(); }
@@ -574,12 +586,18 @@ void do_finalize(smax_kernel_s *k) {
                 SMAX_CUDA(cudaMemcpyAsync(host + r.off * vb, dev + r.off * vb, r.count * vb, cudaMemcpyDeviceToHost,
                                           k->copy_stream));
         }
+        // the status word is read while the output downloads: its copy waits
+        // only for the kernels on the kernel's stream; an error is reported
+        // once no download into the caller's memory is in flight
+        const DevStatus st = k->status.p ? fetch_status(k) : DevStatus{};
         SMAX_CUDA(cudaStreamSynchronize(k->copy_stream));
         for (const auto &r : k->out_ranges) k->ev_pool.push_back(r.ev);
         k->out_ranges.clear();
+        if (k->status.p) check_status(k, st);
+    } else {
+        SMAX_CUDA(cudaStreamSynchronize(k->stream));
+        read_status(k);
     }
-    SMAX_CUDA(cudaStreamSynchronize(k->stream));
-    read_status(k);
     k->timers["apply"] += k->apply_events.drain();
     k->timers["finalize"] += wall_s() - t0;
 }
