@@ -253,3 +253,47 @@ def test_spgemm_timers_off():
     for name in ("apply", "Symbolic_Setup", "Fused_Gustavson", "Alloc_C", "Compress"):
         assert k.timer(name) == 0.0, name
     smax.close()
+
+
+def test_spgemm_direct_path_with_a_growing_and_shrinking_product():
+    """Three runs on one kernel object, each on the direct merge path from the
+    last run's hint: rows of A with at most 4 entries, then up to 8 (a larger
+    C: more entries and a fuller warp to stage), then at most 4 again.  C's
+    arrays and the staging size follow each product; every run matches the
+    oracle."""
+    from smaxkernels_b200 import FloatType, Interface, IntType, KernelType, PlatformType
+    rng = np.random.default_rng(129)
+    n = 2500
+    blens = rng.integers(1, 9, n)
+    brp = np.zeros(n + 1, np.int32)
+    brp[1:] = np.cumsum(blens)
+    bcol = np.concatenate([np.sort(rng.choice(n, int(l), replace=False)) for l in blens]).astype(np.int32)
+    B = (brp, bcol, rng.uniform(-1, 1, len(bcol)))
+
+    def make_a(max_len, seed):
+        r = np.random.default_rng(seed)
+        lens = r.integers(0, max_len + 1, n)
+        rows = [r.choice(n, int(l), replace=False) for l in lens]
+        rp = np.zeros(n + 1, np.int32)
+        rp[1:] = np.cumsum(lens)
+        col = np.concatenate(rows).astype(np.int32)
+        return rp, col, r.uniform(-1, 1, len(col))
+
+    small, big = make_a(4, 130), make_a(8, 131)
+    smax = Interface()
+    smax.register_kernel("g", KernelType.SPGEMM, PlatformType.CUDA, IntType.INT32, FloatType.FLOAT64)
+    k = smax.kernel("g")
+    k.register_B(n, n, len(B[1]), B[1], B[0], B[2])
+    nnzs = []
+    for a in (small, big, small):
+        k.register_A(n, n, len(a[1]), a[1], a[0], a[2])
+        k.register_C()
+        k.run()
+        _, _, nnz, crp, ccol, cval = k.result()
+        orp, ocol, oval = O.spgemm(*a, *B, n)
+        np.testing.assert_array_equal(crp, orp)
+        np.testing.assert_array_equal(ccol, ocol)
+        assert normwise(cval, oval) <= 1e-12
+        nnzs.append(nnz)
+    assert nnzs[1] > nnzs[0]
+    smax.close()
